@@ -1,0 +1,187 @@
+// instance_cull.cu — per-draw frustum + sub-pixel cull (IndirectDispatchPass) and
+// per-draw Hi-Z occlusion cull (OcclusionCullPass), separately or fused.
+//
+// References:
+//   crates/helio-pass-indirect-dispatch/shaders/indirect_dispatch.wgsl:79-176
+//   crates/helio-pass-occlusion-cull/shaders/occlusion_cull.wgsl:101-220
+//     (the static Hi-Z branch, :222-259, is off in every supported configuration)
+// One thread per draw call. Statistics are aggregated per warp (ballot + popc)
+// before one atomic per warp and slot; the totals equal the reference's
+// per-thread atomics.
+
+#include "common.cuh"
+#include "kernels.h"
+#include "instance_cull.h"
+
+namespace helio {
+
+namespace {
+
+template <bool kFrustum, bool kOcclusion>
+__global__ void __launch_bounds__(256) instance_cull_kernel(InstanceCullParams P) {
+    __shared__ HizView s_hiz;
+    if (kOcclusion) {
+        if (threadIdx.x == 0) copy_hiz(P.hiz, s_hiz);
+        __syncthreads();
+    }
+    const uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool active = idx < P.draw_count;
+    const int lane = threadIdx.x & 31;
+
+    bool c_total = false, c_frustum = false, c_subpixel = false, c_visible = false, c_shadow = false,
+         c_shadow_vis = false, c_occ = false, c_shadow_occ = false;
+
+    if (active && P.draw_calls[idx].first_instance >= P.instance_count) {
+        // A draw whose representative instance lies outside the instance buffer has
+        // no bounds to test: it is written as frustum-culled and not occlusion-tested.
+        if (kFrustum) {
+            const HelioGpuDrawCall dc = P.draw_calls[idx];
+            uint32_t* o = P.indirect + (size_t)idx * 5;
+            o[0] = dc.index_count;
+            o[1] = 0u;
+            o[2] = dc.first_index;
+            o[3] = (uint32_t)dc.vertex_offset;
+            o[4] = dc.first_instance;
+            c_frustum = true;
+            c_total = true;
+        }
+    } else if (active) {
+        const HelioGpuDrawCall dc = P.draw_calls[idx];
+        const uint32_t ii = dc.first_instance;
+        const float4 bounds = __ldg(reinterpret_cast<const float4*>(P.instances[ii].bounds));
+        const uint32_t flags = __ldg(&P.instances[ii].flags);
+        const HelioGpuCameraUniforms* cam = P.camera;
+        const Mat4 vp = ldg_mat4(cam->view_proj);
+        const F3 center = f3(bounds.x, bounds.y, bounds.z);
+        const float radius = bounds.w;
+        uint32_t instance_count_out = 0u;  // value of indirect[idx].instance_count after the frustum stage
+
+        if (kFrustum) {
+            const float4 amin = __ldg(reinterpret_cast<const float4*>(P.aabbs[ii].min));
+            const float4 amax = __ldg(reinterpret_cast<const float4*>(P.aabbs[ii].max));
+            // aabb_in_frustum (:88-98)
+            bool aabb_visible = true;
+#pragma unroll
+            for (int i = 0; i < 6; ++i) {
+                const float* pl = P.planes + i * 4;
+                float px = pl[0] >= 0.0f ? amax.x : amin.x;
+                float py = pl[1] >= 0.0f ? amax.y : amin.y;
+                float pz = pl[2] >= 0.0f ? amax.z : amin.z;
+                float dist = fadd(dot3(f3(pl[0], pl[1], pl[2]), f3(px, py, pz)), pl[3]);
+                aabb_visible = aabb_visible && !(dist < 0.0f);
+            }
+            const bool degenerate = amin.x == amax.x && amin.y == amax.y && amin.z == amax.z;
+            // sphere_in_frustum (:79-86)
+            bool sphere_visible = true;
+#pragma unroll
+            for (int i = 0; i < 6; ++i) {
+                const float* pl = P.planes + i * 4;
+                float dist = fadd(dot3(f3(pl[0], pl[1], pl[2]), center), pl[3]);
+                sphere_visible = sphere_visible && !(fadd(dist, radius) < 0.0f);
+            }
+            const bool visible = degenerate ? sphere_visible : aabb_visible;
+            bool should_draw = visible;
+            if (visible) {
+                const float4 clip = mat4_point4(vp, center);
+                if (clip.w > 0.0f) {
+                    const float p11 = __ldg(&cam->proj[5]);
+                    float r_ndc = fabsf(fdiv(fmul(radius, p11), clip.w));
+                    if (r_ndc < 0.001f) should_draw = false;
+                }
+            }
+            const bool shadow = (flags & 1u) != 0u;
+            c_shadow = shadow;
+            instance_count_out = should_draw ? dc.instance_count : 0u;
+            uint32_t* o = P.indirect + (size_t)idx * 5;
+            o[0] = dc.index_count;
+            o[1] = instance_count_out;
+            o[2] = dc.first_index;
+            o[3] = (uint32_t)dc.vertex_offset;
+            o[4] = dc.first_instance;
+            if (should_draw) {
+                c_visible = true;
+                c_shadow_vis = shadow;
+            } else if (!visible) {
+                c_frustum = true;
+            } else {
+                c_subpixel = true;
+            }
+            c_total = true;
+        }
+
+        if (kOcclusion) {
+            bool occluded = false;
+            if (radius > 0.0f) {
+                const float4 clip = mat4_point4(vp, center);
+                if (clip.w > 0.0f) {
+                    const float p00 = __ldg(&cam->proj[0]), p11 = __ldg(&cam->proj[5]);
+                    const float ndc_x = fdiv(clip.x, clip.w), ndc_y = fdiv(clip.y, clip.w);
+                    const float uv_x = fadd(fmul(ndc_x, 0.5f), 0.5f), uv_y = fadd(fmul(ndc_y, -0.5f), 0.5f);
+                    const float ndc_r = fmaxf(fabsf(fdiv(fmul(radius, p00), clip.w)), fabsf(fdiv(fmul(radius, p11), clip.w)));
+                    const bool off = fadd(ndc_x, ndc_r) < -1.0f || fsub(ndc_x, ndc_r) > 1.0f ||
+                                     fadd(ndc_y, ndc_r) < -1.0f || fsub(ndc_y, ndc_r) > 1.0f;
+                    if (!off) {
+                        // sphere_near_depth (:124-140)
+                        const float4 pn = __ldg(reinterpret_cast<const float4*>(cam->position_near));
+                        const F3 tc = sub3(center, f3(pn.x, pn.y, pn.z));
+                        const float dist_sq = dot3(tc, tc);
+                        float near_z = 0.0f;
+                        if (!(dist_sq <= fmul(radius, radius))) {
+                            const F3 dir = muls3(tc, fdiv(1.0f, fsqrt(dist_sq)));
+                            const F3 nws = sub3(center, muls3(dir, radius));
+                            const float4 nc = mat4_point4(vp, nws);
+                            near_z = nc.w <= 0.0f ? 0.0f : clampf(fdiv(nc.z, nc.w), 0.0f, 1.0f);
+                        }
+                        // screen_radius_px (:110-113), pick_mip (:116-120)
+                        const float half_h = fmul((float)P.screen_h, 0.5f);
+                        const float r_px = fabsf(fmul(fmul(fdiv(radius, clip.w), p11), half_h));
+                        const float diameter = fmaxf(fmul(r_px, 2.0f), 1.0f);
+                        const uint32_t mip = min(ceil_log2_exact(diameter), P.hiz_mip_count - 1u);
+                        const float uv_half = fmul(ndc_r, 0.5f);
+                        const float u0 = clampf(fsub(uv_x, uv_half), 0.0f, 1.0f), v0 = clampf(fsub(uv_y, uv_half), 0.0f, 1.0f);
+                        const float u1 = clampf(fadd(uv_x, uv_half), 0.0f, 1.0f), v1 = clampf(fadd(uv_y, uv_half), 0.0f, 1.0f);
+                        const float h00 = hiz_sample(s_hiz, u0, v0, mip);
+                        const float h01 = hiz_sample(s_hiz, u1, v0, mip);
+                        const float h10 = hiz_sample(s_hiz, u0, v1, mip);
+                        const float h11 = hiz_sample(s_hiz, u1, v1, mip);
+                        const float hz = fmaxf(fmaxf(h00, h01), fmaxf(h10, h11));
+                        occluded = near_z > fadd(hz, 1.0f / 65536.0f);
+                    }
+                }
+            }
+            if (occluded) {
+                uint32_t* ic = P.indirect + (size_t)idx * 5 + 1;
+                const bool was_visible = kFrustum ? (instance_count_out != 0u) : (*ic != 0u);
+                *ic = 0u;
+                if (was_visible) {
+                    c_occ = true;
+                    c_shadow_occ = (flags & 1u) != 0u;
+                }
+            }
+        }
+    }
+
+    // Warp-aggregated statistics (same totals as one atomic per thread).
+    const bool conds[8] = {c_total, c_frustum, c_subpixel, c_visible, c_occ, c_shadow, c_shadow_vis, c_shadow_occ};
+#pragma unroll
+    for (int s = 0; s < 8; ++s) {
+        const bool used = kFrustum ? (s != 4 && s != 7) : (s == 4 || s == 7);
+        if (!used && !(kFrustum && kOcclusion)) continue;
+        const uint32_t n = __popc(__ballot_sync(0xffffffffu, conds[s]));
+        if (lane == 0 && n) atomicAdd(P.stats + s, n);
+    }
+}
+
+}  // namespace
+
+void launch_instance_cull(const InstanceCullParams& p, bool frustum, bool occlusion, cudaStream_t stream) {
+    if (p.draw_count == 0) return;
+    const uint32_t blocks = (p.draw_count + 255u) / 256u;
+    if (frustum && occlusion) instance_cull_kernel<true, true><<<blocks, 256, 0, stream>>>(p);
+    else if (frustum) instance_cull_kernel<true, false><<<blocks, 256, 0, stream>>>(p);
+    else if (occlusion) instance_cull_kernel<false, true><<<blocks, 256, 0, stream>>>(p);
+    else return;
+    helio_note_launch();
+}
+
+}  // namespace helio

@@ -1,0 +1,475 @@
+// vg_cull.cu — virtual-geometry object select and meshlet cull (VirtualGeometryPass).
+//
+// References (crates/helio-pass-virtual-geometry/):
+//   shaders/vg_cull.wgsl:282-352   cs_select_objects  -> vg_select_kernel
+//   shaders/vg_cull.wgsl:135-264   cull_meshlet       -> meshlet_visible + emission
+//   shaders/vg_cull.wgsl:354-405   cs_cull_meshlets   -> vg_cull_kernel
+//   src/lib.rs:132-167             InstanceCullData::from_instance -> instance_cull_data_kernel
+//
+// Layout and scheduling (B200 design, not a translation of the WGSL dispatches):
+//   * meshlet descriptors are re-laid once per upload into four 16-byte streams;
+//   * a warp owns 32 consecutive work items (one per lane); the lanes first read
+//     their item and the object's selected-LOD record, then the warp packs the
+//     active meshlets of all 32 items densely into 32-lane windows, so a work item
+//     whose LOD has 13 meshlets occupies 13 lanes instead of a 64-lane group;
+//   * visible meshlets are compacted deterministically: window ballots are kept in
+//     shared memory, each CTA publishes its count with a decoupled look-back
+//     (one warp inspects 32 predecessors per step), then every visible meshlet is
+//     written at slot = (visible meshlets before it in (work item, lane) order).
+//     The reference appends with atomicAdd (vg_cull.wgsl:247), so its order is
+//     unspecified; this order is reproducible and first_instance = slot.
+
+#include "common.cuh"
+#include "kernels.h"
+#include "vg.h"
+
+namespace helio {
+
+namespace {
+
+// ── Scene preparation ─────────────────────────────────────────────────────────
+
+__global__ void pack_meshlets_kernel(const HelioGpuMeshletEntry* __restrict__ aos, uint32_t n,
+                                     float4* __restrict__ bounds, float4* __restrict__ cone,
+                                     float4* __restrict__ axis, uint4* __restrict__ draw) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float4* src = reinterpret_cast<const float4*>(aos + i);
+        bounds[i] = __ldcs(src + 0);
+        cone[i] = __ldcs(src + 1);
+        axis[i] = __ldcs(src + 2);
+        draw[i] = __ldcs(reinterpret_cast<const uint4*>(src + 3));
+    }
+}
+
+// InstanceCullData::from_instance (lib.rs:132-167), Rust f32 evaluation order.
+__global__ void instance_cull_data_kernel(const HelioGpuInstanceData* __restrict__ inst, uint32_t n,
+                                          HelioInstanceCullData* __restrict__ out) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        float m[16];
+        const float4* src = reinterpret_cast<const float4*>(inst[i].model);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            float4 q = __ldg(src + k);
+            m[4 * k + 0] = q.x;
+            m[4 * k + 1] = q.y;
+            m[4 * k + 2] = q.z;
+            m[4 * k + 3] = q.w;
+        }
+        const float sx = fsqrt(fadd(fadd(fmul(m[0], m[0]), fmul(m[1], m[1])), fmul(m[2], m[2])));
+        const float sy = fsqrt(fadd(fadd(fmul(m[4], m[4]), fmul(m[5], m[5])), fmul(m[6], m[6])));
+        const float sz = fsqrt(fadd(fadd(fmul(m[8], m[8]), fmul(m[9], m[9])), fmul(m[10], m[10])));
+        const float max_scale = fmaxf(fmaxf(sx, sy), sz);
+        const float min_scale = fminf(fminf(sx, sy), sz);
+        const float dot_xy = fadd(fadd(fmul(m[0], m[4]), fmul(m[1], m[5])), fmul(m[2], m[6]));
+        const float dot_xz = fadd(fadd(fmul(m[0], m[8]), fmul(m[1], m[9])), fmul(m[2], m[10]));
+        const float dot_yz = fadd(fadd(fmul(m[4], m[8]), fmul(m[5], m[9])), fmul(m[6], m[10]));
+        const float det = fadd(fsub(fmul(m[0], fsub(fmul(m[5], m[10]), fmul(m[6], m[9]))),
+                                    fmul(m[4], fsub(fmul(m[1], m[10]), fmul(m[2], m[9])))),
+                               fmul(m[8], fsub(fmul(m[1], m[6]), fmul(m[2], m[5]))));
+        const bool affine = fabsf(m[3]) <= 1.0e-6f && fabsf(m[7]) <= 1.0e-6f && fabsf(m[11]) <= 1.0e-6f &&
+                            fabsf(fsub(m[15], 1.0f)) <= 1.0e-4f;
+        bool finite = true;
+#pragma unroll
+        for (int k = 0; k < 16; ++k) finite = finite && isfinite(m[k]);
+        const bool valid = finite && isfinite(max_scale) && min_scale > 1.0e-8f && affine;
+        const float ut = fmul(max_scale, 1.0e-4f);
+        const float ot = fmul(fmul(max_scale, max_scale), 1.0e-4f);
+        const bool ap = fsub(max_scale, min_scale) <= ut && fabsf(dot_xy) <= ot && fabsf(dot_xz) <= ot &&
+                        fabsf(dot_yz) <= ot;
+        const bool cone = valid && ap && det > 0.0f;
+        HelioInstanceCullData r;
+        r.max_scale = valid ? max_scale : 0.0f;
+        r.min_scale = valid ? min_scale : 0.0f;
+        r.cone_cull_enabled = cone ? 1u : 0u;
+        r.valid_transform = valid ? 1u : 0u;
+        out[i] = r;
+    }
+}
+
+__device__ __forceinline__ HelioInstanceCullData load_cull(const HelioInstanceCullData* p) {
+    const uint4 q = __ldg(reinterpret_cast<const uint4*>(p));
+    HelioInstanceCullData r;
+    r.max_scale = __uint_as_float(q.x);
+    r.min_scale = __uint_as_float(q.y);
+    r.cone_cull_enabled = q.z;
+    r.valid_transform = q.w;
+    return r;
+}
+
+// ── Object select: cs_select_objects (vg_cull.wgsl:282-352) ───────────────────
+
+__global__ void __launch_bounds__(256) vg_select_kernel(VgSelectParams P) {
+    __shared__ Planes s_planes;
+    const HelioGpuCameraUniforms* cam = P.camera;
+    if (threadIdx.x == 0) s_planes = publish_planes(cam->view_proj);
+    __syncthreads();
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    const VgSceneDev& S = P.scene;
+    bool vis = false;
+    uint32_t selected = 0, lod_count = 0;
+    if (i < S.object_count) {
+        const HelioGpuVgObject* o = S.objects + i;
+        const uint4 head = __ldg(reinterpret_cast<const uint4*>(o));  // instance_index, lod_count, max_meshlet_count, reserved
+        lod_count = min(head.y, 8u);
+        const uint32_t ii = head.x;
+        uint32_t sel = 0;
+        if (lod_count > 0u && ii < S.instance_count) {
+            const HelioInstanceCullData cd = load_cull(S.cull + ii);
+            if (cd.valid_transform != 0u) {
+                const float4 lb = __ldg(reinterpret_cast<const float4*>(o->local_bounds));
+                const Mat4 model = ldg_mat4(S.instances[ii].model);
+                const F3 c = mat4_point3(model, f3(lb.x, lb.y, lb.z));
+                const float wr = fmaxf(fmul(lb.w, cd.max_scale), 0.0f);
+                if (sphere_visible_vg(s_planes, c, wr)) {
+                    const float4 pn = __ldg(reinterpret_cast<const float4*>(cam->position_near));
+                    const F3 d = sub3(c, f3(pn.x, pn.y, pn.z));
+                    const float dist = fsqrt(dot3(d, d));
+                    const float closest = fmaxf(fsub(dist, wr), fmaxf(pn.w, 1.0e-4f));
+                    const float focal = fmul(fmul(fabsf(__ldg(&cam->proj[5])), (float)P.screen_height), 0.5f);
+                    const float4 e0 = __ldg(reinterpret_cast<const float4*>(o->lod_errors));
+                    const float4 e1 = __ldg(reinterpret_cast<const float4*>(o->lod_errors + 4));
+                    const float err[8] = {e0.x, e0.y, e0.z, e0.w, e1.x, e1.y, e1.z, e1.w};
+                    uint32_t lod = 0;
+#pragma unroll
+                    for (uint32_t level = 1; level < 8; ++level) {
+                        if (level >= lod_count) break;
+                        const float px = fdiv(fmul(fmul(err[level], cd.max_scale), focal), closest);
+                        if (px <= P.lod_threshold_px) lod = level;
+                        else break;
+                    }
+                    selected = lod;
+                    sel = lod + 1;
+                    vis = true;
+                }
+            }
+        }
+        SelRecord rec = make_uint4(0u, 0u, ii, sel);
+        if (sel) {
+            rec.x = __ldg(&o->lod_first_meshlets[sel - 1]);
+            rec.y = __ldg(&o->lod_meshlet_counts[sel - 1]);
+        }
+        P.sel[i] = rec;
+        if (P.write_reserved) S.objects[i].reserved = sel;
+    }
+    if (P.counter_count >= 11u) {
+#pragma unroll
+        for (uint32_t l = 0; l < 8; ++l) {
+            const uint32_t n = __popc(__ballot_sync(0xffffffffu, vis && selected == l));
+            if (lane == 0 && n) atomicAdd(P.counters + 2 + l, n);
+        }
+        uint32_t mx = vis ? lod_count - 1u : 0u;
+        const bool any = __ballot_sync(0xffffffffu, vis) != 0u;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        if (lane == 0 && any) atomicMax(P.counters + 10, mx);
+    }
+}
+
+// ── Meshlet cull ──────────────────────────────────────────────────────────────
+
+struct CamState {
+    Mat4 vp;
+    float4 pos_near;
+    float p00, p11;
+};
+
+// cull_meshlet decision part (vg_cull.wgsl:143-240): true = emit a draw.
+__device__ __forceinline__ bool meshlet_visible(const VgSceneDev& S, const CamState& C, const Planes& pl,
+                                                const HizView& hz, uint32_t screen_h, uint32_t hiz_mip_count,
+                                                uint32_t mi, const Mat4& model, const HelioInstanceCullData& cd,
+                                                const HelioGpuInstanceData* inst) {
+    if (cd.valid_transform == 0u) return false;
+    const float4 b = __ldg(S.m_bounds + mi);
+    const F3 c = mat4_point3(model, f3(b.x, b.y, b.z));
+    const float wr = fmaxf(fmul(b.w, cd.max_scale), 0.0f);
+    const F3 cam = f3(C.pos_near.x, C.pos_near.y, C.pos_near.z);
+    const F3 ctc = sub3(c, cam);
+    if (!sphere_visible_vg(pl, c, wr)) return false;
+    // Perspective normal-cone test (:159-182).
+    if (cd.cone_cull_enabled != 0u) {
+        const float4 cone = __ldg(S.m_cone + mi);
+        const float cam_dist_sq = dot3(ctc, ctc);
+        const float guard = fmul(wr, 1.5f);
+        if (cam_dist_sq > fmul(guard, guard) && cone.w <= 1.0f) {
+            const float4 ax = __ldg(S.m_axis + mi);
+            const float4* nm = reinterpret_cast<const float4*>(inst->normal_mat);
+            const F3 a = mat3_vec(__ldg(nm), __ldg(nm + 1), __ldg(nm + 2), f3(ax.x, ax.y, ax.z));
+            const F3 axis_ws = divs3(a, fsqrt(dot3(a, a)));
+            const F3 apex = mat4_point3(model, f3(cone.x, cone.y, cone.z));
+            const F3 cta = sub3(apex, cam);
+            const float ads = dot3(cta, cta);
+            if (ads > 1.0e-12f && dot3(divs3(cta, fsqrt(ads)), axis_ws) >= cone.w) return false;
+        }
+    }
+    // Conservative Hi-Z test (:184-240).
+    const float4 clip = mat4_point4(C.vp, c);
+    if (clip.w > 0.0f) {
+        const float ndc_x = fdiv(clip.x, clip.w), ndc_y = fdiv(clip.y, clip.w);
+        const float uv_x = fadd(fmul(ndc_x, 0.5f), 0.5f), uv_y = fadd(fmul(ndc_y, -0.5f), 0.5f);
+        const float nvd = fsub(clip.w, wr);
+        if (nvd > C.pos_near.w) {
+            const float ndc_r = fmaxf(fabsf(fdiv(fmul(wr, C.p00), nvd)), fabsf(fdiv(fmul(wr, C.p11), nvd)));
+            const float uvr = fmul(ndc_r, 0.5f);
+            const float u0 = fsub(uv_x, uvr), v0 = fsub(uv_y, uvr), u1 = fadd(uv_x, uvr), v1 = fadd(uv_y, uvr);
+            if (u0 >= 0.0f && v0 >= 0.0f && u1 <= 1.0f && v1 <= 1.0f) {
+                const float dist_sq = dot3(ctc, ctc);
+                float near_z = 0.0f;
+                if (dist_sq > fmul(wr, wr)) {
+                    const F3 dir = divs3(ctc, fsqrt(dist_sq));
+                    const F3 nws = sub3(c, muls3(dir, wr));
+                    const float4 nc = mat4_point4(C.vp, nws);
+                    if (nc.w > 0.0f) near_z = clampf(fdiv(nc.z, nc.w), 0.0f, 1.0f);
+                }
+                const float half_h = fmul((float)screen_h, 0.5f);
+                const float dpx = fmaxf(fmul(fmul(ndc_r, half_h), 2.0f), 1.0f);
+                const uint32_t mip = min(ceil_log2_exact(dpx), hiz_mip_count - 1u);
+                const float h00 = hiz_sample(hz, u0, v0, mip);
+                const float h01 = hiz_sample(hz, u1, v0, mip);
+                const float h10 = hiz_sample(hz, u0, v1, mip);
+                const float h11 = hiz_sample(hz, u1, v1, mip);
+                const float hzv = fmaxf(fmaxf(h00, h01), fmaxf(h10, h11));
+                if (near_z > fadd(hzv, 1.0f / 65536.0f)) return false;
+            }
+        }
+    }
+    return true;
+}
+
+// Largest lane j whose exclusive offset is <= s (for s below the warp total this
+// is the item that owns window slot s; empty items are skipped because they share
+// their offset with the next item).
+__device__ __forceinline__ int owner_lane(uint32_t off, uint32_t s) {
+    int lo = 0;
+#pragma unroll
+    for (int step = 16; step > 0; step >>= 1) {
+        const uint32_t o = __shfl_sync(0xffffffffu, off, lo + step);
+        if (o <= s) lo += step;
+    }
+    return lo;
+}
+
+constexpr unsigned long long kFlagAgg = 1ull << 62;
+constexpr unsigned long long kFlagIncl = 2ull << 62;
+constexpr int kBitWordsPerWarp = 66;  // 64 windows of 32 slots (+2 so bit-field reads stay in bounds)
+
+// Decoupled look-back executed by one full warp; returns the exclusive prefix of
+// `tile` and publishes its inclusive value. Waits are bounded: after kSpinLimit
+// polls the error word is set and 0 is returned (outputs are then invalid and the
+// host reports HELIO_ERR_TIMEOUT).
+__device__ uint32_t warp_lookback(unsigned long long* lb, uint32_t tile, uint32_t agg, uint32_t* err) {
+    const int lane = threadIdx.x & 31;
+    if (tile == 0) {
+        if (lane == 0) atomicExch(lb, kFlagIncl | agg);
+        return 0u;
+    }
+    if (lane == 0) atomicExch(lb + tile, kFlagAgg | agg);
+    uint32_t prefix = 0;
+    long long base = (long long)tile - 1;
+    uint32_t polls = 0;
+    while (true) {
+        const long long idx = base - lane;
+        const unsigned long long v = idx >= 0 ? __ldcv(lb + idx) : kFlagIncl;
+        const uint32_t flag = (uint32_t)(v >> 62);
+        const uint32_t incl = __ballot_sync(0xffffffffu, flag == 2u);
+        const uint32_t notready = __ballot_sync(0xffffffffu, flag == 0u);
+        const int first_incl = incl ? __ffs(incl) - 1 : 32;
+        const uint32_t needed = first_incl >= 31 ? 0xffffffffu : ((2u << first_incl) - 1u);
+        if (notready & needed) {
+            if (++polls > kSpinLimit) {
+                // Give up: flag the error and unblock the successors with this
+                // tile's own count; the outputs of this launch are invalid.
+                if (lane == 0) {
+                    atomicExch(err, kDevTimeout);
+                    atomicExch(lb + tile, kFlagIncl | agg);
+                }
+                return 0u;
+            }
+            __nanosleep(polls < 64 ? 32 : 256);
+            continue;
+        }
+        uint32_t contrib = (lane <= first_incl) ? (uint32_t)v : 0u;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) contrib += __shfl_xor_sync(0xffffffffu, contrib, o);
+        prefix += contrib;
+        if (first_incl < 32) break;
+        base -= 32;
+    }
+    if (lane == 0) atomicExch(lb + tile, kFlagIncl | (unsigned long long)(prefix + agg));
+    return prefix;
+}
+
+__global__ void __launch_bounds__(kCullWarps * 32) vg_cull_kernel(VgCullParams P) {
+    __shared__ Planes s_planes;
+    __shared__ CamState s_cam;
+    __shared__ uint32_t s_tile;
+    __shared__ uint32_t s_warp_cnt[kCullWarps];
+    __shared__ uint32_t s_prefix;
+    __shared__ uint32_t s_bits[kCullWarps][kBitWordsPerWarp];
+    __shared__ HizView s_hiz;
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const VgSceneDev& S = P.scene;
+    if (tid == 0) {
+        s_tile = atomicAdd(P.scratch.tile_counter, 1u);  // tiles are processed in ticket order
+        const HelioGpuCameraUniforms* cam = P.camera;
+        s_planes = publish_planes(cam->view_proj);
+        s_cam.vp = ldg_mat4(cam->view_proj);
+        s_cam.pos_near = __ldg(reinterpret_cast<const float4*>(cam->position_near));
+        s_cam.p00 = __ldg(&cam->proj[0]);
+        s_cam.p11 = __ldg(&cam->proj[5]);
+        copy_hiz(P.hiz, s_hiz);
+    }
+    for (int k = lane; k < kBitWordsPerWarp; k += 32) s_bits[warp][k] = 0u;
+    __syncthreads();
+    const uint32_t tile = s_tile;
+    const CamState C = s_cam;
+
+    // Each lane owns one work item.
+    const uint32_t w_idx = tile * kCullItemsPerTile + warp * 32 + lane;
+    uint32_t n = 0, first = 0, inst = 0, lod = 0;
+    if (w_idx < S.work_item_count) {
+        const HelioGpuVgWorkItem it = S.items[w_idx];
+        if (it.object_index < S.object_count) {
+            const SelRecord r = __ldg(P.sel + it.object_index);
+            if (r.w != 0u && it.local_meshlet_base < r.y) {
+                n = min(64u, r.y - it.local_meshlet_base);
+                first = r.x + it.local_meshlet_base;
+                inst = r.z;
+                lod = r.w - 1u;
+            }
+        }
+    }
+    // Exclusive scan of the active meshlet counts over the warp's 32 items.
+    uint32_t incl = n;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    const uint32_t off = incl - n;
+    const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+
+    // Test windows of 32 packed slots.
+    uint32_t warp_count = 0;
+    const uint32_t windows = (total + 31u) >> 5;
+    for (uint32_t win = 0; win < windows; ++win) {
+        const uint32_t s = win * 32u + lane;
+        const int j = owner_lane(off, s);
+        const uint32_t j_off = __shfl_sync(0xffffffffu, off, j);
+        const uint32_t j_first = __shfl_sync(0xffffffffu, first, j);
+        const uint32_t j_inst = __shfl_sync(0xffffffffu, inst, j);
+        bool vis = false;
+        if (s < total) {
+            const uint32_t mi = j_first + (s - j_off);
+            if (mi < S.meshlet_count) {
+                const HelioGpuInstanceData* in = S.instances + j_inst;
+                const HelioInstanceCullData cd = load_cull(S.cull + j_inst);
+                const Mat4 model = ldg_mat4(in->model);
+                vis = meshlet_visible(S, C, s_planes, s_hiz, P.screen_height, P.hiz_mip_count, mi, model, cd, in);
+            }
+        }
+        const uint32_t bits = __ballot_sync(0xffffffffu, vis);
+        if (lane == 0) s_bits[warp][win] = bits;
+        warp_count += __popc(bits);
+    }
+    if (lane == 0) s_warp_cnt[warp] = warp_count;
+    __syncthreads();
+
+    // Tile aggregate and look-back.
+    if (warp == 0) {
+        uint32_t agg = 0;
+#pragma unroll
+        for (int w = 0; w < (int)kCullWarps; ++w) agg += s_warp_cnt[w];
+        const uint32_t prefix = warp_lookback(P.scratch.lookback, tile, agg, P.scratch.error_word);
+        if (lane == 0) {
+            s_prefix = prefix;
+            if (agg) {
+                atomicAdd(P.counters + 0, agg);
+                const unsigned long long end = (unsigned long long)prefix + agg;
+                const unsigned long long lo = prefix > P.capacity ? prefix : P.capacity;
+                if (end > lo) atomicAdd(P.counters + 1, (uint32_t)(end - lo));
+            }
+        }
+    }
+    __syncthreads();
+
+    // Emission in (work item, lane) order.
+    uint32_t base = s_prefix;
+    for (int w = 0; w < warp; ++w) base += s_warp_cnt[w];
+    for (uint32_t win = 0; win < windows; ++win) {
+        const uint32_t bits = s_bits[warp][win];
+        if (bits == 0u) continue;
+        const uint32_t s = win * 32u + lane;
+        const int j = owner_lane(off, s);
+        const uint32_t j_off = __shfl_sync(0xffffffffu, off, j);
+        const uint32_t j_first = __shfl_sync(0xffffffffu, first, j);
+        const uint32_t j_inst = __shfl_sync(0xffffffffu, inst, j);
+        const uint32_t j_lod = __shfl_sync(0xffffffffu, lod, j);
+        if ((bits >> lane) & 1u) {
+            const uint32_t slot = base + __popc(bits & ((1u << lane) - 1u));
+            if (slot < P.capacity) {
+                const uint32_t mi = j_first + (s - j_off);
+                const uint4 d = __ldg(S.m_draw + mi);
+                uint32_t* o = reinterpret_cast<uint32_t*>(P.indirect + slot);
+                o[0] = d.y;  // index_count
+                o[1] = 1u;
+                o[2] = d.x;  // first_index
+                o[3] = d.z;  // vertex_offset
+                o[4] = slot; // first_instance
+                reinterpret_cast<uint4*>(P.draws)[slot] = make_uint4(j_inst, mi, j_lod, 0u);
+            }
+        }
+        base += __popc(bits);
+    }
+
+    // Per-work-item visibility words: bits [off, off + n) of the warp's window bits.
+    if (P.visibility && w_idx < S.work_item_count) {
+        uint32_t lo = 0, hi = 0;
+        if (n) {
+            const uint32_t w0 = off >> 5, sh = off & 31u;
+            const unsigned long long a = (unsigned long long)s_bits[warp][w0] |
+                                         ((unsigned long long)s_bits[warp][w0 + 1] << 32);
+            const unsigned long long c = s_bits[warp][w0 + 2];
+            unsigned long long field = sh ? ((a >> sh) | (c << (64 - sh))) : a;
+            if (n < 64) field &= (1ull << n) - 1ull;
+            lo = (uint32_t)field;
+            hi = (uint32_t)(field >> 32);
+        }
+        reinterpret_cast<uint2*>(P.visibility)[w_idx] = make_uint2(lo, hi);
+    }
+}
+
+}  // namespace
+
+void launch_pack_meshlets(const HelioGpuMeshletEntry* aos, uint32_t n, float4* bounds, float4* cone, float4* axis,
+                          uint4* draw, cudaStream_t stream) {
+    if (!n) return;
+    uint32_t blocks = (n + 255u) / 256u;
+    if (blocks > 148u * 16u) blocks = 148u * 16u;
+    pack_meshlets_kernel<<<blocks, 256, 0, stream>>>(aos, n, bounds, cone, axis, draw);
+    helio_note_launch();
+}
+
+void launch_instance_cull_data(const HelioGpuInstanceData* inst, uint32_t n, HelioInstanceCullData* out,
+                               cudaStream_t stream) {
+    if (!n) return;
+    uint32_t blocks = (n + 255u) / 256u;
+    if (blocks > 148u * 16u) blocks = 148u * 16u;
+    instance_cull_data_kernel<<<blocks, 256, 0, stream>>>(inst, n, out);
+    helio_note_launch();
+}
+
+void launch_vg_select(const VgSelectParams& p, cudaStream_t stream) {
+    if (!p.scene.object_count) return;
+    vg_select_kernel<<<(p.scene.object_count + 255u) / 256u, 256, 0, stream>>>(p);
+    helio_note_launch();
+}
+
+void launch_vg_cull(const VgCullParams& p, cudaStream_t stream) {
+    if (!p.num_tiles) return;
+    vg_cull_kernel<<<p.num_tiles, kCullWarps * 32, 0, stream>>>(p);
+    helio_note_launch();
+}
+
+}  // namespace helio

@@ -1,0 +1,227 @@
+"""ctypes binding of ``include/helio_cull.h`` (the C-ABI of libhelio_cull.so).
+
+The structures mirror the libhelio byte layouts; their sizes are asserted at import.
+Loading fails loudly when the library is missing: there is no fallback path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+LIB_DIR = Path(__file__).resolve().parent / "lib"
+CULL_LIB = LIB_DIR / "libhelio_cull.so"
+SCENEGEN_LIB = LIB_DIR / "libhelio_scenegen.so"
+
+u32, i32, u64, f32 = C.c_uint32, C.c_int32, C.c_uint64, C.c_float
+vp = C.c_void_p
+
+HELIO_OK = 0
+HELIO_ERR_CUDA = 1
+HELIO_ERR_INVALID_ARG = 2
+HELIO_ERR_RESOURCE = 3
+HELIO_ERR_CAPACITY = 4
+HELIO_ERR_TIMEOUT = 5
+HELIO_ERR_BUDGET = 6
+HELIO_ERR_NOT_READY = 7
+HELIO_MEM_HOST = 0
+HELIO_MEM_DEVICE = 1
+HELIO_HIZ_MAX_MIPS = 12
+HELIO_HIZ_ALIAS_MIP0 = 1
+HELIO_VG_COUNTER_COUNT = 11
+HELIO_VG_DEFAULT_PUBLICATION_LIMIT = 262144
+HELIO_LOD_LOW, HELIO_LOD_MEDIUM, HELIO_LOD_HIGH, HELIO_LOD_ULTRA = 0, 1, 2, 3
+
+
+class GpuCameraUniforms(C.Structure):
+    _fields_ = [("view", f32 * 16), ("proj", f32 * 16), ("view_proj", f32 * 16), ("inv_view_proj", f32 * 16),
+                ("position_near", f32 * 4), ("forward_far", f32 * 4), ("jitter_frame", f32 * 4),
+                ("prev_view_proj", f32 * 16)]
+
+
+class GpuInstanceData(C.Structure):
+    _fields_ = [("model", f32 * 16), ("normal_mat", f32 * 12), ("bounds", f32 * 4), ("mesh_id", u32),
+                ("material_id", u32), ("flags", u32), ("lightmap_index", u32)]
+
+
+class GpuInstanceAabb(C.Structure):
+    _fields_ = [("min", f32 * 3), ("pad0", f32), ("max", f32 * 3), ("pad1", f32)]
+
+
+class GpuDrawCall(C.Structure):
+    _fields_ = [("index_count", u32), ("first_index", u32), ("vertex_offset", i32), ("first_instance", u32),
+                ("instance_count", u32)]
+
+
+class DrawIndexedIndirectArgs(C.Structure):
+    _fields_ = [("index_count", u32), ("instance_count", u32), ("first_index", u32), ("base_vertex", i32),
+                ("first_instance", u32)]
+
+
+class GpuMeshletEntry(C.Structure):
+    _fields_ = [("center", f32 * 3), ("radius", f32), ("cone_apex", f32 * 3), ("cone_cutoff", f32),
+                ("cone_axis", f32 * 3), ("lod_error", f32), ("first_index", u32), ("index_count", u32),
+                ("vertex_offset", i32), ("instance_index", u32)]
+
+
+class GpuVgObject(C.Structure):
+    _fields_ = [("instance_index", u32), ("lod_count", u32), ("max_meshlet_count", u32), ("reserved", u32),
+                ("local_bounds", f32 * 4), ("lod_errors", f32 * 8), ("lod_first_meshlets", u32 * 8),
+                ("lod_meshlet_counts", u32 * 8)]
+
+
+class GpuVgDraw(C.Structure):
+    _fields_ = [("instance_index", u32), ("meshlet_index", u32), ("lod_level", u32), ("reserved", u32)]
+
+
+class GpuVgWorkItem(C.Structure):
+    _fields_ = [("object_index", u32), ("local_meshlet_base", u32)]
+
+
+class InstanceCullData(C.Structure):
+    _fields_ = [("max_scale", f32), ("min_scale", f32), ("cone_cull_enabled", u32), ("valid_transform", u32)]
+
+
+class HizConfig(C.Structure):
+    _fields_ = [("width", u32), ("height", u32), ("flags", u32)]
+
+
+class HizPyramid(C.Structure):
+    _fields_ = [("mip_count", u32), ("width", u32 * 12), ("height", u32 * 12), ("pitch", u32 * 12),
+                ("levels", vp * 12)]
+
+
+class SceneBuffers(C.Structure):
+    _fields_ = [("camera", vp), ("instances", vp), ("instance_count", u32), ("draw_calls", vp),
+                ("draw_count", u32), ("aabbs", vp), ("indirect", vp)]
+
+
+class VgFrameData(C.Structure):
+    _fields_ = [("meshlets", vp), ("objects", vp), ("instances", vp), ("work_items", vp),
+                ("meshlet_count", u32), ("object_count", u32), ("work_item_count", u32), ("max_draw_count", u32),
+                ("buffer_version", u64), ("instance_version", u64), ("instance_dirty_start", u32),
+                ("instance_dirty_count", u32), ("memory", u32), ("reserved0", u32)]
+
+
+class VgConfig(C.Structure):
+    _fields_ = [("width", u32), ("height", u32), ("lod_quality", u32), ("publication_limit", u32),
+                ("counter_count", u32), ("flags", u32)]
+
+
+class VgOutputs(C.Structure):
+    _fields_ = [("indirect", vp), ("draws", vp), ("counters", vp), ("visibility", vp), ("objects", vp),
+                ("capacity", u32), ("counter_count", u32), ("work_item_count", u32), ("object_count", u32)]
+
+
+_SIZES = {GpuCameraUniforms: 368, GpuInstanceData: 144, GpuInstanceAabb: 32, GpuDrawCall: 20,
+          DrawIndexedIndirectArgs: 20, GpuMeshletEntry: 64, GpuVgObject: 128, GpuVgDraw: 16, GpuVgWorkItem: 8,
+          InstanceCullData: 16, VgFrameData: 80}
+for _t, _n in _SIZES.items():
+    assert C.sizeof(_t) == _n, (_t.__name__, C.sizeof(_t), _n)
+
+
+def np_dtype(struct_type) -> np.dtype:
+    """numpy structured dtype with the byte layout of a ctypes structure."""
+    return np.dtype(np.ctypeslib.as_ctypes_type(np.dtype(struct_type)))
+
+
+# Every exported entry point with its signature: (restype, argtypes).
+CULL_EXPORTS = {
+    "helio_abi_version": (i32, []),
+    "helio_last_error": (C.c_char_p, []),
+    "helio_status_string": (C.c_char_p, [i32]),
+    "helio_kernel_launch_count": (u64, []),
+    "helio_mip_levels": (u32, [u32, u32]),
+    "helio_extract_frustum_planes": (None, [vp, vp]),
+    "helio_instance_cull_data": (i32, [vp, u32, vp, vp]),
+    "helio_hiz_create": (i32, [C.POINTER(HizConfig), C.POINTER(vp)]),
+    "helio_hiz_prepare": (i32, [vp, vp, u32, u64]),
+    "helio_hiz_execute": (i32, [vp, vp]),
+    "helio_hiz_resize": (i32, [vp, u32, u32]),
+    "helio_hiz_publish": (i32, [vp, C.POINTER(HizPyramid)]),
+    "helio_hiz_destroy": (None, [vp]),
+    "helio_indirect_dispatch_create": (i32, [vp, C.POINTER(vp)]),
+    "helio_indirect_dispatch_prepare": (i32, [vp, C.POINTER(GpuCameraUniforms), u32]),
+    "helio_indirect_dispatch_execute": (i32, [vp, C.POINTER(SceneBuffers), vp]),
+    "helio_indirect_dispatch_destroy": (None, [vp]),
+    "helio_occlusion_cull_create": (i32, [u32, u32, vp, C.POINTER(vp)]),
+    "helio_occlusion_cull_prepare": (i32, [vp, u32]),
+    "helio_occlusion_cull_execute": (i32, [vp, C.POINTER(SceneBuffers), C.POINTER(HizPyramid), u64, vp]),
+    "helio_occlusion_cull_resize": (i32, [vp, u32, u32]),
+    "helio_occlusion_cull_destroy": (None, [vp]),
+    "helio_instance_cull_fused_execute": (i32, [vp, vp, C.POINTER(SceneBuffers), C.POINTER(HizPyramid), u64, vp]),
+    "helio_lod_max_error_pixels": (f32, [u32]),
+    "helio_vg_create": (i32, [C.POINTER(VgConfig), C.POINTER(vp)]),
+    "helio_vg_prepare": (i32, [vp, C.POINTER(VgFrameData), vp]),
+    "helio_vg_execute": (i32, [vp, vp, C.POINTER(HizPyramid), vp]),
+    "helio_vg_resize": (i32, [vp, u32, u32]),
+    "helio_vg_set_lod_quality": (i32, [vp, u32]),
+    "helio_vg_publish": (i32, [vp, C.POINTER(VgOutputs)]),
+    "helio_vg_device_status": (i32, [vp, vp]),
+    "helio_vg_destroy": (None, [vp]),
+}
+
+_cull = None
+_scenegen = None
+
+
+class HelioError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"helio status {status}: {message}")
+        self.status = status
+
+
+def cull_lib() -> C.CDLL:
+    """The CUDA library; raises if it was not built (no CPU fallback exists)."""
+    global _cull
+    if _cull is None:
+        if not CULL_LIB.exists():
+            raise FileNotFoundError(f"{CULL_LIB} missing: run `python -m helio_b200.build`")
+        lib = C.CDLL(str(CULL_LIB))
+        for name, (res, args) in CULL_EXPORTS.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _cull = lib
+    return _cull
+
+
+def check(status: int) -> None:
+    if status != HELIO_OK:
+        msg = cull_lib().helio_last_error()
+        raise HelioError(status, msg.decode() if msg else "")
+
+
+class SceneParams(C.Structure):
+    _fields_ = [("seed", u64), ("instance_count", u32), ("lod0_meshlets", u32), ("lod_count", u32),
+                ("placement", u32), ("cube_half", f32), ("blob_count", u32), ("blob_sigma", f32),
+                ("lod_error_mode", u32), ("coverage_height_px", f32), ("coverage_tau_px", f32),
+                ("mesh_library", u32), ("threads", u32), ("scale_min", f32), ("scale_max", f32)]
+
+
+class SceneCounts(C.Structure):
+    _fields_ = [("meshlets", u64), ("objects", u64), ("work_items", u64), ("max_draw_count", u64),
+                ("mesh_count", u64), ("meshlets_per_mesh", u64)]
+
+
+def scenegen_lib() -> C.CDLL:
+    global _scenegen
+    if _scenegen is None:
+        if not SCENEGEN_LIB.exists():
+            raise FileNotFoundError(f"{SCENEGEN_LIB} missing: run `python -m helio_b200.build`")
+        lib = C.CDLL(str(SCENEGEN_LIB))
+        lib.sg_scene_counts_fn.argtypes = [C.POINTER(SceneParams), C.POINTER(SceneCounts)]
+        lib.sg_scene_counts_fn.restype = i32
+        lib.sg_scene_generate.argtypes = [C.POINTER(SceneParams), vp, vp, vp, vp, vp, vp]
+        lib.sg_scene_generate.restype = i32
+        d3 = C.POINTER(C.c_double)
+        lib.sg_camera_perspective.argtypes = [d3, d3, d3, C.c_double, C.c_double, C.c_double, C.c_double,
+                                              C.POINTER(GpuCameraUniforms)]
+        lib.sg_camera_perspective.restype = None
+        lib.sg_camera_ortho.argtypes = [d3, d3, d3] + [C.c_double] * 6 + [C.POINTER(GpuCameraUniforms)]
+        lib.sg_camera_ortho.restype = None
+        lib.sg_depth.argtypes = [u64, u32, u32, u32, u32, f32, f32, f32, u32, vp, u32]
+        lib.sg_depth.restype = i32
+        _scenegen = lib
+    return _scenegen

@@ -1,0 +1,227 @@
+"""Python mirror of the reference passes, over the C-ABI of libhelio_cull.so.
+
+Each class follows the reference ``RenderPass`` lifecycle (crates/helio-core/src/
+traits.rs:276-470): ``prepare`` → ``execute`` → ``publish``, with ``on_resize``.
+Device memory and streams come from PyTorch (plumbing only); every kernel is in the
+native library, and a missing library raises instead of falling back.
+
+  HiZBuildPass           crates/helio-pass-hiz/src/lib.rs:381-548
+  IndirectDispatchPass   crates/helio-pass-indirect-dispatch/src/lib.rs:164-258
+  OcclusionCullPass      crates/helio-pass-occlusion-cull/src/lib.rs:279-411
+  VirtualGeometryPass    crates/helio-pass-virtual-geometry/src/rendering.rs:703-1165 (cull half)
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import native as N
+
+UINT64_MAX = (1 << 64) - 1
+
+
+class _CudaArray:
+    """Zero-copy __cuda_array_interface__ view of library-owned device memory."""
+
+    def __init__(self, ptr: int, shape, typestr: str, strides=None):
+        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": typestr, "data": (int(ptr), False),
+                                         "version": 2, "strides": strides}
+
+
+def device_view(ptr: int, shape, dtype: str = "<i4", strides=None) -> torch.Tensor:
+    """torch tensor aliasing `ptr` (int32 words by default)."""
+    if not ptr:
+        raise N.HelioError(N.HELIO_ERR_RESOURCE, "null device pointer")
+    return torch.as_tensor(_CudaArray(ptr, shape, dtype, strides), device="cuda")
+
+
+def _stream_ptr(stream) -> C.c_void_p:
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    return C.c_void_p(stream.cuda_stream)
+
+
+def _ptr(t) -> C.c_void_p:
+    if t is None:
+        return C.c_void_p(0)
+    if isinstance(t, torch.Tensor):
+        return C.c_void_p(t.data_ptr())
+    if isinstance(t, np.ndarray):
+        return C.c_void_p(t.ctypes.data)
+    return C.c_void_p(int(t))
+
+
+def camera_bytes(cam: N.GpuCameraUniforms) -> np.ndarray:
+    return np.frombuffer(bytes(cam), dtype=np.uint8).copy()
+
+
+class HiZBuildPass:
+    """Hi-Z pyramid (max reduction, standard Z) built by one fused launch."""
+
+    def __init__(self, width: int, height: int, alias_mip0: bool = False):
+        self._lib = N.cull_lib()
+        cfg = N.HizConfig(width, height, N.HELIO_HIZ_ALIAS_MIP0 if alias_mip0 else 0)
+        h = C.c_void_p()
+        N.check(self._lib.helio_hiz_create(C.byref(cfg), C.byref(h)))
+        self._h = h
+        self.width, self.height = width, height
+        self._depth = None
+
+    def name(self) -> str:
+        return "HiZBuild"
+
+    def prepare(self, depth: torch.Tensor, camera_generation: int = UINT64_MAX) -> None:
+        assert depth.is_cuda and depth.dtype == torch.float32 and depth.dim() == 2
+        assert depth.stride(1) == 1 and depth.shape[0] == self.height and depth.shape[1] == self.width
+        self._depth = depth  # keep alive while the pyramid may alias it
+        N.check(self._lib.helio_hiz_prepare(self._h, _ptr(depth), depth.stride(0), camera_generation))
+
+    def execute(self, stream=None) -> None:
+        N.check(self._lib.helio_hiz_execute(self._h, _stream_ptr(stream)))
+
+    def on_resize(self, width: int, height: int) -> None:
+        N.check(self._lib.helio_hiz_resize(self._h, width, height))
+        self.width, self.height = width, height
+
+    def publish(self) -> N.HizPyramid:
+        pyr = N.HizPyramid()
+        N.check(self._lib.helio_hiz_publish(self._h, C.byref(pyr)))
+        return pyr
+
+    def level(self, l: int) -> torch.Tensor:
+        pyr = self.publish()
+        w, h, p = pyr.width[l], pyr.height[l], pyr.pitch[l]
+        return device_view(pyr.levels[l], (h, w), "<f4", (p * 4, 4))
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            self._lib.helio_hiz_destroy(h)
+            self._h = None
+
+
+def scene_buffers(camera_dev, instances, draw_calls, aabbs, indirect) -> N.SceneBuffers:
+    return N.SceneBuffers(_ptr(camera_dev), _ptr(instances), instances.shape[0] if instances is not None else 0,
+                          _ptr(draw_calls), draw_calls.shape[0], _ptr(aabbs), _ptr(indirect))
+
+
+class IndirectDispatchPass:
+    """Per-draw frustum + sub-pixel cull writing DrawIndexedIndirect (non-compacting)."""
+
+    def __init__(self, stats: torch.Tensor):
+        self._lib = N.cull_lib()
+        assert stats.is_cuda and stats.numel() >= 8
+        self.stats = stats
+        h = C.c_void_p()
+        N.check(self._lib.helio_indirect_dispatch_create(_ptr(stats), C.byref(h)))
+        self._h = h
+
+    def name(self) -> str:
+        return "IndirectDispatch"
+
+    def prepare(self, camera: N.GpuCameraUniforms, draw_count: int) -> None:
+        N.check(self._lib.helio_indirect_dispatch_prepare(self._h, C.byref(camera), draw_count))
+
+    def execute(self, scene: N.SceneBuffers, stream=None) -> None:
+        N.check(self._lib.helio_indirect_dispatch_execute(self._h, C.byref(scene), _stream_ptr(stream)))
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            self._lib.helio_indirect_dispatch_destroy(h)
+            self._h = None
+
+
+class OcclusionCullPass:
+    """Per-draw Hi-Z occlusion test against the (previous frame's) pyramid."""
+
+    def __init__(self, width: int, height: int, stats: torch.Tensor):
+        self._lib = N.cull_lib()
+        self.stats = stats
+        h = C.c_void_p()
+        N.check(self._lib.helio_occlusion_cull_create(width, height, _ptr(stats), C.byref(h)))
+        self._h = h
+
+    def name(self) -> str:
+        return "OcclusionCull"
+
+    def prepare(self, draw_count: int) -> None:
+        N.check(self._lib.helio_occlusion_cull_prepare(self._h, draw_count))
+
+    def execute(self, scene: N.SceneBuffers, hiz: N.HizPyramid, frame_num: int, stream=None) -> None:
+        N.check(self._lib.helio_occlusion_cull_execute(self._h, C.byref(scene), C.byref(hiz), frame_num,
+                                                       _stream_ptr(stream)))
+
+    def on_resize(self, width: int, height: int) -> None:
+        N.check(self._lib.helio_occlusion_cull_resize(self._h, width, height))
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            self._lib.helio_occlusion_cull_destroy(h)
+            self._h = None
+
+
+def fused_instance_cull(frustum: IndirectDispatchPass, occlusion: OcclusionCullPass, scene: N.SceneBuffers,
+                        hiz: N.HizPyramid, frame_num: int, stream=None) -> None:
+    lib = N.cull_lib()
+    N.check(lib.helio_instance_cull_fused_execute(frustum._h, occlusion._h, C.byref(scene), C.byref(hiz), frame_num,
+                                                  _stream_ptr(stream)))
+
+
+class VirtualGeometryPass:
+    """Virtual-geometry cull: object LOD select + meshlet cull + deterministic compaction."""
+
+    def __init__(self, width: int, height: int, lod_quality: int = N.HELIO_LOD_MEDIUM, publication_limit: int = 0,
+                 counter_count: int = 11):
+        self._lib = N.cull_lib()
+        cfg = N.VgConfig(width, height, lod_quality, publication_limit, counter_count, 0)
+        h = C.c_void_p()
+        N.check(self._lib.helio_vg_create(C.byref(cfg), C.byref(h)))
+        self._h = h
+        self.width, self.height = width, height
+
+    def name(self) -> str:
+        return "VirtualGeometry"
+
+    def prepare(self, frame: N.VgFrameData, stream=None) -> None:
+        N.check(self._lib.helio_vg_prepare(self._h, C.byref(frame), _stream_ptr(stream)))
+
+    def execute(self, camera_dev: torch.Tensor, hiz: N.HizPyramid, stream=None) -> None:
+        N.check(self._lib.helio_vg_execute(self._h, _ptr(camera_dev), C.byref(hiz), _stream_ptr(stream)))
+
+    def on_resize(self, width: int, height: int) -> None:
+        N.check(self._lib.helio_vg_resize(self._h, width, height))
+        self.width, self.height = width, height
+
+    def set_lod_quality(self, q: int) -> None:
+        N.check(self._lib.helio_vg_set_lod_quality(self._h, q))
+
+    def publish(self) -> N.VgOutputs:
+        out = N.VgOutputs()
+        N.check(self._lib.helio_vg_publish(self._h, C.byref(out)))
+        return out
+
+    def device_status(self, stream=None) -> None:
+        N.check(self._lib.helio_vg_device_status(self._h, _stream_ptr(stream)))
+
+    def outputs(self) -> dict:
+        """Zero-copy torch views of the published buffers (int32 words)."""
+        o = self.publish()
+        cap = max(o.capacity, 1)
+        return {
+            "indirect": device_view(o.indirect, (cap, 5)),
+            "draws": device_view(o.draws, (cap, 4)),
+            "counters": device_view(o.counters, (o.counter_count,)),
+            "visibility": device_view(o.visibility, (max(o.work_item_count, 1), 2)),
+            "objects": device_view(o.objects, (max(o.object_count, 1), 32)),
+            "capacity": o.capacity,
+        }
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            self._lib.helio_vg_destroy(h)
+            self._h = None

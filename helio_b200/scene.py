@@ -1,0 +1,235 @@
+"""Seeded synthetic workloads of the visibility path (numpy arrays in libhelio layouts).
+
+Scenes, cameras and depth come from libhelio_scenegen.so (deterministic for a given
+seed, independent of the thread count). The workloads:
+
+  0  plain single view: 4,096 instances x 64 LOD0 meshlets (LOD k = ceil(64 / 2^k), 4 levels),
+     200 m cube, LOD errors from coverage thresholds 0.25/0.06/0.015; 1024x1024 depth,
+     256 occluder rectangles, perspective fov 60 deg, aspect 1, near 0.1, far 1000.
+  1  10,000 x 100 meshlets (1M), LOD errors log-uniform in [1e-4, 1e-1]; 1920x1080, 2,000 rectangles.
+  2  100,000 x 100 (10M), 64 Gaussian blobs (sigma 20 m) in a 2 km cube; 3840x2160, 20,000 rectangles.
+  3  200,000 x 50 (10M), distributions of 2; 85 views (1 main 3840x2160, 4 orthographic cascades
+     2048^2, 16 spot 512^2, 64 probe 128^2), occluder count proportional to pixel count.
+  4  8 scenes, instance counts log-uniform in [10k, 2M] x 100 meshlets sharing a library of
+     4,096 meshes per scene; requests carry 1..85 views of the configuration-3 mix.
+
+Occluder rectangles: side ~ U[W/64, W/4] scaled so every view keeps configuration 0's
+expected coverage; linear depth t ~ U[0, 1] of the near..far range stored as NDC depth.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import native as N
+
+SEED_BASE = 0x48454C494F00
+DT_MESHLET = np.dtype(N.GpuMeshletEntry)
+DT_OBJECT = np.dtype(N.GpuVgObject)
+DT_INSTANCE = np.dtype(N.GpuInstanceData)
+DT_ITEM = np.dtype(N.GpuVgWorkItem)
+DT_AABB = np.dtype(N.GpuInstanceAabb)
+DT_DRAWCALL = np.dtype(N.GpuDrawCall)
+
+
+@dataclass
+class Scene:
+    meshlets: np.ndarray
+    objects: np.ndarray
+    instances: np.ndarray
+    work_items: np.ndarray
+    aabbs: np.ndarray
+    draw_calls: np.ndarray
+    max_draw_count: int
+    lod0_meshlets: int  # LOD0 meshlets per instance (unit of the meshlets/s metric)
+
+    @property
+    def lod0_total(self) -> int:
+        return self.lod0_meshlets * len(self.objects)
+
+    def device_bytes(self) -> int:
+        return (self.meshlets.nbytes + self.objects.nbytes + self.instances.nbytes + self.work_items.nbytes
+                + len(self.objects) * 16 + len(self.objects) * 16 + self.work_items.nbytes)
+
+
+@dataclass
+class View:
+    camera: N.GpuCameraUniforms
+    width: int
+    height: int
+    depth: np.ndarray  # (height, width) float32
+    kind: str = "perspective"
+    lod_threshold_px: float = 2.0
+
+
+@dataclass
+class Workload:
+    config_id: int
+    scene: Scene
+    views: list = field(default_factory=list)
+
+
+def _threads() -> int:
+    return max(1, min(32, os.cpu_count() or 1))
+
+
+def make_scene(seed: int, instances: int, lod0: int, lod_count: int = 4, placement: int = 0, cube_half: float = 100.0,
+               blobs: int = 0, sigma: float = 0.0, lod_error_mode: int = 1, coverage_height: float = 1024.0,
+               mesh_library: int = 0, threads: int | None = None) -> Scene:
+    lib = N.scenegen_lib()
+    p = N.SceneParams(seed, instances, lod0, lod_count, placement, cube_half, blobs, sigma, lod_error_mode,
+                      coverage_height, 2.0, mesh_library, threads or _threads(), 0.5, 4.0)
+    cnt = N.SceneCounts()
+    N.check(lib.sg_scene_counts_fn(C.byref(p), C.byref(cnt)))
+    meshlets = np.zeros(cnt.meshlets, DT_MESHLET)
+    objects = np.zeros(cnt.objects, DT_OBJECT)
+    inst = np.zeros(cnt.objects, DT_INSTANCE)
+    items = np.zeros(cnt.work_items, DT_ITEM)
+    aabbs = np.zeros(cnt.objects, DT_AABB)
+    draws = np.zeros(cnt.objects, DT_DRAWCALL)
+    N.check(lib.sg_scene_generate(C.byref(p), meshlets.ctypes.data, objects.ctypes.data, inst.ctypes.data,
+                                  items.ctypes.data, aabbs.ctypes.data, draws.ctypes.data))
+    return Scene(meshlets, objects, inst, items, aabbs, draws, int(cnt.max_draw_count), lod0)
+
+
+def _d3(v):
+    return (C.c_double * 3)(*[float(x) for x in v])
+
+
+def perspective(eye, target, up, fov_y_deg, aspect, near=0.1, far=1000.0) -> N.GpuCameraUniforms:
+    cam = N.GpuCameraUniforms()
+    N.scenegen_lib().sg_camera_perspective(_d3(eye), _d3(target), _d3(up), math.radians(fov_y_deg), aspect, near,
+                                           far, C.byref(cam))
+    return cam
+
+
+def orthographic(eye, target, up, half, near, far) -> N.GpuCameraUniforms:
+    cam = N.GpuCameraUniforms()
+    N.scenegen_lib().sg_camera_ortho(_d3(eye), _d3(target), _d3(up), -half, half, -half, half, near, far,
+                                     C.byref(cam))
+    return cam
+
+
+def make_depth(seed: int, width: int, height: int, n_rects: int, near: float, far: float, ortho: bool,
+               pitch: int | None = None, threads: int | None = None) -> np.ndarray:
+    pitch = pitch or width
+    out = np.empty((height, pitch), np.float32)
+    side = math.sqrt((256.0 / max(n_rects, 1)) * (width * height) / (1024.0 * 1024.0))
+    N.check(N.scenegen_lib().sg_depth(seed, width, height, pitch, n_rects, side, near, far, 1 if ortho else 0,
+                                      out.ctypes.data, threads or _threads()))
+    return out[:, :width] if pitch != width else out
+
+
+class _Split:
+    """splitmix64 uniform stream for view parameters."""
+
+    def __init__(self, seed: int):
+        self.x = seed & 0xFFFFFFFFFFFFFFFF
+
+    def u(self, a=0.0, b=1.0) -> float:
+        self.x = (self.x + 0x9E3779B97F4A7C15) & 0xFFFFFFFFFFFFFFFF
+        z = self.x
+        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & 0xFFFFFFFFFFFFFFFF
+        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & 0xFFFFFFFFFFFFFFFF
+        z ^= z >> 31
+        return a + (b - a) * ((z >> 11) / float(1 << 53))
+
+
+def main_view(seed: int, width: int, height: int, n_rects: int) -> View:
+    cam = perspective((0, 0, 0), (0, 0, -1), (0, 1, 0), 60.0, width / height)
+    depth = make_depth(seed, width, height, n_rects, 0.1, 1000.0, False)
+    return View(cam, width, height, depth)
+
+
+def multiview_set(seed: int, depth: bool = True, scale: float = 1.0) -> list:
+    """The 85-view mix: main 3840x2160, 4 orthographic cascades 2048^2, 16 spot 512^2, 64 probes 128^2.
+    `scale` shrinks every view size (tests); occluder counts stay proportional to pixels."""
+    rng = _Split(seed ^ 0x5EED)
+    views = []
+
+    def n_rects(w, h):
+        return max(1, int(round(20000 * (w * h) / (3840 * 2160))))
+
+    def add(cam, w, h, kind, idx, ortho=False):
+        w, h = max(1, int(w * scale)), max(1, int(h * scale))
+        d = make_depth(seed + 1000 + idx, w, h, n_rects(w, h), cam.position_near[3], cam.forward_far[3], ortho) \
+            if depth else np.ones((h, w), np.float32)
+        views.append(View(cam, w, h, d, kind))
+
+    add(perspective((0, 0, 0), (0, 0, -1), (0, 1, 0), 60.0, 16 / 9), 3840, 2160, "main", 0)
+    light = np.array([-0.3, -1.0, -0.2])
+    light /= np.linalg.norm(light)
+    t30 = math.tan(math.radians(30.0))
+    for i, (n, f) in enumerate([(0.0, 8.0), (8.0, 32.0), (32.0, 128.0), (128.0, 512.0)]):
+        hh, hw = f * t30, f * t30 * 16 / 9
+        r = math.sqrt(hw * hw + hh * hh + ((f - n) / 2) ** 2)
+        center = np.array([0.0, 0.0, -(n + f) / 2])
+        eye = center - light * (r + 600.0)
+        add(orthographic(eye, center, (0, 0, 1), r, 0.1, 2 * r + 1200.0), 2048, 2048, "cascade", 1 + i, ortho=True)
+    for i in range(16):
+        pos = [rng.u(-150, 150) for _ in range(3)]
+        z = rng.u(-1, 1)
+        phi = rng.u(0, 2 * math.pi)
+        s = math.sqrt(max(0.0, 1 - z * z))
+        d = (s * math.cos(phi), s * math.sin(phi), z)
+        up = (0, 1, 0) if abs(d[1]) < 0.95 else (1, 0, 0)
+        fov = rng.u(30.0, 90.0)
+        add(perspective(pos, [pos[k] + d[k] for k in range(3)], up, fov, 1.0, 0.1, 500.0), 512, 512, "spot", 5 + i)
+    dirs = [(1, 0, 0), (-1, 0, 0), (0, 1, 0), (0, -1, 0), (0, 0, 1), (0, 0, -1)]
+    k = 0
+    for ix in range(4):
+        for iy in range(4):
+            for iz in range(4):
+                pos = (-150 + 100 * ix, -150 + 100 * iy, -150 + 100 * iz)
+                d = dirs[k % 6]
+                up = (0, 0, 1) if d[1] != 0 else (0, 1, 0)
+                add(perspective(pos, [pos[j] + d[j] for j in range(3)], up, 90.0, 1.0, 0.1, 500.0), 128, 128,
+                    "probe", 21 + k)
+                k += 1
+    return views
+
+
+def config(config_id: int, scale: float = 1.0, with_depth: bool = True, threads: int | None = None) -> Workload:
+    """Builds workload `config_id` (0..3). `scale` (<= 1) shrinks instance counts and view
+    sizes for quick tests while keeping every distribution."""
+    seed = SEED_BASE + config_id
+
+    def cnt(n):
+        return max(1, int(round(n * scale)))
+
+    if config_id == 0:
+        sc = make_scene(seed, cnt(4096), 64, 4, 0, 100.0, lod_error_mode=0, coverage_height=1024.0 * scale,
+                        threads=threads)
+        w = max(8, int(1024 * scale))
+        return Workload(0, sc, [main_view(seed, w, w, 256)])
+    if config_id == 1:
+        sc = make_scene(seed, cnt(10000), 100, 4, 0, 100.0, lod_error_mode=1, threads=threads)
+        w, h = max(16, int(1920 * scale)), max(9, int(1080 * scale))
+        return Workload(1, sc, [main_view(seed, w, h, max(1, int(2000 * scale)))])
+    if config_id == 2:
+        sc = make_scene(seed, cnt(100000), 100, 4, 1, 1000.0, 64, 20.0, lod_error_mode=1, threads=threads)
+        w, h = max(16, int(3840 * scale)), max(9, int(2160 * scale))
+        return Workload(2, sc, [main_view(seed, w, h, max(1, int(20000 * scale)))])
+    if config_id == 3:
+        sc = make_scene(seed, cnt(200000), 50, 4, 1, 1000.0, 64, 20.0, lod_error_mode=1, threads=threads)
+        return Workload(3, sc, multiview_set(seed, with_depth, scale))
+    raise ValueError(f"unknown config {config_id}")
+
+
+def frame_data(scene: Scene, buffer_version: int = 1, instance_version: int = 1, dirty=(0, 0),
+               device: dict | None = None) -> N.VgFrameData:
+    """VgFrameData over host arrays (or device tensors when `device` holds them)."""
+    src = device or {"meshlets": scene.meshlets, "objects": scene.objects, "instances": scene.instances,
+                     "work_items": scene.work_items}
+
+    def p(a):
+        return a.data_ptr() if hasattr(a, "data_ptr") else a.ctypes.data
+
+    return N.VgFrameData(p(src["meshlets"]), p(src["objects"]), p(src["instances"]), p(src["work_items"]),
+                         len(scene.meshlets), len(scene.objects), len(scene.work_items),
+                         min(scene.max_draw_count, 0xFFFFFFFF), buffer_version, instance_version, dirty[0], dirty[1],
+                         N.HELIO_MEM_DEVICE if device else N.HELIO_MEM_HOST, 0)

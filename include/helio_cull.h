@@ -1,0 +1,380 @@
+/*
+ * helio_cull.h — C-ABI of the B200 (sm_100a) GPU visibility path:
+ *   Hi-Z pyramid → instance frustum / Hi-Z occlusion cull → virtual-geometry
+ *   object LOD select + meshlet frustum / normal-cone / Hi-Z cull →
+ *   deterministic draw-argument compaction.
+ *
+ * Each reference RenderPass (crates/helio-core/src/traits.rs:276-470) becomes one
+ * opaque context with the same lifecycle:
+ *     create  (RenderPass::new)
+ *     prepare (RenderPass::prepare, PrepareContext: uploads, uniforms)
+ *     execute (RenderPass::execute, PassContext: GPU work on one stream)
+ *     resize  (RenderPass::on_resize)
+ *     publish (RenderPass::publish: device pointers of the outputs)
+ *     destroy
+ * Byte layouts of every buffer are libhelio's (crates/libhelio/src/*.rs) and are
+ * asserted by static_assert in the library.
+ *
+ * Conventions
+ *   - Every entry point returns an int32_t status (HELIO_OK on success). No
+ *     exception or abort crosses this boundary; helio_last_error() returns the
+ *     message of the calling thread's last failure.
+ *   - `stream` arguments are cudaStream_t passed as void* (NULL = legacy stream).
+ *   - Pointers documented "device" are CUDA device pointers owned by the caller
+ *     and borrowed for the duration of the call's GPU work. Pointers returned by
+ *     *_publish stay owned by the context and remain valid until the next
+ *     prepare/resize/destroy of that context.
+ *   - A context is externally synchronised: one thread and one stream at a time
+ *     (reference: RenderPass is Send + Sync and driven by one thread per frame,
+ *     crates/helio-core/src/graph/execution.rs:343-606). Distinct contexts may
+ *     run concurrently on distinct streams.
+ *   - execute() never allocates device memory (reference rule for the hot path,
+ *     crates/helio-core/src/traits.rs:164-166); buffers grow in prepare().
+ *   - Arithmetic is IEEE-754 binary32 without contraction (no FMA), with
+ *     correctly-rounded division and square root, in the WGSL operation order
+ *     of the reference shaders, so decisions are bit-reproducible.
+ */
+#ifndef HELIO_CULL_H
+#define HELIO_CULL_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HELIO_ABI_VERSION 1
+
+/* ── Status codes (reference: helio_core::Error, crates/helio-core/src/error.rs:62-167) ── */
+#define HELIO_OK 0
+#define HELIO_ERR_CUDA 1          /* a CUDA runtime call failed (Error::Gpu)                 */
+#define HELIO_ERR_INVALID_ARG 2   /* bad pointer / size / config (Error::InvalidPassConfig)   */
+#define HELIO_ERR_RESOURCE 3      /* missing input: no Hi-Z, no scene (Error::ResourceNotFound) */
+#define HELIO_ERR_CAPACITY 4      /* soft: visible draws exceeded capacity; counters valid    */
+#define HELIO_ERR_TIMEOUT 5       /* a bounded device-side wait gave up; outputs invalid      */
+#define HELIO_ERR_BUDGET 6        /* admission refused: device-memory budget exceeded         */
+#define HELIO_ERR_NOT_READY 7     /* nothing to return yet (serving poll)                     */
+
+/* Memory space of caller-provided input arrays. */
+#define HELIO_MEM_HOST 0u
+#define HELIO_MEM_DEVICE 1u
+
+/* ════════════════════════════════════════════════════════════════════════════
+ * libhelio byte layouts (all little-endian, 4-byte aligned, tightly packed)
+ * ════════════════════════════════════════════════════════════════════════════ */
+
+/* GpuCameraUniforms, crates/libhelio/src/camera.rs:10-57. 368 bytes.
+ * Matrices are column-major: m[c*4 + r]. view_proj = proj * view. */
+typedef struct HelioGpuCameraUniforms {
+    float view[16];
+    float proj[16];
+    float view_proj[16];
+    float inv_view_proj[16];
+    float position_near[4]; /* xyz = camera position, w = near plane */
+    float forward_far[4];   /* xyz = forward, w = far plane */
+    float jitter_frame[4];
+    float prev_view_proj[16];
+} HelioGpuCameraUniforms;
+
+/* GpuInstanceData, crates/libhelio/src/instance.rs:28-45. 144 bytes. */
+typedef struct HelioGpuInstanceData {
+    float model[16];      /* column-major model matrix */
+    float normal_mat[12]; /* three vec4 columns of the normal matrix (w unused) */
+    float bounds[4];      /* world-space sphere: xyz centre, w radius */
+    uint32_t mesh_id;
+    uint32_t material_id;
+    uint32_t flags;       /* bit 0 = casts shadow */
+    uint32_t lightmap_index;
+} HelioGpuInstanceData;
+
+/* GpuInstanceAabb, crates/libhelio/src/instance.rs:47-65. 32 bytes. */
+typedef struct HelioGpuInstanceAabb {
+    float min[3];
+    float pad0;
+    float max[3];
+    float pad1;
+} HelioGpuInstanceAabb;
+
+/* GpuDrawCall, crates/libhelio/src/draw.rs:26-37. 20 bytes. */
+typedef struct HelioGpuDrawCall {
+    uint32_t index_count;
+    uint32_t first_index;
+    int32_t vertex_offset;
+    uint32_t first_instance;
+    uint32_t instance_count;
+} HelioGpuDrawCall;
+
+/* DrawIndexedIndirectArgs, crates/libhelio/src/draw.rs:39-50. 20 bytes. */
+typedef struct HelioDrawIndexedIndirectArgs {
+    uint32_t index_count;
+    uint32_t instance_count;
+    uint32_t first_index;
+    int32_t base_vertex;
+    uint32_t first_instance;
+} HelioDrawIndexedIndirectArgs;
+
+/* GpuMeshletEntry, crates/libhelio/src/meshlet.rs:41-70. 64 bytes. */
+typedef struct HelioGpuMeshletEntry {
+    float center[3];
+    float radius;
+    float cone_apex[3];
+    float cone_cutoff; /* > 1 disables the cone test */
+    float cone_axis[3];
+    float lod_error;
+    uint32_t first_index;
+    uint32_t index_count;
+    int32_t vertex_offset;
+    uint32_t instance_index; /* reserved */
+} HelioGpuMeshletEntry;
+
+#define HELIO_VG_LOD_LEVELS 8
+#define HELIO_VG_MESHLETS_PER_WORK_ITEM 64
+
+/* GpuVgObject, crates/libhelio/src/meshlet.rs:72-97. 128 bytes. `reserved` receives
+ * selected LOD + 1 (0 = culled) from the object-select stage. */
+typedef struct HelioGpuVgObject {
+    uint32_t instance_index;
+    uint32_t lod_count;
+    uint32_t max_meshlet_count;
+    uint32_t reserved;
+    float local_bounds[4];
+    float lod_errors[HELIO_VG_LOD_LEVELS];
+    uint32_t lod_first_meshlets[HELIO_VG_LOD_LEVELS];
+    uint32_t lod_meshlet_counts[HELIO_VG_LOD_LEVELS];
+} HelioGpuVgObject;
+
+/* GpuVgDraw, crates/libhelio/src/meshlet.rs:99-111. 16 bytes. */
+typedef struct HelioGpuVgDraw {
+    uint32_t instance_index;
+    uint32_t meshlet_index;
+    uint32_t lod_level;
+    uint32_t reserved;
+} HelioGpuVgDraw;
+
+/* GpuVgWorkItem, crates/libhelio/src/meshlet.rs:113-124. 8 bytes. */
+typedef struct HelioGpuVgWorkItem {
+    uint32_t object_index;
+    uint32_t local_meshlet_base;
+} HelioGpuVgWorkItem;
+
+/* InstanceCullData, crates/helio-pass-virtual-geometry/src/lib.rs:122-130. 16 bytes. */
+typedef struct HelioInstanceCullData {
+    float max_scale;
+    float min_scale;
+    uint32_t cone_cull_enabled;
+    uint32_t valid_transform;
+} HelioInstanceCullData;
+
+/* ════════════════════════════════════════════════════════════════════════════
+ * Library-wide
+ * ════════════════════════════════════════════════════════════════════════════ */
+
+int32_t helio_abi_version(void);
+/* Message of this thread's last failing call ("" if none). */
+const char* helio_last_error(void);
+const char* helio_status_string(int32_t status);
+/* Number of kernels this library has launched in this process (all contexts). */
+uint64_t helio_kernel_launch_count(void);
+
+/* mip_levels(w, h) = bit length of max(w, h), at least 1.
+ * Reference: crates/helio-pass-hiz/src/lib.rs:376-379. */
+uint32_t helio_mip_levels(uint32_t width, uint32_t height);
+
+/* CPU Gribb–Hartmann plane extraction with the len > 1e-10 guard, used by the
+ * instance frustum pass. planes_out[6*4] = left, right, bottom, top, near, far.
+ * Reference: crates/helio-pass-indirect-dispatch/src/lib.rs:271-300. */
+void helio_extract_frustum_planes(const float view_proj[16], float planes_out[24]);
+
+/* InstanceCullData::from_instance over `count` instances, computed on the GPU
+ * (device in, device out). Reference: crates/helio-pass-virtual-geometry/src/lib.rs:132-167. */
+int32_t helio_instance_cull_data(const HelioGpuInstanceData* instances_dev, uint32_t count,
+                                 HelioInstanceCullData* out_dev, void* stream);
+
+/* ════════════════════════════════════════════════════════════════════════════
+ * Hi-Z pyramid — HiZBuildPass (crates/helio-pass-hiz/src/lib.rs:381-548)
+ *   hiz_depth_copy.wgsl:13-19 + hiz_build.wgsl:12-23, fused into one launch.
+ * ════════════════════════════════════════════════════════════════════════════ */
+
+#define HELIO_HIZ_MAX_MIPS 12 /* crates/helio-pass-hiz/src/lib.rs:27 */
+
+/* Level 0 is the caller's depth buffer itself instead of a copy (saves 8 B/px).
+ * Only valid while the depth buffer is not overwritten before the pyramid is read. */
+#define HELIO_HIZ_ALIAS_MIP0 1u
+
+typedef struct helio_hiz_config {
+    uint32_t width;
+    uint32_t height;
+    uint32_t flags;
+} helio_hiz_config;
+
+/* The published pyramid: R32Float levels, level l is width[l] x height[l] floats,
+ * row-major with row pitch pitch[l] floats. width[l] = max(1, width >> l). */
+typedef struct helio_hiz_pyramid {
+    uint32_t mip_count; /* min(helio_mip_levels(w, h), 12) */
+    uint32_t width[HELIO_HIZ_MAX_MIPS];
+    uint32_t height[HELIO_HIZ_MAX_MIPS];
+    uint32_t pitch[HELIO_HIZ_MAX_MIPS];
+    const float* levels[HELIO_HIZ_MAX_MIPS];
+} helio_hiz_pyramid;
+
+typedef struct helio_hiz_pass helio_hiz_pass;
+
+int32_t helio_hiz_create(const helio_hiz_config* config, helio_hiz_pass** out);
+/* depth_dev: device, width x height floats, row pitch depth_pitch floats (0 = width).
+ * camera_generation: the pass skips the rebuild when it equals the previous
+ * frame's value (reference lib.rs:472-478); pass UINT64_MAX to always rebuild. */
+int32_t helio_hiz_prepare(helio_hiz_pass* pass, const float* depth_dev, uint32_t depth_pitch,
+                          uint64_t camera_generation);
+int32_t helio_hiz_execute(helio_hiz_pass* pass, void* stream);
+int32_t helio_hiz_resize(helio_hiz_pass* pass, uint32_t width, uint32_t height);
+int32_t helio_hiz_publish(const helio_hiz_pass* pass, helio_hiz_pyramid* out);
+void helio_hiz_destroy(helio_hiz_pass* pass);
+
+/* ════════════════════════════════════════════════════════════════════════════
+ * Instance-level culling — IndirectDispatchPass + OcclusionCullPass
+ * ════════════════════════════════════════════════════════════════════════════ */
+
+/* SceneResources subset (crates/helio-core/src/scene/resources.rs:118-131); all device. */
+typedef struct helio_scene_buffers {
+    const HelioGpuCameraUniforms* camera;
+    const HelioGpuInstanceData* instances;
+    uint32_t instance_count;
+    const HelioGpuDrawCall* draw_calls;
+    uint32_t draw_count;
+    const HelioGpuInstanceAabb* aabbs; /* one per instance */
+    uint32_t* indirect;                /* draw_count x 5 u32 (DrawIndexedIndirectArgs) */
+} helio_scene_buffers;
+
+/* Cull statistics (crates/helio-pass-indirect-dispatch/shaders/indirect_dispatch.wgsl:69-77):
+ * [0] total draws [1] frustum culled [2] sub-pixel culled [3] frustum visible
+ * [4] occlusion culled [5] shadow casters [6] shadow visible [7] shadow occlusion culled.
+ * Passes accumulate; the caller clears once per frame (crates/helio/src/renderer/render.rs:441). */
+#define HELIO_CULL_STATS_COUNT 8
+
+typedef struct helio_indirect_dispatch_pass helio_indirect_dispatch_pass;
+
+/* stats_dev: device u32[8] shared with the occlusion pass (reference: new(device, cull_stats_buf)). */
+int32_t helio_indirect_dispatch_create(uint32_t* stats_dev, helio_indirect_dispatch_pass** out);
+/* Extracts the frustum planes on the host from camera->view_proj (host pointer) and
+ * records draw_count. Reference: crates/helio-pass-indirect-dispatch/src/lib.rs:178-191. */
+int32_t helio_indirect_dispatch_prepare(helio_indirect_dispatch_pass* pass,
+                                        const HelioGpuCameraUniforms* camera_host,
+                                        uint32_t draw_count);
+/* One thread per draw: indirect_dispatch.wgsl:100-176. */
+int32_t helio_indirect_dispatch_execute(helio_indirect_dispatch_pass* pass,
+                                        const helio_scene_buffers* scene, void* stream);
+void helio_indirect_dispatch_destroy(helio_indirect_dispatch_pass* pass);
+
+typedef struct helio_occlusion_cull_pass helio_occlusion_cull_pass;
+
+int32_t helio_occlusion_cull_create(uint32_t screen_width, uint32_t screen_height,
+                                    uint32_t* stats_dev, helio_occlusion_cull_pass** out);
+/* Reference: crates/helio-pass-occlusion-cull/src/lib.rs:297-317 (static Hi-Z off). */
+int32_t helio_occlusion_cull_prepare(helio_occlusion_cull_pass* pass, uint32_t draw_count);
+/* One thread per draw: occlusion_cull.wgsl:146-220. Frame 0 is skipped
+ * (no temporal pyramid yet, reference lib.rs:321). */
+int32_t helio_occlusion_cull_execute(helio_occlusion_cull_pass* pass,
+                                     const helio_scene_buffers* scene,
+                                     const helio_hiz_pyramid* hiz, uint64_t frame_num,
+                                     void* stream);
+int32_t helio_occlusion_cull_resize(helio_occlusion_cull_pass* pass, uint32_t w, uint32_t h);
+void helio_occlusion_cull_destroy(helio_occlusion_cull_pass* pass);
+
+/* Both instance passes in one kernel launch (frustum + sub-pixel, then the Hi-Z
+ * test when frame_num > 0). Writes the same indirect bytes and stats as
+ * helio_indirect_dispatch_execute followed by helio_occlusion_cull_execute. */
+int32_t helio_instance_cull_fused_execute(helio_indirect_dispatch_pass* frustum,
+                                          helio_occlusion_cull_pass* occlusion,
+                                          const helio_scene_buffers* scene,
+                                          const helio_hiz_pyramid* hiz, uint64_t frame_num,
+                                          void* stream);
+
+/* ════════════════════════════════════════════════════════════════════════════
+ * Virtual geometry — VirtualGeometryPass cull half
+ *   (crates/helio-pass-virtual-geometry/src/rendering.rs:703-1165,
+ *    shaders/vg_cull.wgsl:126-405)
+ * ════════════════════════════════════════════════════════════════════════════ */
+
+/* VgFrameData, crates/libhelio/src/frame.rs:485-516. `memory` says whether the four
+ * arrays are host or device pointers. instances has one entry per object. */
+typedef struct helio_vg_frame_data {
+    const HelioGpuMeshletEntry* meshlets;
+    const HelioGpuVgObject* objects;
+    const HelioGpuInstanceData* instances;
+    const HelioGpuVgWorkItem* work_items;
+    uint32_t meshlet_count;
+    uint32_t object_count;
+    uint32_t work_item_count;
+    uint32_t max_draw_count;
+    uint64_t buffer_version;
+    uint64_t instance_version;
+    uint32_t instance_dirty_start;
+    uint32_t instance_dirty_count;
+    uint32_t memory; /* HELIO_MEM_HOST or HELIO_MEM_DEVICE */
+    uint32_t reserved0;
+} helio_vg_frame_data;
+
+/* LodQuality, crates/helio-pass-virtual-geometry/src/lib.rs:174-203. */
+#define HELIO_LOD_LOW 0u    /* 4.0 px */
+#define HELIO_LOD_MEDIUM 1u /* 2.0 px (default) */
+#define HELIO_LOD_HIGH 2u   /* 1.0 px */
+#define HELIO_LOD_ULTRA 3u  /* 0.5 px */
+float helio_lod_max_error_pixels(uint32_t lod_quality);
+
+/* DEFAULT_MAX_PUBLISHED_MESHLETS, crates/helio-pass-virtual-geometry/src/lib.rs:76. */
+#define HELIO_VG_DEFAULT_PUBLICATION_LIMIT 262144u
+/* Counter layout (lib.rs:21-28): [0] attempted visible draws, [1] rejected by
+ * capacity, [2..9] selected-LOD object histogram, [10] deepest LOD among visible objects. */
+#define HELIO_VG_COUNTER_COUNT 11u
+
+typedef struct helio_vg_config {
+    uint32_t width;             /* render size: CullUniforms.screen_width/height */
+    uint32_t height;
+    uint32_t lod_quality;       /* HELIO_LOD_* */
+    uint32_t publication_limit; /* 0 = HELIO_VG_DEFAULT_PUBLICATION_LIMIT */
+    uint32_t counter_count;     /* 2 (benchmark layout) or 11 (production layout); 0 = 11 */
+    uint32_t flags;
+} helio_vg_config;
+
+/* Published outputs (device pointers owned by the pass). */
+typedef struct helio_vg_outputs {
+    HelioDrawIndexedIndirectArgs* indirect; /* [capacity]; first `min(counters[0], capacity)` valid */
+    HelioGpuVgDraw* draws;                  /* [capacity] */
+    uint32_t* counters;                     /* [counter_count] */
+    uint32_t* visibility;                   /* [2 * work_item_count]: bit l of word 2w+(l>>5)
+                                               = meshlet l of work item w visible */
+    HelioGpuVgObject* objects;              /* [object_count]; reserved = selected LOD + 1 */
+    uint32_t capacity;
+    uint32_t counter_count;
+    uint32_t work_item_count;
+    uint32_t object_count;
+} helio_vg_outputs;
+
+typedef struct helio_vg_pass helio_vg_pass;
+
+int32_t helio_vg_create(const helio_vg_config* config, helio_vg_pass** out);
+/* Uploads on buffer_version change, else patches [instance_dirty_start, +count) on
+ * instance_version change; recomputes InstanceCullData on the GPU for what changed.
+ * Reference: rendering.rs:708-859. May allocate (growth). */
+int32_t helio_vg_prepare(helio_vg_pass* pass, const helio_vg_frame_data* frame, void* stream);
+/* Clears the counters, runs object select then meshlet cull with deterministic
+ * compaction: the visible draws are stored in (work item, lane) order and
+ * first_instance = slot. camera: device pointer. hiz: published pyramid.
+ * Returns HELIO_ERR_CAPACITY only if the caller asks for it via
+ * helio_vg_check_overflow(); execute itself never reads back. */
+int32_t helio_vg_execute(helio_vg_pass* pass, const HelioGpuCameraUniforms* camera_dev,
+                         const helio_hiz_pyramid* hiz, void* stream);
+int32_t helio_vg_resize(helio_vg_pass* pass, uint32_t width, uint32_t height);
+int32_t helio_vg_set_lod_quality(helio_vg_pass* pass, uint32_t lod_quality);
+int32_t helio_vg_publish(const helio_vg_pass* pass, helio_vg_outputs* out);
+/* Device-side error word of the last execute (0 = none, else HELIO_ERR_TIMEOUT);
+ * synchronises `stream`. */
+int32_t helio_vg_device_status(helio_vg_pass* pass, void* stream);
+void helio_vg_destroy(helio_vg_pass* pass);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+
+#endif /* HELIO_CULL_H */

@@ -1,0 +1,99 @@
+/*
+ * oracle.h — CPU restatement of Helio's GPU visibility path.
+ *
+ * TEST INFRASTRUCTURE ONLY. This library is the checker for the CUDA path: it
+ * may be loaded by tests/, by __graft_entry__.smoke() and by bench.py's CPU
+ * baseline / reference arm, and by nothing else. The product library
+ * (helio_b200/lib/libhelio_cull.so) never links, loads or calls it.
+ *
+ * Every function restates one reference shader entry point or Rust helper, in
+ * the WGSL operation order, with IEEE binary32 arithmetic and no contraction
+ * (built with -O2 -ffp-contract=off). Citations are per function in oracle.cpp.
+ *
+ * Parity status: the reference's shaders cannot execute on either machine
+ * (no Rust toolchain, browser-only wgpu, no graphics stack). The restatement is
+ * pinned against every known-answer test that the reference's own test files
+ * hold for this path (tests/golden/reference_kats.json); end-to-end execution of
+ * the WGSL itself is unpinned.
+ */
+#ifndef HELIO_ORACLE_H
+#define HELIO_ORACLE_H
+
+#include <stdint.h>
+#include "../include/helio_cull.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Decision statistics gathered while culling (for the 1e-6 relative margin band
+ * and for the algorithmic byte count). */
+typedef struct oracle_stats {
+    uint64_t objects_tested;
+    uint64_t objects_visible;
+    uint64_t meshlets_tested;      /* meshlets of a selected LOD of a visible object */
+    uint64_t meshlets_cone_loaded; /* passed frustum (cone inputs needed) */
+    uint64_t meshlets_visible;
+    uint64_t marginal_decisions;   /* comparisons whose operands lie within 1e-6 relative */
+    uint64_t marginal_meshlets;    /* meshlets with at least one marginal decision */
+    uint64_t marginal_objects;
+} oracle_stats;
+
+uint32_t oracle_mip_levels(uint32_t w, uint32_t h);
+uint32_t oracle_ceil_log2(float d);
+void oracle_extract_frustum_planes(const float vp[16], float planes[24]);
+void oracle_instance_cull_data(const HelioGpuInstanceData* inst, uint32_t n,
+                               HelioInstanceCullData* out);
+
+/* Builds every level of the pyramid. levels[l] must hold width[l]*height[l]
+ * floats (dense); level 0 receives the copy of depth. Returns mip count. */
+uint32_t oracle_hiz_build(const float* depth, uint32_t w, uint32_t h, uint32_t pitch,
+                          float* const* levels);
+
+void oracle_indirect_dispatch(const HelioGpuCameraUniforms* cam, const float planes[24],
+                              const HelioGpuInstanceData* inst, const HelioGpuDrawCall* dc,
+                              const HelioGpuInstanceAabb* aabb, uint32_t draw_count,
+                              uint32_t instance_count, uint32_t* indirect, uint32_t* stats);
+
+void oracle_occlusion_cull(const HelioGpuCameraUniforms* cam, uint32_t screen_w,
+                           uint32_t screen_h, const helio_hiz_pyramid* hiz,
+                           const HelioGpuInstanceData* inst, const HelioGpuDrawCall* dc,
+                           uint32_t draw_count, uint32_t instance_count, uint32_t* indirect,
+                           uint32_t* stats, oracle_stats* st);
+
+/* Uniforms of the VG cull (CullUniforms, rendering.rs:828-859). */
+typedef struct oracle_vg_uniforms {
+    uint32_t object_count;
+    uint32_t screen_width;
+    uint32_t screen_height;
+    uint32_t hiz_mip_count;
+    uint32_t draw_capacity;
+    float lod_error_threshold_px;
+    uint32_t work_item_count;
+    uint32_t meshlet_count;
+    uint32_t instance_count;
+    uint32_t counter_count;
+} oracle_vg_uniforms;
+
+/* cs_select_objects: writes selected[i] = LOD + 1 (0 = culled) and the LOD
+ * histogram / max-LOD counters when counter_count >= 11. */
+void oracle_vg_select(const HelioGpuCameraUniforms* cam, const oracle_vg_uniforms* u,
+                      const HelioGpuVgObject* objects, const HelioGpuInstanceData* inst,
+                      const HelioInstanceCullData* cull, uint32_t* selected, uint32_t* counters,
+                      oracle_stats* st, int threads);
+
+/* cs_cull_meshlets in the canonical (work item, lane) order. visibility receives
+ * 2 words per work item. counters[0] = attempted, counters[1] = rejected. */
+void oracle_vg_cull(const HelioGpuCameraUniforms* cam, const oracle_vg_uniforms* u,
+                    const HelioGpuMeshletEntry* meshlets, const HelioGpuVgObject* objects,
+                    const uint32_t* selected, const HelioGpuInstanceData* inst,
+                    const HelioInstanceCullData* cull, const HelioGpuVgWorkItem* items,
+                    const helio_hiz_pyramid* hiz, HelioDrawIndexedIndirectArgs* indirect,
+                    HelioGpuVgDraw* draws, uint32_t* counters, uint32_t* visibility,
+                    oracle_stats* st, int threads);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif
