@@ -19,8 +19,67 @@
 #include "kernels.h"
 #include "vg.h"
 
+#include <map>
+#include <mutex>
+#include <vector>
+
 static std::atomic<uint64_t> g_launches{0};
-void helio_note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
+namespace {
+
+// Event profiler state: pending (name, start, end) records until collected.
+struct ProfRecord {
+    const char* name;
+    cudaEvent_t start, end;
+};
+struct Profiler {
+    std::mutex mu;
+    std::atomic<bool> enabled{false};
+    std::vector<ProfRecord> pending;
+    std::vector<cudaEvent_t> free_events;
+    std::map<std::string, std::pair<uint64_t, double>> totals;
+    thread_local static cudaEvent_t open_start;
+    thread_local static const char* open_name;
+    cudaEvent_t take() {
+        if (!free_events.empty()) {
+            cudaEvent_t e = free_events.back();
+            free_events.pop_back();
+            return e;
+        }
+        cudaEvent_t e = nullptr;
+        cudaEventCreate(&e);
+        return e;
+    }
+};
+thread_local cudaEvent_t Profiler::open_start = nullptr;
+thread_local const char* Profiler::open_name = nullptr;
+Profiler g_prof;
+
+bool capturing(cudaStream_t s) {
+    cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+    return cudaStreamIsCapturing(s, &st) == cudaSuccess && st != cudaStreamCaptureStatusNone;
+}
+
+}  // namespace
+
+void helio_launch_begin(const char* kernel, cudaStream_t stream) {
+    if (!g_prof.enabled.load(std::memory_order_relaxed) || capturing(stream)) return;
+    std::lock_guard<std::mutex> lk(g_prof.mu);
+    Profiler::open_start = g_prof.take();
+    Profiler::open_name = kernel;
+    cudaEventRecord(Profiler::open_start, stream);
+}
+
+void helio_launch_end(cudaStream_t stream) {
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    if (!Profiler::open_start) return;
+    std::lock_guard<std::mutex> lk(g_prof.mu);
+    cudaEvent_t end = g_prof.take();
+    cudaEventRecord(end, stream);
+    g_prof.pending.push_back({Profiler::open_name, Profiler::open_start, end});
+    Profiler::open_start = nullptr;
+    Profiler::open_name = nullptr;
+}
 
 namespace {
 
@@ -149,6 +208,7 @@ struct helio_vg_pass {
     bool have_version = false;
     uint32_t num_tiles = 0;
     size_t scratch_clear_bytes = 0;
+    size_t view_offset = 0;
 };
 
 // ════════════════════════════════════════════════════════════════════════════
@@ -160,6 +220,50 @@ extern "C" {
 int32_t helio_abi_version(void) { return HELIO_ABI_VERSION; }
 const char* helio_last_error(void) { return t_last_error.c_str(); }
 uint64_t helio_kernel_launch_count(void) { return g_launches.load(); }
+
+int32_t helio_profiler_enable(int32_t enabled) {
+    g_prof.enabled.store(enabled != 0);
+    return HELIO_OK;
+}
+
+int32_t helio_profiler_collect(helio_kernel_timing* out, uint32_t capacity, uint32_t* count) {
+    HELIO_ARG(count && (capacity == 0 || out), "null pointer");
+    std::lock_guard<std::mutex> lk(g_prof.mu);
+    for (const ProfRecord& r : g_prof.pending) {
+        HELIO_CK(cudaEventSynchronize(r.end));
+        float ms = 0.0f;
+        HELIO_CK(cudaEventElapsedTime(&ms, r.start, r.end));
+        auto& t = g_prof.totals[r.name];
+        t.first += 1;
+        t.second += ms;
+        g_prof.free_events.push_back(r.start);
+        g_prof.free_events.push_back(r.end);
+    }
+    g_prof.pending.clear();
+    uint32_t n = 0;
+    for (const auto& kv : g_prof.totals) {
+        if (n < capacity) {
+            std::memset(&out[n], 0, sizeof(out[n]));
+            std::strncpy(out[n].name, kv.first.c_str(), sizeof(out[n].name) - 1);
+            out[n].launches = kv.second.first;
+            out[n].total_ms = kv.second.second;
+        }
+        ++n;
+    }
+    *count = n;
+    return HELIO_OK;
+}
+
+void helio_profiler_reset(void) {
+    std::lock_guard<std::mutex> lk(g_prof.mu);
+    for (const ProfRecord& r : g_prof.pending) {
+        cudaEventSynchronize(r.end);
+        g_prof.free_events.push_back(r.start);
+        g_prof.free_events.push_back(r.end);
+    }
+    g_prof.pending.clear();
+    g_prof.totals.clear();
+}
 
 const char* helio_status_string(int32_t status) {
     switch (status) {
@@ -194,11 +298,7 @@ void helio_extract_frustum_planes(const float vp[16], float planes_out[24]) {
         p[5][c] = r[3][c] - r[2][c];
     }
     for (int k = 0; k < 6; ++k) {
-        volatile float xx = p[k][0] * p[k][0];
-        volatile float yy = p[k][1] * p[k][1];
-        volatile float zz = p[k][2] * p[k][2];
-        volatile float s = xx + yy;
-        float len = std::sqrt((float)(s + zz));
+        float len = std::sqrt((p[k][0] * p[k][0] + p[k][1] * p[k][1]) + p[k][2] * p[k][2]);
         for (int c = 0; c < 4; ++c) planes_out[k * 4 + c] = (len > 1e-10f) ? p[k][c] / len : p[k][c];
     }
 }
@@ -523,9 +623,11 @@ int32_t helio_vg_prepare(helio_vg_pass* p, const helio_vg_frame_data* f, void* s
         }
         p->max_draw_count = bounded;
         p->num_tiles = helio::vg_cull_tiles(p->work_item_count);
-        // scratch: counters (16 words) | tile ticket | error | pad | look-back states
-        p->scratch_clear_bytes = 64 + 16 + (size_t)p->num_tiles * 8;
-        HELIO_CK(p->scratch.ensure(p->scratch_clear_bytes));
+        // scratch: counters (16 words) | tile counts (both cleared per execute) | warp counts |
+        //          window bits | view constants (16-byte aligned)
+        p->scratch_clear_bytes = 64 + (size_t)p->num_tiles * 4;
+        p->view_offset = (64 + helio::vg_cull_scratch_words(p->num_tiles) * 4 + 15) & ~(size_t)15;
+        HELIO_CK(p->scratch.ensure(p->view_offset + sizeof(helio::CullView)));
         HELIO_CK(cudaMemsetAsync(p->scratch.ptr, 0, p->scratch_clear_bytes, s));
         p->last_version = f->buffer_version;
         p->last_instance_version = f->instance_version;
@@ -572,32 +674,38 @@ int32_t helio_vg_execute(helio_vg_pass* p, const HelioGpuCameraUniforms* camera_
     scene.instance_count = p->object_count;
     scene.work_item_count = p->work_item_count;
 
+    helio::CullView* view =
+        reinterpret_cast<helio::CullView*>(reinterpret_cast<char*>(p->scratch.ptr) + p->view_offset);
+    helio::ViewSetupParams vs{};
+    vs.camera = camera_dev;
+    vs.out = view;
+    vs.hiz = to_view(*hiz);
+    vs.screen_height = p->cfg.height;
+    vs.hiz_mip_count = mip_levels(p->cfg.width, p->cfg.height);  // unclamped, rendering.rs:828-829
+    vs.lod_threshold_px = p->lod_threshold;
+    helio::launch_vg_view_setup(vs, s);
+
     helio::VgSelectParams sp{};
     sp.scene = scene;
-    sp.camera = camera_dev;
+    sp.view = view;
     sp.sel = p->sel.as<helio::SelRecord>();
     sp.counters = scratch;
     sp.counter_count = p->counter_count;
-    sp.screen_height = p->cfg.height;
-    sp.lod_threshold_px = p->lod_threshold;
     sp.write_reserved = 1u;
     helio::launch_vg_select(sp, s);
 
     helio::VgCullParams cp{};
     cp.scene = scene;
-    cp.camera = camera_dev;
+    cp.view = view;
     cp.sel = p->sel.as<helio::SelRecord>();
     cp.indirect = p->indirect.as<HelioDrawIndexedIndirectArgs>();
     cp.draws = p->draws.as<HelioGpuVgDraw>();
     cp.counters = scratch;
     cp.visibility = p->visibility.as<uint32_t>();
-    cp.scratch.tile_counter = scratch + 16;
-    cp.scratch.error_word = scratch + 17;
-    cp.scratch.lookback = reinterpret_cast<unsigned long long*>(reinterpret_cast<char*>(p->scratch.ptr) + 80);
-    cp.hiz = to_view(*hiz);
+    cp.scratch.tile_counts = scratch + 16;
+    cp.scratch.warp_counts = cp.scratch.tile_counts + p->num_tiles;
+    cp.scratch.bits = cp.scratch.warp_counts + (size_t)p->num_tiles * helio::kCullWarps;
     cp.capacity = p->max_draw_count;  // min(draw_capacity, buffer lengths), vg_cull.wgsl:248-251
-    cp.screen_height = p->cfg.height;
-    cp.hiz_mip_count = mip_levels(p->cfg.width, p->cfg.height);
     cp.num_tiles = p->num_tiles;
     helio::launch_vg_cull(cp, s);
     HELIO_CK(cudaGetLastError());
@@ -635,11 +743,10 @@ int32_t helio_vg_publish(const helio_vg_pass* p, helio_vg_outputs* out) {
 
 int32_t helio_vg_device_status(helio_vg_pass* p, void* stream) {
     HELIO_ARG(p, "null pointer");
-    if (!p->scratch.ptr) return HELIO_OK;
-    uint32_t word = 0;
-    HELIO_CK(cudaMemcpyAsync(&word, p->scratch.as<uint32_t>() + 17, 4, cudaMemcpyDeviceToHost, as_stream(stream)));
+    // The VG kernels never wait on one another inside a launch; this reports any
+    // asynchronous CUDA error of the work queued so far.
     HELIO_CK(cudaStreamSynchronize(as_stream(stream)));
-    if (word == helio::kDevTimeout) return fail(HELIO_ERR_TIMEOUT, "meshlet cull look-back wait timed out");
+    HELIO_CK(cudaGetLastError());
     return HELIO_OK;
 }
 

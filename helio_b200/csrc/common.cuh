@@ -140,6 +140,27 @@ __device__ __forceinline__ Planes publish_planes(const float* vp) {
     return out;
 }
 
+// The same planes computed by lanes 0..5 of one warp in parallel (lane i builds
+// plane i); every lane of the warp must call it. Writes `out` (shared memory).
+__device__ __forceinline__ void publish_planes_warp(const float* vp, Planes& out) {
+    const int lane = threadIdx.x & 31;
+    if (lane < 6) {
+        float p[4];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const float r3 = __ldg(vp + c * 4 + 3);
+            const float rr = __ldg(vp + c * 4 + (lane >> 1));  // rows 0,0,1,1,2,2
+            if (lane == 4) p[c] = __ldg(vp + c * 4 + 2);
+            else if (lane == 5) p[c] = fsub(r3, __ldg(vp + c * 4 + 2));
+            else if (lane & 1) p[c] = fsub(r3, rr);
+            else p[c] = fadd(r3, rr);
+        }
+        const float len = fsqrt(dot3(f3(p[0], p[1], p[2]), f3(p[0], p[1], p[2])));
+        out.p[lane] = make_float4(fdiv(p[0], len), fdiv(p[1], len), fdiv(p[2], len), fdiv(p[3], len));
+    }
+    __syncwarp();
+}
+
 // sphere_visible, vg_cull.wgsl:126-133: every plane satisfies dot(n, c) + d >= -r.
 __device__ __forceinline__ bool sphere_visible_vg(const Planes& pl, F3 c, float r) {
     float nr = -r;
@@ -159,5 +180,7 @@ constexpr uint32_t kSpinLimit = 1u << 22;  // polls before a bounded wait gives 
 
 }  // namespace helio
 
-// Host-side launch accounting (helio_kernel_launch_count).
-void helio_note_launch();
+// Host-side launch accounting (helio_kernel_launch_count) and the optional
+// event profiler (helio_profiler_*): every launch is bracketed by these two calls.
+void helio_launch_begin(const char* kernel, cudaStream_t stream);
+void helio_launch_end(cudaStream_t stream);

@@ -39,38 +39,57 @@ __device__ __forceinline__ float red4(float a, float b, float c, float d, bool x
 
 constexpr int kTailBuf = 2304;  // floats per shared tail buffer
 
-__device__ void hiz_tail(const HizJob& J) {
+// Levels 7.. of one pyramid, built by one warp (lane = threadIdx.x & 31) of the
+// CTA that finished the view's last tile. A source level that lives only in
+// global memory is read in batches of 8 texels per lane (32 loads in flight);
+// levels that fit are kept in shared memory for the next step.
+__device__ void hiz_tail_warp(const HizJob& J) {
     __shared__ float bufA[kTailBuf];
     __shared__ float bufB[kTailBuf];
+    const uint32_t lane = threadIdx.x & 31u;
     float* cur = nullptr;  // shared copy of the current source level (or null)
     float* nxt = bufA;
     for (uint32_t l = 7; l < J.mip_count; ++l) {
         const uint32_t sw = J.lw[l - 1], sh = J.lh[l - 1], sp = J.lpitch[l - 1];
         const uint32_t dw = J.lw[l], dh = J.lh[l], dp = J.lpitch[l];
-        const float* src = J.levels[l - 1];
-        float* dst = J.levels[l];
-        const bool fits = (size_t)dw * dh <= (size_t)kTailBuf;
-        for (uint32_t i = threadIdx.x; i < dw * dh; i += blockDim.x) {
-            uint32_t y = i / dw, x = i - y * dw;
-            uint32_t x0 = 2 * x, y0 = 2 * y;
-            uint32_t x1 = min(x0 + 1, sw - 1), y1 = min(y0 + 1, sh - 1);
-            float s00, s10, s01, s11;
-            if (cur) {
-                s00 = cur[y0 * sw + x0];
-                s10 = cur[y0 * sw + x1];
-                s01 = cur[y1 * sw + x0];
-                s11 = cur[y1 * sw + x1];
-            } else {
-                s00 = __ldcg(src + (size_t)y0 * sp + x0);
-                s10 = __ldcg(src + (size_t)y0 * sp + x1);
-                s01 = __ldcg(src + (size_t)y1 * sp + x0);
-                s11 = __ldcg(src + (size_t)y1 * sp + x1);
+        const float* __restrict__ src = J.levels[l - 1];
+        float* __restrict__ dst = J.levels[l];
+        const uint32_t n = dw * dh;
+        const bool fits = (size_t)n <= (size_t)kTailBuf;
+        for (uint32_t base = lane; base < n; base += 32u * 8u) {
+            float s[8][4];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const uint32_t i = base + 32u * j;
+                if (i < n) {
+                    const uint32_t y = i / dw, x = i - y * dw;
+                    const uint32_t x0 = 2 * x, y0 = 2 * y;
+                    const uint32_t x1 = min(x0 + 1, sw - 1), y1 = min(y0 + 1, sh - 1);
+                    if (cur) {
+                        s[j][0] = cur[y0 * sw + x0];
+                        s[j][1] = cur[y0 * sw + x1];
+                        s[j][2] = cur[y1 * sw + x0];
+                        s[j][3] = cur[y1 * sw + x1];
+                    } else {
+                        s[j][0] = __ldcg(src + (size_t)y0 * sp + x0);
+                        s[j][1] = __ldcg(src + (size_t)y0 * sp + x1);
+                        s[j][2] = __ldcg(src + (size_t)y1 * sp + x0);
+                        s[j][3] = __ldcg(src + (size_t)y1 * sp + x1);
+                    }
+                }
             }
-            float v = fmaxf(fmaxf(s00, s10), fmaxf(s01, s11));
-            dst[(size_t)y * dp + x] = v;
-            if (fits) nxt[i] = v;
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const uint32_t i = base + 32u * j;
+                if (i < n) {
+                    const uint32_t y = i / dw, x = i - y * dw;
+                    const float v = fmaxf(fmaxf(s[j][0], s[j][1]), fmaxf(s[j][2], s[j][3]));
+                    dst[(size_t)y * dp + x] = v;
+                    if (fits) nxt[i] = v;
+                }
+            }
         }
-        __syncthreads();
+        __syncwarp();
         if (fits) {
             cur = nxt;
             nxt = (nxt == bufA) ? bufB : bufA;
@@ -88,7 +107,6 @@ __global__ void __launch_bounds__(256) hiz_build_kernel(HizJob single, const Hiz
     __shared__ float s_m3[8][9];
     __shared__ HizJob s_J;
     __shared__ uint32_t s_job;
-    __shared__ uint32_t s_last;
     const uint32_t tile = blockIdx.x;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (tid == 0) {
@@ -201,8 +219,9 @@ __global__ void __launch_bounds__(256) hiz_build_kernel(HizJob single, const Hiz
         }
     }
     __syncthreads();
+    if (warp != 0) return;  // levels 4.. and the tail need only warp 0
     // Levels 4..6: warp 0.
-    if (warp == 0 && J.mip_count > 4) {
+    if (J.mip_count > 4) {
         const int x4 = lane & 3, y4 = (lane >> 2) & 3;
         float m4 = red4(s_m3[2 * y4][2 * x4], s_m3[2 * y4][2 * x4 + 1], s_m3[2 * y4 + 1][2 * x4],
                         s_m3[2 * y4 + 1][2 * x4 + 1], J.lw[3] == 1u, J.lh[3] == 1u);
@@ -231,21 +250,23 @@ __global__ void __launch_bounds__(256) hiz_build_kernel(HizJob single, const Hiz
             }
         }
     }
-    if (J.mip_count <= 7) return;
+    if (warp != 0 || J.mip_count <= 7) return;
 
-    // Tail: the last CTA of this job builds levels 7.. from level 6.
+    // Tail: level 6 is written by warp 0 only, so warp 0 alone takes the ticket;
+    // the warp of the last CTA of this job builds levels 7.. from level 6.
     __threadfence();
-    __syncthreads();
-    if (tid == 0) {
+    __syncwarp();
+    uint32_t last = 0u;
+    if (lane == 0) {
         const uint32_t tiles = J.tiles_x * J.tiles_y;
-        uint32_t t = atomicAdd(&tickets[s_job], 1u);
-        s_last = (t + 1 == tiles) ? 1u : 0u;
-        if (s_last) tickets[s_job] = 0u;  // every other CTA of this job has already taken its ticket
+        const uint32_t t = atomicAdd(&tickets[s_job], 1u);
+        last = (t + 1 == tiles) ? 1u : 0u;
+        if (last) tickets[s_job] = 0u;  // every other CTA of this job has already taken its ticket
     }
-    __syncthreads();
-    if (s_last) {
+    last = __shfl_sync(0xffffffffu, last, 0);
+    if (last) {
         __threadfence();
-        hiz_tail(J);
+        hiz_tail_warp(J);
     }
 }
 
@@ -296,15 +317,17 @@ void hiz_assign(HizJob* job, const float* depth, float* levels_base) {
 void launch_hiz_build(const HizJob* jobs_dev, uint32_t n_jobs, uint32_t total_tiles, uint32_t* tickets_dev,
                       cudaStream_t stream) {
     if (total_tiles == 0 || n_jobs == 0) return;
+    helio_launch_begin("hiz_build", stream);
     hiz_build_kernel<<<total_tiles, 256, 0, stream>>>(HizJob{}, jobs_dev, n_jobs, tickets_dev);
-    helio_note_launch();
+    helio_launch_end(stream);
 }
 
 void launch_hiz_build_single(const HizJob& job, uint32_t* ticket_dev, cudaStream_t stream) {
     const uint32_t tiles = job.tiles_x * job.tiles_y;
     if (tiles == 0) return;
+    helio_launch_begin("hiz_build", stream);
     hiz_build_kernel<<<tiles, 256, 0, stream>>>(job, nullptr, 1u, ticket_dev);
-    helio_note_launch();
+    helio_launch_end(stream);
 }
 
 }  // namespace helio

@@ -177,11 +177,13 @@ __global__ void __launch_bounds__(256) instance_cull_kernel(InstanceCullParams P
 void launch_instance_cull(const InstanceCullParams& p, bool frustum, bool occlusion, cudaStream_t stream) {
     if (p.draw_count == 0) return;
     const uint32_t blocks = (p.draw_count + 255u) / 256u;
+    if (!frustum && !occlusion) return;
+    helio_launch_begin(frustum && occlusion ? "instance_cull_fused" : frustum ? "indirect_dispatch" : "occlusion_cull",
+                       stream);
     if (frustum && occlusion) instance_cull_kernel<true, true><<<blocks, 256, 0, stream>>>(p);
     else if (frustum) instance_cull_kernel<true, false><<<blocks, 256, 0, stream>>>(p);
-    else if (occlusion) instance_cull_kernel<false, true><<<blocks, 256, 0, stream>>>(p);
-    else return;
-    helio_note_launch();
+    else instance_cull_kernel<false, true><<<blocks, 256, 0, stream>>>(p);
+    helio_launch_end(stream);
 }
 
 }  // namespace helio

@@ -22,46 +22,75 @@ struct VgSceneDev {
     uint32_t work_item_count;
 };
 
+// View constants shared by every CTA of the select / cull kernels, computed once
+// per launch by vg_view_setup_kernel from the device camera (vg_cull.wgsl:266-280
+// planes; fields of GpuCameraUniforms) and the Hi-Z pyramid descriptor.
+struct CullView {
+    Planes planes;
+    Mat4 vp;
+    float4 pos_near;
+    float p00, p11;
+    float focal;      // |proj[1][1]| * screen_height * 0.5 (vg_cull.wgsl:321-322)
+    float lod_threshold_px;
+    HizView hiz;
+    uint32_t screen_height;
+    uint32_t hiz_mip_count;
+    uint32_t pad[2];
+};
+static_assert(sizeof(CullView) % 16 == 0, "CullView is copied as 16-byte words");
+
 // Per-object result of the select stage: selected LOD range of the object.
 // x = first meshlet of the LOD, y = meshlets in it, z = instance index, w = LOD + 1 (0 = culled).
 using SelRecord = uint4;
 
 struct VgSelectParams {
     VgSceneDev scene;
-    const HelioGpuCameraUniforms* camera;
+    const CullView* view;
     SelRecord* sel;     // [object_count]
     uint32_t* counters; // [counter_count]
     uint32_t counter_count;
-    uint32_t screen_height;
-    float lod_threshold_px;
     uint32_t write_reserved;  // also store LOD + 1 into objects[i].reserved
 };
 
-// Scratch of one cull launch, cleared before it: [counters..][tile ticket][error][look-back states].
-struct VgCullScratch {
-    uint32_t* tile_counter;
-    uint32_t* error_word;
-    unsigned long long* lookback;  // [num_tiles]
+// Inputs of vg_view_setup_kernel: computes *out from the device camera.
+struct ViewSetupParams {
+    const HelioGpuCameraUniforms* camera;
+    CullView* out;
+    HizView hiz;
+    uint32_t screen_height;
+    uint32_t hiz_mip_count;
+    float lod_threshold_px;
 };
+
+constexpr uint32_t kCullWarps = 8;                       // warps per CTA tile
+constexpr uint32_t kCullItemsPerTile = kCullWarps * 32;  // one work item per lane
+constexpr uint32_t kWindowsPerWarp = 64;                 // 32 items x 64 meshlets / 32 lanes
+
+// Scratch of one cull launch. tile_counts must be zero before the test kernel
+// (it accumulates per-warp counts); warp_counts and bits are written before
+// they are read.
+struct VgCullScratch {
+    uint32_t* tile_counts;  // [num_tiles] visible meshlets per tile
+    uint32_t* warp_counts;  // [num_tiles * kCullWarps]
+    uint32_t* bits;         // [num_tiles * kCullWarps * kWindowsPerWarp] window ballots
+};
+
+inline size_t vg_cull_scratch_words(uint32_t tiles) {
+    return (size_t)tiles * (1 + kCullWarps + (size_t)kCullWarps * kWindowsPerWarp);
+}
 
 struct VgCullParams {
     VgSceneDev scene;
-    const HelioGpuCameraUniforms* camera;
+    const CullView* view;
     const SelRecord* sel;
     HelioDrawIndexedIndirectArgs* indirect;
     HelioGpuVgDraw* draws;
     uint32_t* counters;
     uint32_t* visibility;  // [2 * work_item_count] or null
     VgCullScratch scratch;
-    HizView hiz;
     uint32_t capacity;
-    uint32_t screen_height;
-    uint32_t hiz_mip_count;  // mip_levels(width, height), unclamped (rendering.rs:828-829)
     uint32_t num_tiles;
 };
-
-constexpr uint32_t kCullWarps = 4;
-constexpr uint32_t kCullItemsPerTile = kCullWarps * 32;
 
 inline uint32_t vg_cull_tiles(uint32_t work_items) { return (work_items + kCullItemsPerTile - 1) / kCullItemsPerTile; }
 
@@ -69,7 +98,9 @@ void launch_pack_meshlets(const HelioGpuMeshletEntry* aos, uint32_t n, float4* b
                           uint4* draw, cudaStream_t stream);
 void launch_instance_cull_data(const HelioGpuInstanceData* inst, uint32_t n, HelioInstanceCullData* out,
                                cudaStream_t stream);
+void launch_vg_view_setup(const ViewSetupParams& p, cudaStream_t stream);
 void launch_vg_select(const VgSelectParams& p, cudaStream_t stream);
+// Test kernel then emit kernel on `stream`.
 void launch_vg_cull(const VgCullParams& p, cudaStream_t stream);
 
 }  // namespace helio

@@ -3,19 +3,20 @@
 // References (crates/helio-pass-virtual-geometry/):
 //   shaders/vg_cull.wgsl:282-352   cs_select_objects  -> vg_select_kernel
 //   shaders/vg_cull.wgsl:135-264   cull_meshlet       -> meshlet_visible + emission
-//   shaders/vg_cull.wgsl:354-405   cs_cull_meshlets   -> vg_cull_kernel
+//   shaders/vg_cull.wgsl:354-405   cs_cull_meshlets   -> vg_cull_test_kernel + vg_cull_emit_kernel
 //   src/lib.rs:132-167             InstanceCullData::from_instance -> instance_cull_data_kernel
 //
 // Layout and scheduling (B200 design, not a translation of the WGSL dispatches):
 //   * meshlet descriptors are re-laid once per upload into four 16-byte streams;
-//   * a warp owns 32 consecutive work items (one per lane); the lanes first read
-//     their item and the object's selected-LOD record, then the warp packs the
-//     active meshlets of all 32 items densely into 32-lane windows, so a work item
-//     whose LOD has 13 meshlets occupies 13 lanes instead of a 64-lane group;
-//   * visible meshlets are compacted deterministically: window ballots are kept in
-//     shared memory, each CTA publishes its count with a decoupled look-back
-//     (one warp inspects 32 predecessors per step), then every visible meshlet is
-//     written at slot = (visible meshlets before it in (work item, lane) order).
+//   * a warp owns 32 consecutive work items (one per lane); the lanes read their
+//     item and the object's selected-LOD record, then the warp packs the active
+//     meshlets of all 32 items densely into 32-lane windows, so a work item whose
+//     LOD has 13 meshlets occupies 13 lanes instead of a 64-lane group;
+//   * visible meshlets are compacted deterministically in two launches without
+//     any device-side wait: the test kernel stores each warp's window ballots and
+//     the per-tile / per-warp visible counts; the emit kernel runs only for tiles
+//     with visible meshlets, sums the counts of the tiles before it, and writes
+//     each draw at slot = (visible meshlets before it in (work item, lane) order).
 //     The reference appends with atomicAdd (vg_cull.wgsl:247), so its order is
 //     unspecified; this order is reproducible and first_instance = slot.
 
@@ -96,13 +97,43 @@ __device__ __forceinline__ HelioInstanceCullData load_cull(const HelioInstanceCu
     return r;
 }
 
+// ── View constants (one warp per launch) ──────────────────────────────────────
+
+__global__ void __launch_bounds__(32) vg_view_setup_kernel(ViewSetupParams P) {
+    __shared__ Planes s_planes;
+    publish_planes_warp(P.camera->view_proj, s_planes);
+    if (threadIdx.x == 0) {
+        const HelioGpuCameraUniforms* cam = P.camera;
+        CullView v;
+        v.planes = s_planes;
+        v.vp = ldg_mat4(cam->view_proj);
+        v.pos_near = __ldg(reinterpret_cast<const float4*>(cam->position_near));
+        v.p00 = __ldg(&cam->proj[0]);
+        v.p11 = __ldg(&cam->proj[5]);
+        v.focal = fmul(fmul(fabsf(v.p11), (float)P.screen_height), 0.5f);
+        v.lod_threshold_px = P.lod_threshold_px;
+        v.hiz = P.hiz;
+        v.screen_height = P.screen_height;
+        v.hiz_mip_count = P.hiz_mip_count;
+        v.pad[0] = v.pad[1] = 0u;
+        *P.out = v;
+    }
+}
+
+// Cooperative copy of the view constants into shared memory (16-byte words).
+__device__ __forceinline__ void load_view(const CullView* src, CullView& dst, int tid, int nthreads) {
+    const uint4* s = reinterpret_cast<const uint4*>(src);
+    uint4* d = reinterpret_cast<uint4*>(&dst);
+    for (int k = tid; k < (int)(sizeof(CullView) / 16); k += nthreads) d[k] = __ldg(s + k);
+}
+
 // ── Object select: cs_select_objects (vg_cull.wgsl:282-352) ───────────────────
 
 __global__ void __launch_bounds__(256) vg_select_kernel(VgSelectParams P) {
-    __shared__ Planes s_planes;
-    const HelioGpuCameraUniforms* cam = P.camera;
-    if (threadIdx.x == 0) s_planes = publish_planes(cam->view_proj);
+    __shared__ CullView s_view;
+    load_view(P.view, s_view, threadIdx.x, blockDim.x);
     __syncthreads();
+    const Planes& s_planes = s_view.planes;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31;
     const VgSceneDev& S = P.scene;
@@ -110,32 +141,34 @@ __global__ void __launch_bounds__(256) vg_select_kernel(VgSelectParams P) {
     uint32_t selected = 0, lod_count = 0;
     if (i < S.object_count) {
         const HelioGpuVgObject* o = S.objects + i;
+        // One round trip for the object fields, one for the instance fields.
         const uint4 head = __ldg(reinterpret_cast<const uint4*>(o));  // instance_index, lod_count, max_meshlet_count, reserved
+        const float4 lb = __ldg(reinterpret_cast<const float4*>(o->local_bounds));
+        const float4 e0 = __ldg(reinterpret_cast<const float4*>(o->lod_errors));
+        const float4 e1 = __ldg(reinterpret_cast<const float4*>(o->lod_errors + 4));
         lod_count = min(head.y, 8u);
         const uint32_t ii = head.x;
         uint32_t sel = 0;
         if (lod_count > 0u && ii < S.instance_count) {
             const HelioInstanceCullData cd = load_cull(S.cull + ii);
+            const Mat4 model = ldg_mat4(S.instances[ii].model);
             if (cd.valid_transform != 0u) {
-                const float4 lb = __ldg(reinterpret_cast<const float4*>(o->local_bounds));
-                const Mat4 model = ldg_mat4(S.instances[ii].model);
                 const F3 c = mat4_point3(model, f3(lb.x, lb.y, lb.z));
                 const float wr = fmaxf(fmul(lb.w, cd.max_scale), 0.0f);
                 if (sphere_visible_vg(s_planes, c, wr)) {
-                    const float4 pn = __ldg(reinterpret_cast<const float4*>(cam->position_near));
+                    const float4 pn = s_view.pos_near;
                     const F3 d = sub3(c, f3(pn.x, pn.y, pn.z));
                     const float dist = fsqrt(dot3(d, d));
                     const float closest = fmaxf(fsub(dist, wr), fmaxf(pn.w, 1.0e-4f));
-                    const float focal = fmul(fmul(fabsf(__ldg(&cam->proj[5])), (float)P.screen_height), 0.5f);
-                    const float4 e0 = __ldg(reinterpret_cast<const float4*>(o->lod_errors));
-                    const float4 e1 = __ldg(reinterpret_cast<const float4*>(o->lod_errors + 4));
+                    const float focal = s_view.focal;
+                    const float thr = s_view.lod_threshold_px;
                     const float err[8] = {e0.x, e0.y, e0.z, e0.w, e1.x, e1.y, e1.z, e1.w};
                     uint32_t lod = 0;
 #pragma unroll
                     for (uint32_t level = 1; level < 8; ++level) {
                         if (level >= lod_count) break;
                         const float px = fdiv(fmul(fmul(err[level], cd.max_scale), focal), closest);
-                        if (px <= P.lod_threshold_px) lod = level;
+                        if (px <= thr) lod = level;
                         else break;
                     }
                     selected = lod;
@@ -168,17 +201,13 @@ __global__ void __launch_bounds__(256) vg_select_kernel(VgSelectParams P) {
 
 // ── Meshlet cull ──────────────────────────────────────────────────────────────
 
-struct CamState {
-    Mat4 vp;
-    float4 pos_near;
-    float p00, p11;
-};
-
 // cull_meshlet decision part (vg_cull.wgsl:143-240): true = emit a draw.
-__device__ __forceinline__ bool meshlet_visible(const VgSceneDev& S, const CamState& C, const Planes& pl,
-                                                const HizView& hz, uint32_t screen_h, uint32_t hiz_mip_count,
-                                                uint32_t mi, const Mat4& model, const HelioInstanceCullData& cd,
+__device__ __forceinline__ bool meshlet_visible(const VgSceneDev& S, const CullView& C, uint32_t mi,
+                                                const Mat4& model, const HelioInstanceCullData& cd,
                                                 const HelioGpuInstanceData* inst) {
+    const Planes& pl = C.planes;
+    const HizView& hz = C.hiz;
+    const uint32_t screen_h = C.screen_height, hiz_mip_count = C.hiz_mip_count;
     if (cd.valid_transform == 0u) return false;
     const float4 b = __ldg(S.m_bounds + mi);
     const F3 c = mat4_point3(model, f3(b.x, b.y, b.z));
@@ -249,163 +278,153 @@ __device__ __forceinline__ int owner_lane(uint32_t off, uint32_t s) {
     return lo;
 }
 
-constexpr unsigned long long kFlagAgg = 1ull << 62;
-constexpr unsigned long long kFlagIncl = 2ull << 62;
-constexpr int kBitWordsPerWarp = 66;  // 64 windows of 32 slots (+2 so bit-field reads stay in bounds)
+// The 32 work items of one warp (lane = item): active meshlet range and packing offsets.
+struct WarpItems {
+    uint32_t n, first, inst, lod, off, total;
+};
 
-// Decoupled look-back executed by one full warp; returns the exclusive prefix of
-// `tile` and publishes its inclusive value. Waits are bounded: after kSpinLimit
-// polls the error word is set and 0 is returned (outputs are then invalid and the
-// host reports HELIO_ERR_TIMEOUT).
-__device__ uint32_t warp_lookback(unsigned long long* lb, uint32_t tile, uint32_t agg, uint32_t* err) {
+__device__ __forceinline__ WarpItems load_warp_items(const VgSceneDev& S, const SelRecord* sel, uint32_t w_idx) {
     const int lane = threadIdx.x & 31;
-    if (tile == 0) {
-        if (lane == 0) atomicExch(lb, kFlagIncl | agg);
-        return 0u;
-    }
-    if (lane == 0) atomicExch(lb + tile, kFlagAgg | agg);
-    uint32_t prefix = 0;
-    long long base = (long long)tile - 1;
-    uint32_t polls = 0;
-    while (true) {
-        const long long idx = base - lane;
-        const unsigned long long v = idx >= 0 ? __ldcv(lb + idx) : kFlagIncl;
-        const uint32_t flag = (uint32_t)(v >> 62);
-        const uint32_t incl = __ballot_sync(0xffffffffu, flag == 2u);
-        const uint32_t notready = __ballot_sync(0xffffffffu, flag == 0u);
-        const int first_incl = incl ? __ffs(incl) - 1 : 32;
-        const uint32_t needed = first_incl >= 31 ? 0xffffffffu : ((2u << first_incl) - 1u);
-        if (notready & needed) {
-            if (++polls > kSpinLimit) {
-                // Give up: flag the error and unblock the successors with this
-                // tile's own count; the outputs of this launch are invalid.
-                if (lane == 0) {
-                    atomicExch(err, kDevTimeout);
-                    atomicExch(lb + tile, kFlagIncl | agg);
-                }
-                return 0u;
-            }
-            __nanosleep(polls < 64 ? 32 : 256);
-            continue;
-        }
-        uint32_t contrib = (lane <= first_incl) ? (uint32_t)v : 0u;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) contrib += __shfl_xor_sync(0xffffffffu, contrib, o);
-        prefix += contrib;
-        if (first_incl < 32) break;
-        base -= 32;
-    }
-    if (lane == 0) atomicExch(lb + tile, kFlagIncl | (unsigned long long)(prefix + agg));
-    return prefix;
-}
-
-__global__ void __launch_bounds__(kCullWarps * 32) vg_cull_kernel(VgCullParams P) {
-    __shared__ Planes s_planes;
-    __shared__ CamState s_cam;
-    __shared__ uint32_t s_tile;
-    __shared__ uint32_t s_warp_cnt[kCullWarps];
-    __shared__ uint32_t s_prefix;
-    __shared__ uint32_t s_bits[kCullWarps][kBitWordsPerWarp];
-    __shared__ HizView s_hiz;
-
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const VgSceneDev& S = P.scene;
-    if (tid == 0) {
-        s_tile = atomicAdd(P.scratch.tile_counter, 1u);  // tiles are processed in ticket order
-        const HelioGpuCameraUniforms* cam = P.camera;
-        s_planes = publish_planes(cam->view_proj);
-        s_cam.vp = ldg_mat4(cam->view_proj);
-        s_cam.pos_near = __ldg(reinterpret_cast<const float4*>(cam->position_near));
-        s_cam.p00 = __ldg(&cam->proj[0]);
-        s_cam.p11 = __ldg(&cam->proj[5]);
-        copy_hiz(P.hiz, s_hiz);
-    }
-    for (int k = lane; k < kBitWordsPerWarp; k += 32) s_bits[warp][k] = 0u;
-    __syncthreads();
-    const uint32_t tile = s_tile;
-    const CamState C = s_cam;
-
-    // Each lane owns one work item.
-    const uint32_t w_idx = tile * kCullItemsPerTile + warp * 32 + lane;
-    uint32_t n = 0, first = 0, inst = 0, lod = 0;
+    WarpItems w{0u, 0u, 0u, 0u, 0u, 0u};
     if (w_idx < S.work_item_count) {
         const HelioGpuVgWorkItem it = S.items[w_idx];
         if (it.object_index < S.object_count) {
-            const SelRecord r = __ldg(P.sel + it.object_index);
+            const SelRecord r = __ldg(sel + it.object_index);
             if (r.w != 0u && it.local_meshlet_base < r.y) {
-                n = min(64u, r.y - it.local_meshlet_base);
-                first = r.x + it.local_meshlet_base;
-                inst = r.z;
-                lod = r.w - 1u;
+                w.n = min(64u, r.y - it.local_meshlet_base);
+                w.first = r.x + it.local_meshlet_base;
+                w.inst = r.z;
+                w.lod = r.w - 1u;
             }
         }
     }
-    // Exclusive scan of the active meshlet counts over the warp's 32 items.
-    uint32_t incl = n;
+    uint32_t incl = w.n;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
         const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
         if (lane >= o) incl += t;
     }
-    const uint32_t off = incl - n;
-    const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+    w.off = incl - w.n;
+    w.total = __shfl_sync(0xffffffffu, incl, 31);
+    return w;
+}
 
-    // Test windows of 32 packed slots.
+constexpr int kBitWordsPerWarp = kWindowsPerWarp + 2;  // +2 so bit-field reads stay in bounds
+
+__global__ void __launch_bounds__(kCullWarps * 32) vg_cull_test_kernel(VgCullParams P) {
+    __shared__ CullView s_view;
+    __shared__ uint32_t s_bits[kCullWarps][kBitWordsPerWarp];
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const VgSceneDev& S = P.scene;
+    const uint32_t tile = blockIdx.x;
+    for (int k = lane; k < kBitWordsPerWarp; k += 32) s_bits[warp][k] = 0u;
+    const uint32_t w_idx = tile * kCullItemsPerTile + warp * 32 + lane;
+    const WarpItems it = load_warp_items(S, P.sel, w_idx);
+
+    // View constants are staged only when some warp of the tile has work.
+    if (__syncthreads_or(it.total > 0u)) {
+        load_view(P.view, s_view, tid, blockDim.x);
+        __syncthreads();
+    }
+
     uint32_t warp_count = 0;
-    const uint32_t windows = (total + 31u) >> 5;
+    const uint32_t windows = (it.total + 31u) >> 5;
     for (uint32_t win = 0; win < windows; ++win) {
         const uint32_t s = win * 32u + lane;
-        const int j = owner_lane(off, s);
-        const uint32_t j_off = __shfl_sync(0xffffffffu, off, j);
-        const uint32_t j_first = __shfl_sync(0xffffffffu, first, j);
-        const uint32_t j_inst = __shfl_sync(0xffffffffu, inst, j);
+        const int j = owner_lane(it.off, s);
+        const uint32_t j_off = __shfl_sync(0xffffffffu, it.off, j);
+        const uint32_t j_first = __shfl_sync(0xffffffffu, it.first, j);
+        const uint32_t j_inst = __shfl_sync(0xffffffffu, it.inst, j);
         bool vis = false;
-        if (s < total) {
+        if (s < it.total) {
             const uint32_t mi = j_first + (s - j_off);
             if (mi < S.meshlet_count) {
                 const HelioGpuInstanceData* in = S.instances + j_inst;
                 const HelioInstanceCullData cd = load_cull(S.cull + j_inst);
                 const Mat4 model = ldg_mat4(in->model);
-                vis = meshlet_visible(S, C, s_planes, s_hiz, P.screen_height, P.hiz_mip_count, mi, model, cd, in);
+                vis = meshlet_visible(S, s_view, mi, model, cd, in);
             }
         }
         const uint32_t bits = __ballot_sync(0xffffffffu, vis);
         if (lane == 0) s_bits[warp][win] = bits;
         warp_count += __popc(bits);
     }
-    if (lane == 0) s_warp_cnt[warp] = warp_count;
-    __syncthreads();
-
-    // Tile aggregate and look-back.
-    if (warp == 0) {
-        uint32_t agg = 0;
-#pragma unroll
-        for (int w = 0; w < (int)kCullWarps; ++w) agg += s_warp_cnt[w];
-        const uint32_t prefix = warp_lookback(P.scratch.lookback, tile, agg, P.scratch.error_word);
-        if (lane == 0) {
-            s_prefix = prefix;
-            if (agg) {
-                atomicAdd(P.counters + 0, agg);
-                const unsigned long long end = (unsigned long long)prefix + agg;
-                const unsigned long long lo = prefix > P.capacity ? prefix : P.capacity;
-                if (end > lo) atomicAdd(P.counters + 1, (uint32_t)(end - lo));
-            }
+    __syncwarp();
+    const size_t wslot = (size_t)tile * kCullWarps + warp;
+    if (lane == 0) {
+        P.scratch.warp_counts[wslot] = warp_count;
+        if (warp_count) {
+            atomicAdd(P.scratch.tile_counts + tile, warp_count);
+            atomicAdd(P.counters + 0, warp_count);
         }
+    }
+    if (warp_count) {
+        for (uint32_t k = lane; k < windows; k += 32) P.scratch.bits[wslot * kWindowsPerWarp + k] = s_bits[warp][k];
+    }
+    // Per-work-item visibility words: bits [off, off + n) of the warp's window bits.
+    if (P.visibility && w_idx < S.work_item_count) {
+        uint32_t lo = 0, hi = 0;
+        if (it.n) {
+            const uint32_t w0 = it.off >> 5, sh = it.off & 31u;
+            const unsigned long long a = (unsigned long long)s_bits[warp][w0] |
+                                         ((unsigned long long)s_bits[warp][w0 + 1] << 32);
+            const unsigned long long c = s_bits[warp][w0 + 2];
+            unsigned long long field = sh ? ((a >> sh) | (c << (64 - sh))) : a;
+            if (it.n < 64) field &= (1ull << it.n) - 1ull;
+            lo = (uint32_t)field;
+            hi = (uint32_t)(field >> 32);
+        }
+        reinterpret_cast<uint2*>(P.visibility)[w_idx] = make_uint2(lo, hi);
+    }
+}
+
+__global__ void __launch_bounds__(kCullWarps * 32) vg_cull_emit_kernel(VgCullParams P) {
+    __shared__ uint32_t s_red[kCullWarps];
+    __shared__ uint32_t s_prefix;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint32_t tile = blockIdx.x;
+    const uint32_t count = P.scratch.tile_counts[tile];
+    if (count == 0u) return;  // uniform: the whole CTA leaves
+
+    // Exclusive prefix: visible meshlets of all earlier tiles.
+    uint32_t sum = 0;
+    for (uint32_t i = tid; i < tile; i += blockDim.x) sum += P.scratch.tile_counts[i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    if (lane == 0) s_red[warp] = sum;
+    __syncthreads();
+    if (tid == 0) {
+        uint32_t p = 0;
+#pragma unroll
+        for (int w = 0; w < (int)kCullWarps; ++w) p += s_red[w];
+        s_prefix = p;
+        const unsigned long long end = (unsigned long long)p + count;
+        const unsigned long long lo = p > P.capacity ? p : P.capacity;
+        if (end > lo) atomicAdd(P.counters + 1, (uint32_t)(end - lo));
     }
     __syncthreads();
 
-    // Emission in (work item, lane) order.
+    const size_t wslot0 = (size_t)tile * kCullWarps;
+    const uint32_t wc = P.scratch.warp_counts[wslot0 + warp];
+    if (wc == 0u) return;  // uniform per warp; no block barrier follows
     uint32_t base = s_prefix;
-    for (int w = 0; w < warp; ++w) base += s_warp_cnt[w];
+    for (int w = 0; w < warp; ++w) base += P.scratch.warp_counts[wslot0 + w];
+
+    const VgSceneDev& S = P.scene;
+    const uint32_t w_idx = tile * kCullItemsPerTile + warp * 32 + lane;
+    const WarpItems it = load_warp_items(S, P.sel, w_idx);
+    const uint32_t windows = (it.total + 31u) >> 5;
+    const uint32_t* wbits = P.scratch.bits + (wslot0 + warp) * kWindowsPerWarp;
     for (uint32_t win = 0; win < windows; ++win) {
-        const uint32_t bits = s_bits[warp][win];
+        const uint32_t bits = wbits[win];
         if (bits == 0u) continue;
         const uint32_t s = win * 32u + lane;
-        const int j = owner_lane(off, s);
-        const uint32_t j_off = __shfl_sync(0xffffffffu, off, j);
-        const uint32_t j_first = __shfl_sync(0xffffffffu, first, j);
-        const uint32_t j_inst = __shfl_sync(0xffffffffu, inst, j);
-        const uint32_t j_lod = __shfl_sync(0xffffffffu, lod, j);
+        const int j = owner_lane(it.off, s);
+        const uint32_t j_off = __shfl_sync(0xffffffffu, it.off, j);
+        const uint32_t j_first = __shfl_sync(0xffffffffu, it.first, j);
+        const uint32_t j_inst = __shfl_sync(0xffffffffu, it.inst, j);
+        const uint32_t j_lod = __shfl_sync(0xffffffffu, it.lod, j);
         if ((bits >> lane) & 1u) {
             const uint32_t slot = base + __popc(bits & ((1u << lane) - 1u));
             if (slot < P.capacity) {
@@ -422,22 +441,6 @@ __global__ void __launch_bounds__(kCullWarps * 32) vg_cull_kernel(VgCullParams P
         }
         base += __popc(bits);
     }
-
-    // Per-work-item visibility words: bits [off, off + n) of the warp's window bits.
-    if (P.visibility && w_idx < S.work_item_count) {
-        uint32_t lo = 0, hi = 0;
-        if (n) {
-            const uint32_t w0 = off >> 5, sh = off & 31u;
-            const unsigned long long a = (unsigned long long)s_bits[warp][w0] |
-                                         ((unsigned long long)s_bits[warp][w0 + 1] << 32);
-            const unsigned long long c = s_bits[warp][w0 + 2];
-            unsigned long long field = sh ? ((a >> sh) | (c << (64 - sh))) : a;
-            if (n < 64) field &= (1ull << n) - 1ull;
-            lo = (uint32_t)field;
-            hi = (uint32_t)(field >> 32);
-        }
-        reinterpret_cast<uint2*>(P.visibility)[w_idx] = make_uint2(lo, hi);
-    }
 }
 
 }  // namespace
@@ -447,8 +450,9 @@ void launch_pack_meshlets(const HelioGpuMeshletEntry* aos, uint32_t n, float4* b
     if (!n) return;
     uint32_t blocks = (n + 255u) / 256u;
     if (blocks > 148u * 16u) blocks = 148u * 16u;
+    helio_launch_begin("pack_meshlets", stream);
     pack_meshlets_kernel<<<blocks, 256, 0, stream>>>(aos, n, bounds, cone, axis, draw);
-    helio_note_launch();
+    helio_launch_end(stream);
 }
 
 void launch_instance_cull_data(const HelioGpuInstanceData* inst, uint32_t n, HelioInstanceCullData* out,
@@ -456,20 +460,32 @@ void launch_instance_cull_data(const HelioGpuInstanceData* inst, uint32_t n, Hel
     if (!n) return;
     uint32_t blocks = (n + 255u) / 256u;
     if (blocks > 148u * 16u) blocks = 148u * 16u;
+    helio_launch_begin("instance_cull_data", stream);
     instance_cull_data_kernel<<<blocks, 256, 0, stream>>>(inst, n, out);
-    helio_note_launch();
+    helio_launch_end(stream);
+}
+
+void launch_vg_view_setup(const ViewSetupParams& p, cudaStream_t stream) {
+    helio_launch_begin("vg_view_setup", stream);
+    vg_view_setup_kernel<<<1, 32, 0, stream>>>(p);
+    helio_launch_end(stream);
 }
 
 void launch_vg_select(const VgSelectParams& p, cudaStream_t stream) {
     if (!p.scene.object_count) return;
+    helio_launch_begin("vg_select", stream);
     vg_select_kernel<<<(p.scene.object_count + 255u) / 256u, 256, 0, stream>>>(p);
-    helio_note_launch();
+    helio_launch_end(stream);
 }
 
 void launch_vg_cull(const VgCullParams& p, cudaStream_t stream) {
     if (!p.num_tiles) return;
-    vg_cull_kernel<<<p.num_tiles, kCullWarps * 32, 0, stream>>>(p);
-    helio_note_launch();
+    helio_launch_begin("vg_cull_test", stream);
+    vg_cull_test_kernel<<<p.num_tiles, kCullWarps * 32, 0, stream>>>(p);
+    helio_launch_end(stream);
+    helio_launch_begin("vg_cull_emit", stream);
+    vg_cull_emit_kernel<<<p.num_tiles, kCullWarps * 32, 0, stream>>>(p);
+    helio_launch_end(stream);
 }
 
 }  // namespace helio

@@ -83,6 +83,20 @@ class InstanceCullData(C.Structure):
     _fields_ = [("max_scale", f32), ("min_scale", f32), ("cone_cull_enabled", u32), ("valid_transform", u32)]
 
 
+class KernelTiming(C.Structure):
+    _fields_ = [("name", C.c_char * 40), ("launches", u64), ("total_ms", C.c_double)]
+
+
+def profiler_collect() -> dict:
+    """{kernel name: (launches, total device ms)} accumulated since the last reset."""
+    lib = cull_lib()
+    n = u32(0)
+    check(lib.helio_profiler_collect(None, 0, C.byref(n)))
+    arr = (KernelTiming * max(n.value, 1))()
+    check(lib.helio_profiler_collect(C.cast(arr, vp), n.value, C.byref(n)))
+    return {arr[i].name.decode(): (int(arr[i].launches), float(arr[i].total_ms)) for i in range(n.value)}
+
+
 class HizConfig(C.Structure):
     _fields_ = [("width", u32), ("height", u32), ("flags", u32)]
 
@@ -132,6 +146,9 @@ CULL_EXPORTS = {
     "helio_last_error": (C.c_char_p, []),
     "helio_status_string": (C.c_char_p, [i32]),
     "helio_kernel_launch_count": (u64, []),
+    "helio_profiler_enable": (i32, [i32]),
+    "helio_profiler_collect": (i32, [vp, u32, C.POINTER(u32)]),
+    "helio_profiler_reset": (None, []),
     "helio_mip_levels": (u32, [u32, u32]),
     "helio_extract_frustum_planes": (None, [vp, vp]),
     "helio_instance_cull_data": (i32, [vp, u32, vp, vp]),

@@ -22,6 +22,51 @@ from . import native as N
 UINT64_MAX = (1 << 64) - 1
 
 
+LOD_LEVEL_COUNT = 8
+DEFAULT_MAX_PUBLISHED_MESHLETS = 262_144
+
+
+class VirtualGeometryDebugStats:
+    """Decoded VG counters (crates/helio-pass-virtual-geometry/src/lib.rs:30-67)."""
+
+    def __init__(self, visible_meshlets, rejected_meshlets, lod_object_counts, max_available_lod):
+        self.visible_meshlets = visible_meshlets
+        self.rejected_meshlets = rejected_meshlets
+        self.lod_object_counts = list(lod_object_counts)
+        self.max_available_lod = max_available_lod
+
+    @classmethod
+    def from_counters(cls, counters):
+        """None unless all 11 counters are present (the 2-counter layout has no histogram)."""
+        c = [int(x) for x in counters]
+        if len(c) < 11:
+            return None
+        return cls(c[0], c[1], c[2:10], min(c[10], LOD_LEVEL_COUNT - 1))
+
+    def visible_objects(self) -> int:
+        return sum(self.lod_object_counts)
+
+    def selected_lod_range(self):
+        nz = [i for i, n in enumerate(self.lod_object_counts) if n]
+        return (nz[0], nz[-1]) if nz else None
+
+
+class VirtualGeometryBudget:
+    """Publication budget (crates/helio-pass-virtual-geometry/src/lib.rs:78-117): 36 bytes
+    per published meshlet (20-byte indirect command + 16-byte GpuVgDraw) plus 11 counters."""
+
+    def __init__(self, max_published_meshlets: int = DEFAULT_MAX_PUBLISHED_MESHLETS):
+        if max_published_meshlets <= 0:
+            raise ValueError("virtual geometry publication budget must be non-zero")
+        self.max_published_meshlets = int(max_published_meshlets)
+
+    def publication_bytes(self) -> int:
+        return self.max_published_meshlets * 36 + 11 * 4
+
+    def clamp_draw_count(self, worst_case: int) -> int:
+        return min(int(worst_case), self.max_published_meshlets)
+
+
 class _CudaArray:
     """Zero-copy __cuda_array_interface__ view of library-owned device memory."""
 

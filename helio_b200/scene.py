@@ -220,6 +220,16 @@ def config(config_id: int, scale: float = 1.0, with_depth: bool = True, threads:
     raise ValueError(f"unknown config {config_id}")
 
 
+def work_items_for(objects) -> list:
+    """64-meshlet work spans of (object_index, max_meshlet_count) pairs, in order
+    (crates/helio/src/scene/virtual_geometry/rebuild.rs:45-58): one span per started
+    block of 64 meshlets of the largest LOD; an object without meshlets has none."""
+    out = []
+    for obj, max_count in objects:
+        out.extend((obj, base) for base in range(0, max_count, 64))
+    return out
+
+
 def frame_data(scene: Scene, buffer_version: int = 1, instance_version: int = 1, dirty=(0, 0),
                device: dict | None = None) -> N.VgFrameData:
     """VgFrameData over host arrays (or device tensors when `device` holds them)."""

@@ -177,6 +177,20 @@ const char* helio_status_string(int32_t status);
 /* Number of kernels this library has launched in this process (all contexts). */
 uint64_t helio_kernel_launch_count(void);
 
+/* GPU-side kernel profiler (reference: the GPU timestamp profiler,
+ * crates/helio-core/src/profiling/gpu.rs:106-155). While enabled, every kernel
+ * launch of this library is bracketed by CUDA events on its own stream;
+ * helio_profiler_collect synchronises those events and returns, per kernel
+ * name, the launch count and the summed device time. */
+typedef struct helio_kernel_timing {
+    char name[40];
+    uint64_t launches;
+    double total_ms;
+} helio_kernel_timing;
+int32_t helio_profiler_enable(int32_t enabled);
+int32_t helio_profiler_collect(helio_kernel_timing* out, uint32_t capacity, uint32_t* count);
+void helio_profiler_reset(void);
+
 /* mip_levels(w, h) = bit length of max(w, h), at least 1.
  * Reference: crates/helio-pass-hiz/src/lib.rs:376-379. */
 uint32_t helio_mip_levels(uint32_t width, uint32_t height);
@@ -368,8 +382,8 @@ int32_t helio_vg_execute(helio_vg_pass* pass, const HelioGpuCameraUniforms* came
 int32_t helio_vg_resize(helio_vg_pass* pass, uint32_t width, uint32_t height);
 int32_t helio_vg_set_lod_quality(helio_vg_pass* pass, uint32_t lod_quality);
 int32_t helio_vg_publish(const helio_vg_pass* pass, helio_vg_outputs* out);
-/* Device-side error word of the last execute (0 = none, else HELIO_ERR_TIMEOUT);
- * synchronises `stream`. */
+/* Synchronises `stream` and reports any asynchronous CUDA error of the queued
+ * work (the cull kernels themselves never wait on one another). */
 int32_t helio_vg_device_status(helio_vg_pass* pass, void* stream);
 void helio_vg_destroy(helio_vg_pass* pass);
 

@@ -160,6 +160,35 @@ uint32_t oracle_mip_levels(uint32_t w, uint32_t h) {
 
 uint32_t oracle_ceil_log2(float d) { return ceil_log2_exact(d); }
 
+int oracle_sphere_visible(const float planes[24], const float center[3], float radius) {
+    float p[6][4];
+    for (int i = 0; i < 24; ++i) p[i / 4][i % 4] = planes[i];
+    return vg_sphere_visible(p, v3(center[0], center[1], center[2]), radius, nullptr) ? 1 : 0;
+}
+
+// Loop of vg_cull.wgsl:323-337 (the shader form; lib.rs:205-234 restates it on the CPU
+// with an explicit max(closest, 1e-4), which the shader applies when forming `closest`).
+uint32_t oracle_select_lod(const float errors[8], uint32_t lod_count, float max_scale, float focal_px,
+                           float closest, float max_error_px) {
+    uint32_t selected = 0;
+    float denom = fmaxf(closest, 1.0e-4f);
+    for (uint32_t level = 1; level < std::min(lod_count, 8u); ++level) {
+        float err = ((errors[level] * max_scale) * focal_px) / denom;
+        if (err <= max_error_px) selected = level;
+        else break;
+    }
+    return selected;
+}
+
+int oracle_cone_reject(const float camera[3], const float apex[3], const float axis_ws[3], float cutoff) {
+    V3 cta = sub(v3(apex[0], apex[1], apex[2]), v3(camera[0], camera[1], camera[2]));
+    float ads = dot3(cta, cta);
+    if (!(ads > 1.0e-12f)) return 0;
+    return dot3(divs(cta, sqrtf(ads)), v3(axis_ws[0], axis_ws[1], axis_ws[2])) >= cutoff ? 1 : 0;
+}
+
+int oracle_hiz_occludes(float near_z, float hiz) { return near_z > hiz + 1.0f / 65536.0f ? 1 : 0; }
+
 // crates/helio-pass-indirect-dispatch/src/lib.rs:271-300 (CPU, len > 1e-10 guard).
 void oracle_extract_frustum_planes(const float vp[16], float planes[24]) {
     auto row = [&](int r, float out[4]) {

@@ -92,6 +92,17 @@ void oracle_vg_cull(const HelioGpuCameraUniforms* cam, const oracle_vg_uniforms*
                     HelioGpuVgDraw* draws, uint32_t* counters, uint32_t* visibility,
                     oracle_stats* st, int threads);
 
+/* Single decisions, for the reference's known-answer tests. */
+/* sphere_visible (vg_cull.wgsl:126-133) against six given planes. */
+int oracle_sphere_visible(const float planes[24], const float center[3], float radius);
+/* select_object_lod (crates/helio-pass-virtual-geometry/src/lib.rs:205-234 / vg_cull.wgsl:323-337). */
+uint32_t oracle_select_lod(const float errors[8], uint32_t lod_count, float max_scale, float focal_px,
+                           float closest, float max_error_px);
+/* Cone rejection of cull_meshlet (vg_cull.wgsl:174-181) with a world-space axis. */
+int oracle_cone_reject(const float camera[3], const float apex[3], const float axis_ws[3], float cutoff);
+/* Hi-Z occlusion decision: near_z > hiz + 1/65536 (occlusion_cull.wgsl:207-208). */
+int oracle_hiz_occludes(float near_z, float hiz);
+
 #ifdef __cplusplus
 }
 #endif

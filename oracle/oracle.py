@@ -77,8 +77,40 @@ def lib() -> C.CDLL:
         L.oracle_vg_cull.argtypes = [vp, C.POINTER(OracleVgUniforms), vp, vp, vp, vp, vp, vp, C.POINTER(Pyramid), vp,
                                      vp, vp, vp, C.POINTER(OracleStats), C.c_int]
         L.oracle_vg_cull.restype = None
+        fp = C.POINTER(C.c_float)
+        L.oracle_sphere_visible.argtypes = [fp, fp, f32]
+        L.oracle_sphere_visible.restype = C.c_int
+        L.oracle_select_lod.argtypes = [fp, u32, f32, f32, f32, f32]
+        L.oracle_select_lod.restype = u32
+        L.oracle_cone_reject.argtypes = [fp, fp, fp, f32]
+        L.oracle_cone_reject.restype = C.c_int
+        L.oracle_hiz_occludes.argtypes = [f32, f32]
+        L.oracle_hiz_occludes.restype = C.c_int
         _lib = L
     return _lib
+
+
+def _fa(values) -> C.Array:
+    values = [float(v) for v in values]
+    return (C.c_float * len(values))(*values)
+
+
+def sphere_visible(planes, center, radius) -> bool:
+    flat = [x for p in planes for x in p]
+    return bool(lib().oracle_sphere_visible(_fa(flat), _fa(center), radius))
+
+
+def select_lod(errors, lod_count, max_scale, focal, closest, max_error) -> int:
+    return int(lib().oracle_select_lod(_fa(list(errors) + [0.0] * (8 - len(errors))), lod_count, max_scale, focal,
+                                       closest, max_error))
+
+
+def cone_reject(camera, apex, axis, cutoff) -> bool:
+    return bool(lib().oracle_cone_reject(_fa(camera), _fa(apex), _fa(axis), cutoff))
+
+
+def hiz_occludes(near_z, hiz) -> bool:
+    return bool(lib().oracle_hiz_occludes(near_z, hiz))
 
 
 def _p(a) -> int:

@@ -81,3 +81,36 @@ def assert_vg_equal(g, o, counter_count=11):
     np.testing.assert_array_equal(g["visibility"], o["visibility"], err_msg="visibility bitmask")
     np.testing.assert_array_equal(g["indirect"], o["indirect"], err_msg="indirect args")
     np.testing.assert_array_equal(g["draws"], o["draws"], err_msg="draw metadata")
+
+
+def benchmark_scene(objects, per_object):
+    """The constant scene of crates/examples/meshlet_cull_benchmark.rs:468-560."""
+    from helio_b200 import native as N
+    from helio_b200 import scene as S
+
+    m = np.zeros(per_object, S.DT_MESHLET)
+    m["center"] = (0.0, 0.0, -10.0)
+    m["radius"] = 0.25
+    m["cone_apex"] = (0.0, 0.0, -10.0)
+    m["cone_cutoff"] = 2.0
+    m["cone_axis"] = (0.0, 0.0, 1.0)
+    m["index_count"] = 3
+    inst = np.zeros(objects, S.DT_INSTANCE)
+    inst["model"] = np.eye(4, dtype=np.float32).reshape(16)
+    inst["normal_mat"] = np.array([1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0], np.float32)
+    inst["bounds"] = (0.0, 0.0, -10.0, 1.0)
+    inst["lightmap_index"] = 0xFFFFFFFF
+    obj = np.zeros(objects, S.DT_OBJECT)
+    obj["instance_index"] = np.arange(objects)
+    obj["lod_count"] = 1
+    obj["max_meshlet_count"] = per_object
+    obj["local_bounds"] = (0.0, 0.0, -10.0, 1.0)
+    obj["lod_meshlet_counts"][:, 0] = per_object
+    spans = (per_object + 63) // 64
+    items = np.zeros(objects * spans, S.DT_ITEM)
+    items["object_index"] = np.repeat(np.arange(objects), spans)
+    items["local_meshlet_base"] = np.tile(np.arange(spans) * 64, objects)
+    cam = S.perspective((0, 0, 0), (0, 0, -1), (0, 1, 0), 60.0, 16 / 9, 0.1, 1000.0)
+    sc = S.Scene(m, obj, inst, items, np.zeros(objects, S.DT_AABB), np.zeros(objects, S.DT_DRAWCALL),
+                 objects * per_object, per_object)
+    return sc, S.View(cam, 1920, 1080, np.ones((1, 1), np.float32))

@@ -4,7 +4,7 @@ order; plus the reference benchmark's invariants and edge cases."""
 import numpy as np
 import pytest
 
-from helpers import assert_vg_equal, gpu_hiz, gpu_vg_view, oracle_vg_view, u32
+from helpers import assert_vg_equal, benchmark_scene as _benchmark_scene, gpu_hiz, gpu_vg_view, oracle_vg_view, u32
 
 pytestmark = pytest.mark.gpu
 
@@ -103,39 +103,6 @@ def test_vg_device_resident_upload_and_dirty_patch(cuda):
     g2 = gpu_vg_view(sc2, v, hz=g["hz"], vg_pass=vg, frame=S.frame_data(sc2, 7, 2, dirty=(lo, n)))
     o2 = oracle_vg_view(sc2, v, _levels(g["hz"]))
     assert_vg_equal(g2, o2)
-
-
-def _benchmark_scene(objects, per_object):
-    """The constant scene of crates/examples/meshlet_cull_benchmark.rs:468-560."""
-    from helio_b200 import native as N
-    from helio_b200 import scene as S
-
-    m = np.zeros(per_object, S.DT_MESHLET)
-    m["center"] = (0.0, 0.0, -10.0)
-    m["radius"] = 0.25
-    m["cone_apex"] = (0.0, 0.0, -10.0)
-    m["cone_cutoff"] = 2.0
-    m["cone_axis"] = (0.0, 0.0, 1.0)
-    m["index_count"] = 3
-    inst = np.zeros(objects, S.DT_INSTANCE)
-    inst["model"] = np.eye(4, dtype=np.float32).reshape(16)
-    inst["normal_mat"] = np.array([1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0], np.float32)
-    inst["bounds"] = (0.0, 0.0, -10.0, 1.0)
-    inst["lightmap_index"] = 0xFFFFFFFF
-    obj = np.zeros(objects, S.DT_OBJECT)
-    obj["instance_index"] = np.arange(objects)
-    obj["lod_count"] = 1
-    obj["max_meshlet_count"] = per_object
-    obj["local_bounds"] = (0.0, 0.0, -10.0, 1.0)
-    obj["lod_meshlet_counts"][:, 0] = per_object
-    spans = (per_object + 63) // 64
-    items = np.zeros(objects * spans, S.DT_ITEM)
-    items["object_index"] = np.repeat(np.arange(objects), spans)
-    items["local_meshlet_base"] = np.tile(np.arange(spans) * 64, objects)
-    cam = S.perspective((0, 0, 0), (0, 0, -1), (0, 1, 0), 60.0, 16 / 9, 0.1, 1000.0)
-    sc = S.Scene(m, obj, inst, items, np.zeros(objects, S.DT_AABB), np.zeros(objects, S.DT_DRAWCALL),
-                 objects * per_object, per_object)
-    return sc, S.View(cam, 1920, 1080, np.ones((1, 1), np.float32))
 
 
 @pytest.mark.parametrize("objects,per_object", [(1, 65536), (16, 4096), (1024, 64), (8192, 8)])
