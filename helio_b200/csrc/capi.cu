@@ -95,6 +95,12 @@ int32_t fail(int32_t code, const char* fmt, ...) {
     return code;
 }
 
+}  // namespace
+
+int32_t helio_report_error(int32_t code, const char* message) { return fail(code, "%s", message); }
+
+namespace {
+
 #define HELIO_CK(call)                                                                          \
     do {                                                                                        \
         cudaError_t e_ = (call);                                                                \

@@ -184,3 +184,5 @@ constexpr uint32_t kSpinLimit = 1u << 22;  // polls before a bounded wait gives 
 // event profiler (helio_profiler_*): every launch is bracketed by these two calls.
 void helio_launch_begin(const char* kernel, cudaStream_t stream);
 void helio_launch_end(cudaStream_t stream);
+// Records `message` as the calling thread's helio_last_error() and returns `code`.
+int32_t helio_report_error(int32_t code, const char* message);

@@ -106,6 +106,10 @@ class HizPyramid(C.Structure):
                 ("levels", vp * 12)]
 
 
+class HizViewInput(C.Structure):
+    _fields_ = [("depth", vp), ("width", u32), ("height", u32), ("pitch", u32), ("flags", u32)]
+
+
 class SceneBuffers(C.Structure):
     _fields_ = [("camera", vp), ("instances", vp), ("instance_count", u32), ("draw_calls", vp),
                 ("draw_count", u32), ("aabbs", vp), ("indirect", vp)]
@@ -158,6 +162,7 @@ CULL_EXPORTS = {
     "helio_hiz_resize": (i32, [vp, u32, u32]),
     "helio_hiz_publish": (i32, [vp, C.POINTER(HizPyramid)]),
     "helio_hiz_destroy": (None, [vp]),
+    "helio_hiz_build_noalloc": (i32, [u32, C.POINTER(HizViewInput), vp, C.c_size_t, C.POINTER(HizPyramid), vp]),
     "helio_indirect_dispatch_create": (i32, [vp, C.POINTER(vp)]),
     "helio_indirect_dispatch_prepare": (i32, [vp, C.POINTER(GpuCameraUniforms), u32]),
     "helio_indirect_dispatch_execute": (i32, [vp, C.POINTER(SceneBuffers), vp]),
