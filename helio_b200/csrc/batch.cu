@@ -1,0 +1,555 @@
+// batch.cu — one persistent, cooperative launch that culls every view of a batch
+// against one device-resident virtual-geometry scene.
+//
+// Per view the results are those of the single-view passes (HiZBuildPass, then
+// VirtualGeometryPass's object select and meshlet cull: crates/helio-pass-hiz/,
+// crates/helio-pass-virtual-geometry/shaders/vg_cull.wgsl:126-405), with the
+// draws of each view compacted in the canonical (object, span, lane) order. The
+// work of all views is shared as follows (phases separated by grid barriers):
+//
+//   0  view constants (planes, camera fields, pyramid descriptor), one warp per view
+//   1  Hi-Z tiles of every view  +  object select: each object is loaded once and
+//      tested against every view; per (view, object) the selected LOD + 1 is stored
+//      and per (view, 256-object chunk) the number of active 64-meshlet spans
+//   2  exclusive scan of the (view, chunk) span counts
+//   3  expansion into one list of active spans, view-major, each view padded to a
+//      multiple of 32 spans so every group of 32 spans belongs to one view
+//   4  meshlet tests: a warp takes a group of 32 spans and packs their meshlets
+//      densely into 32-lane windows (window ballots and per-group counts stored)
+//   5  exclusive scan of the group counts
+//   6  emission of each view's draws at slot = position in the view's order
+//
+// Grid barriers and the Hi-Z hand-off use bounded waits: a barrier that is not
+// released after kSpinLimit polls sets kBatchErrTimeout and lets the CTA go on,
+// so the launch always ends; the host then reports HELIO_ERR_TIMEOUT.
+
+#include "batch.h"
+#include "hiz_tile.cuh"
+#include "vg_device.cuh"
+
+namespace helio {
+
+namespace {
+
+struct SelView {
+    Planes planes;
+    float4 pos_near;
+    float focal, thr;
+    uint32_t pad[2];
+};
+static_assert(sizeof(SelView) == 128, "SelView layout");
+
+// Dynamic shared memory layout (bytes).
+constexpr size_t kSmSelViews = 0;                                            // SelView[kBatchMaxViews]
+constexpr size_t kSmSelCnt = kSmSelViews + sizeof(SelView) * kBatchMaxViews;  // u32[kBatchMaxViews]
+constexpr size_t kSmSelHist = kSmSelCnt + 4 * kBatchMaxViews;                 // u32[kBatchMaxViews][8]
+constexpr size_t kSmSelMax = kSmSelHist + 32 * kBatchMaxViews;                // u32[kBatchMaxViews]
+constexpr size_t kSmHizJob = kSmSelMax + 4 * kBatchMaxViews;                  // HizJob
+constexpr size_t kSmHizM3 = kSmHizJob + ((sizeof(HizJob) + 15) / 16) * 16;    // float[8][9]
+constexpr size_t kSmMisc = kSmHizM3 + 8 * 9 * 4;                              // u32[64]
+constexpr size_t kSmTotal = kSmMisc + 64 * 4;
+// Phases 2..6 reuse the region from offset 0.
+constexpr size_t kSmTestViews = 0;                                       // CullView per warp
+constexpr size_t kSmTestBits = kSmTestViews + sizeof(CullView) * 8;      // u32[8][66]
+constexpr int kBits = kWindowsPerWarp + 2;
+constexpr size_t kSmVStart = 0;                                          // u32[kBatchMaxViews + 1]
+static_assert(kSmTestBits + 8 * kBits * 4 <= kSmMisc, "test phase fits");
+
+__device__ __forceinline__ uint32_t ld_cg(const uint32_t* p) { return __ldcg(p); }
+
+// Grid barrier with a bounded wait (all CTAs are co-resident: cooperative launch).
+__device__ void grid_sync(const BatchParams& P) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile uint32_t* gen = P.barrier + 1;
+        const uint32_t g = *gen;
+        __threadfence();
+        if (atomicAdd(P.barrier, 1u) == gridDim.x - 1) {
+            P.barrier[0] = 0u;
+            __threadfence();
+            atomicAdd(P.barrier + 1, 1u);
+        } else {
+            uint32_t polls = 0;
+            while (*gen == g) {
+                if (++polls > kSpinLimit) {
+                    atomicOr(P.error, kBatchErrTimeout);
+                    break;
+                }
+                __nanosleep(polls < 256 ? 64 : 256);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ uint32_t warp_inclusive(uint32_t x) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += t;
+    }
+    return x;
+}
+
+// Sum over the CTA; every thread gets the result. s: 9 words of shared memory.
+__device__ uint32_t block_sum(uint32_t x, uint32_t* s) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    __syncthreads();
+    if (lane == 0) s[warp] = x;
+    __syncthreads();
+    uint32_t t = 0;
+#pragma unroll
+    for (int w = 0; w < (int)(kBatchThreads / 32); ++w) t += s[w];
+    return t;
+}
+
+// Exclusive scan over the CTA; `total` receives the CTA sum. s: 9 words.
+__device__ uint32_t block_exclusive(uint32_t x, uint32_t* s, uint32_t& total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t inc = warp_inclusive(x);
+    __syncthreads();
+    if (lane == 31) s[warp] = inc;
+    __syncthreads();
+    uint32_t before = 0;
+    total = 0;
+#pragma unroll
+    for (int w = 0; w < (int)(kBatchThreads / 32); ++w) {
+        const uint32_t t = s[w];
+        if (w < warp) before += t;
+        total += t;
+    }
+    return before + inc - x;
+}
+
+// out[i] = sum of in[0..i) for i <= n, over the whole grid (two grid barriers).
+__device__ void grid_exclusive_scan(const BatchParams& P, const uint32_t* in, uint32_t* out, uint32_t n,
+                                    uint32_t* s_tmp) {
+    const uint32_t G = gridDim.x, b = blockIdx.x, tid = threadIdx.x;
+    const uint32_t seg = (n + G - 1) / G;
+    const uint32_t b0 = min(n, b * seg), b1 = min(n, b0 + seg);
+    uint32_t sum = 0;
+    for (uint32_t i = b0 + tid; i < b1; i += kBatchThreads) sum += ld_cg(in + i);
+    sum = block_sum(sum, s_tmp);
+    if (tid == 0) P.seg_totals[b] = sum;
+    grid_sync(P);
+    uint32_t base = 0;
+    for (uint32_t k = tid; k < b; k += kBatchThreads) base += ld_cg(P.seg_totals + k);
+    base = block_sum(base, s_tmp);
+    for (uint32_t t0 = b0; t0 < b1; t0 += kBatchThreads) {
+        const uint32_t i = t0 + tid;
+        const uint32_t x = i < b1 ? ld_cg(in + i) : 0u;
+        uint32_t total;
+        const uint32_t ex = block_exclusive(x, s_tmp, total);
+        if (i < b1) out[i] = base + ex;
+        base += total;
+    }
+    if (b == G - 1 && tid == 0) out[n] = base;
+    grid_sync(P);
+}
+
+// ── Phase 0: view constants ──────────────────────────────────────────────────
+__device__ void phase_setup(const BatchParams& P) {
+    for (uint32_t v = blockIdx.x; v < P.view_count; v += gridDim.x) {
+        if (threadIdx.x >= 32) continue;
+        const BatchViewDev& V = P.views[v];
+        __shared__ Planes s_pl;
+        publish_planes_warp(V.camera.view_proj, s_pl);
+        if (threadIdx.x == 0) {
+            CullView c;
+            c.planes = s_pl;
+            c.vp = ldg_mat4(V.camera.view_proj);
+            c.pos_near = __ldg(reinterpret_cast<const float4*>(V.camera.position_near));
+            c.p00 = __ldg(&V.camera.proj[0]);
+            c.p11 = __ldg(&V.camera.proj[5]);
+            c.focal = fmul(fmul(fabsf(c.p11), (float)V.height), 0.5f);
+            c.lod_threshold_px = V.lod_threshold_px;
+            for (int l = 0; l < HELIO_HIZ_MAX_MIPS; ++l) {
+                c.hiz.levels[l] = V.hiz.levels[l];
+                c.hiz.width[l] = V.hiz.lw[l];
+                c.hiz.height[l] = V.hiz.lh[l];
+                c.hiz.pitch[l] = V.hiz.lpitch[l];
+            }
+            c.hiz.mip_count = V.hiz.mip_count;
+            c.screen_height = V.height;
+            c.hiz_mip_count = V.hiz_mip_count;
+            c.pad[0] = c.pad[1] = 0u;
+            P.cviews[v] = c;
+        }
+        __syncwarp();
+    }
+}
+
+// ── Phase 1a: one Hi-Z tile ───────────────────────────────────────────────────
+__device__ void phase_hiz_tile(const BatchParams& P, uint32_t tile, char* sm) {
+    HizJob& J = *reinterpret_cast<HizJob*>(sm + kSmHizJob);
+    uint32_t* s_job = reinterpret_cast<uint32_t*>(sm + kSmMisc);
+    __syncthreads();  // the previous unit's warp 0 may still read s_m3 / J
+    if (threadIdx.x == 0) {
+        uint32_t lo = 0, hi = P.view_count - 1;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi + 1) >> 1;
+            if (P.views[mid].hiz.tile_begin <= tile) lo = mid;
+            else hi = mid - 1;
+        }
+        J = P.views[lo].hiz;
+        *s_job = lo;
+    }
+    __syncthreads();
+    hiz_tile(J, *s_job, tile - J.tile_begin, P.hiz_tickets, reinterpret_cast<float(*)[9]>(sm + kSmHizM3));
+}
+
+// ── Phase 1b: object select against every view (vg_cull.wgsl:282-352) ────────
+__device__ void phase_select_chunk(const BatchParams& P, uint32_t chunk, char* sm) {
+    const SelView* s_sv = reinterpret_cast<const SelView*>(sm + kSmSelViews);
+    uint32_t* s_cnt = reinterpret_cast<uint32_t*>(sm + kSmSelCnt);
+    uint32_t* s_hist = reinterpret_cast<uint32_t*>(sm + kSmSelHist);
+    uint32_t* s_max = reinterpret_cast<uint32_t*>(sm + kSmSelMax);
+    const uint32_t V = P.view_count, tid = threadIdx.x;
+    __syncthreads();
+    for (uint32_t k = tid; k < V * 10u; k += kBatchThreads) {
+        if (k < V) s_cnt[k] = 0u;
+        else if (k < 9u * V) s_hist[k - V] = 0u;
+        else s_max[k - 9u * V] = 0u;
+    }
+    __syncthreads();
+    const VgSceneDev& S = P.scene;
+    const uint32_t o = chunk * kBatchChunk + tid;
+    if (o < S.object_count) {
+        const HelioGpuVgObject* obj = S.objects + o;
+        const uint4 head = __ldg(reinterpret_cast<const uint4*>(obj));
+        const float4 lb = __ldg(reinterpret_cast<const float4*>(obj->local_bounds));
+        const float4 e0 = __ldg(reinterpret_cast<const float4*>(obj->lod_errors));
+        const float4 e1 = __ldg(reinterpret_cast<const float4*>(obj->lod_errors + 4));
+        const uint4 c0 = __ldg(reinterpret_cast<const uint4*>(obj->lod_meshlet_counts));
+        const uint4 c1 = __ldg(reinterpret_cast<const uint4*>(obj->lod_meshlet_counts + 4));
+        const uint32_t lod_count = min(head.y, 8u), ii = head.x;
+        bool valid = false;
+        F3 c = f3(0.f, 0.f, 0.f);
+        float wr = 0.0f, max_scale = 0.0f;
+        if (lod_count > 0u && ii < S.instance_count) {
+            const HelioInstanceCullData cd = load_cull(S.cull + ii);
+            const Mat4 model = ldg_mat4(S.instances[ii].model);
+            if (cd.valid_transform != 0u) {
+                valid = true;
+                max_scale = cd.max_scale;
+                c = mat4_point3(model, f3(lb.x, lb.y, lb.z));
+                wr = fmaxf(fmul(lb.w, cd.max_scale), 0.0f);
+            }
+        }
+        const float err[8] = {e0.x, e0.y, e0.z, e0.w, e1.x, e1.y, e1.z, e1.w};
+        const uint32_t cnts[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
+        uint8_t* lod_col = P.lod + o;
+        for (uint32_t v = 0; v < V; ++v) {
+            uint32_t sel = 0;
+            if (valid && sphere_visible_vg(s_sv[v].planes, c, wr)) {
+                const float4 pn = s_sv[v].pos_near;
+                const F3 d = sub3(c, f3(pn.x, pn.y, pn.z));
+                const float dist = fsqrt(dot3(d, d));
+                const float closest = fmaxf(fsub(dist, wr), fmaxf(pn.w, 1.0e-4f));
+                const float focal = s_sv[v].focal, thr = s_sv[v].thr;
+                uint32_t lod = 0;
+#pragma unroll
+                for (uint32_t level = 1; level < 8; ++level) {
+                    if (level >= lod_count) break;
+                    const float px = fdiv(fmul(fmul(err[level], max_scale), focal), closest);
+                    if (px <= thr) lod = level;
+                    else break;
+                }
+                sel = lod + 1u;
+                const uint32_t spans = (cnts[lod] + 63u) >> 6;
+                if (spans) atomicAdd(s_cnt + v, spans);
+                atomicAdd(s_hist + v * 8u + lod, 1u);
+                atomicMax(s_max + v, lod_count);  // lod_count - 1 + 1: 0 means no visible object
+            }
+            lod_col[(size_t)v * S.object_count] = (uint8_t)sel;
+        }
+    }
+    __syncthreads();
+    for (uint32_t v = tid; v < V; v += kBatchThreads) {
+        P.chunk_counts[(size_t)v * P.object_chunks + chunk] = s_cnt[v];
+        uint32_t* counters = P.views[v].counters;
+        for (uint32_t l = 0; l < 8u; ++l)
+            if (s_hist[v * 8u + l]) atomicAdd(counters + 2 + l, s_hist[v * 8u + l]);
+        if (s_max[v]) atomicMax(counters + 10, s_max[v] - 1u);
+    }
+}
+
+// ── Phase 3: expansion into the view-major list of active spans ──────────────
+__device__ void phase_expand(const BatchParams& P, char* sm) {
+    uint32_t* s_vstart = reinterpret_cast<uint32_t*>(sm + kSmVStart);
+    uint32_t* s_tmp = reinterpret_cast<uint32_t*>(sm + kSmMisc);
+    const uint32_t V = P.view_count, C = P.object_chunks, tid = threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5;
+    // Padded first span of every view (a multiple of 32).
+    {
+        uint32_t padded = 0;
+        if (tid < V) {
+            const uint32_t a = ld_cg(P.chunk_offs + (size_t)tid * C), e = ld_cg(P.chunk_offs + (size_t)(tid + 1) * C);
+            padded = (e - a + 31u) & ~31u;
+        }
+        uint32_t total;
+        const uint32_t ex = block_exclusive(padded, s_tmp, total);
+        if (tid < V) s_vstart[tid] = ex;
+        if (tid == 0) s_vstart[V] = total;
+        __syncthreads();
+        if (blockIdx.x == 0)
+            for (uint32_t v = tid; v <= V; v += kBatchThreads) P.view_span_start[v] = s_vstart[v];
+        if (tid == 0 && total > P.span_capacity) atomicOr(P.error, kBatchErrSpanCapacity);
+    }
+    const VgSceneDev& S = P.scene;
+    const uint32_t n_units = V * C;
+    const uint32_t gw = blockIdx.x * (kBatchThreads / 32) + warp, GW = gridDim.x * (kBatchThreads / 32);
+    for (uint32_t base = gw * 32u; base < n_units; base += GW * 32u) {
+        const uint32_t u = base + lane;
+        const uint32_t cnt = u < n_units ? ld_cg(P.chunk_counts + u) : 0u;
+        uint32_t mask = __ballot_sync(0xffffffffu, cnt != 0u);
+        while (mask) {
+            const uint32_t uu = base + (__ffs(mask) - 1);
+            mask &= mask - 1u;
+            const uint32_t v = uu / C, ch = uu - v * C;
+            uint32_t pos = s_vstart[v] + (ld_cg(P.chunk_offs + uu) - ld_cg(P.chunk_offs + (size_t)v * C));
+            for (uint32_t r = 0; r < kBatchChunk / 32u; ++r) {
+                const uint32_t o = ch * kBatchChunk + r * 32u + lane;
+                uint32_t ns = 0, first = 0, count = 0, inst = 0, lod = 0;
+                if (o < S.object_count) {
+                    const uint32_t sel = __ldcg(P.lod + (size_t)v * S.object_count + o);
+                    if (sel) {
+                        lod = sel - 1u;
+                        const HelioGpuVgObject* obj = S.objects + o;
+                        count = __ldg(&obj->lod_meshlet_counts[lod]);
+                        first = __ldg(&obj->lod_first_meshlets[lod]);
+                        inst = __ldg(&obj->instance_index);
+                        ns = (count + 63u) >> 6;
+                    }
+                }
+                const uint32_t inc = warp_inclusive(ns);
+                const uint32_t total = __shfl_sync(0xffffffffu, inc, 31);
+                uint32_t p = pos + inc - ns;
+                for (uint32_t j = 0; j < ns; ++j, ++p) {
+                    if (p < P.span_capacity) {
+                        const uint32_t n = min(64u, count - 64u * j);
+                        P.spans[p] = make_uint4(first + 64u * j, n | (lod << 8) | (v << 16), inst, o);
+                    }
+                }
+                pos += total;
+            }
+        }
+    }
+    // Padding spans (n = 0) complete every view to a multiple of 32.
+    for (uint32_t v = blockIdx.x; v < V; v += gridDim.x) {
+        const uint32_t end = ld_cg(P.chunk_offs + (size_t)(v + 1) * C) - ld_cg(P.chunk_offs + (size_t)v * C);
+        for (uint32_t p = s_vstart[v] + end + tid; p < s_vstart[v + 1]; p += kBatchThreads)
+            if (p < P.span_capacity) P.spans[p] = make_uint4(0u, v << 16, 0u, 0u);
+    }
+}
+
+// The 32 spans of a group (lane = span): meshlet range and packing offsets.
+struct GroupSpans {
+    uint32_t n, first, inst, lod, off, total, view;
+};
+
+__device__ __forceinline__ GroupSpans load_group(const BatchParams& P, uint32_t g) {
+    const int lane = threadIdx.x & 31;
+    const ActiveSpan s = __ldcg(P.spans + (size_t)g * 32u + lane);
+    GroupSpans r;
+    r.n = span_n(s);
+    r.first = s.x;
+    r.inst = s.z;
+    r.lod = span_lod(s);
+    r.view = __shfl_sync(0xffffffffu, span_view(s), 0);
+    const uint32_t inc = warp_inclusive(r.n);
+    r.off = inc - r.n;
+    r.total = __shfl_sync(0xffffffffu, inc, 31);
+    return r;
+}
+
+// ── Phase 4: meshlet tests of every group of 32 spans ────────────────────────
+__device__ void phase_test(const BatchParams& P, uint32_t groups, char* sm) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    CullView& cv = *reinterpret_cast<CullView*>(sm + kSmTestViews + sizeof(CullView) * warp);
+    uint32_t* bits = reinterpret_cast<uint32_t*>(sm + kSmTestBits) + warp * kBits;
+    const VgSceneDev& S = P.scene;
+    uint32_t cached_view = 0xFFFFFFFFu;
+    const uint32_t gw = blockIdx.x * (kBatchThreads / 32) + warp, GW = gridDim.x * (kBatchThreads / 32);
+    for (uint32_t g = gw; g < groups; g += GW) {
+        const GroupSpans gs = load_group(P, g);
+        if (gs.view >= P.view_count) continue;  // never true: every span below the group count is written
+        if (gs.view != cached_view) {
+            const uint4* src = reinterpret_cast<const uint4*>(P.cviews + gs.view);
+            uint4* dst = reinterpret_cast<uint4*>(&cv);
+            for (int k = lane; k < (int)(sizeof(CullView) / 16); k += 32) dst[k] = __ldcg(src + k);
+            cached_view = gs.view;
+        }
+        for (int k = lane; k < kBits; k += 32) bits[k] = 0u;
+        __syncwarp();
+        uint32_t count = 0;
+        const uint32_t windows = (gs.total + 31u) >> 5;
+        for (uint32_t win = 0; win < windows; ++win) {
+            const uint32_t s = win * 32u + lane;
+            const int j = owner_lane(gs.off, s);
+            const uint32_t j_off = __shfl_sync(0xffffffffu, gs.off, j);
+            const uint32_t j_first = __shfl_sync(0xffffffffu, gs.first, j);
+            const uint32_t j_inst = __shfl_sync(0xffffffffu, gs.inst, j);
+            bool vis = false;
+            if (s < gs.total) {
+                const uint32_t mi = j_first + (s - j_off);
+                if (mi < S.meshlet_count) {
+                    const HelioGpuInstanceData* in = S.instances + j_inst;
+                    const HelioInstanceCullData cd = load_cull(S.cull + j_inst);
+                    const Mat4 model = ldg_mat4(in->model);
+                    vis = meshlet_visible<true>(S, cv, mi, model, cd, in);
+                }
+            }
+            const uint32_t b = __ballot_sync(0xffffffffu, vis);
+            if (lane == 0) bits[win] = b;
+            count += __popc(b);
+        }
+        __syncwarp();
+        if (lane == 0) P.group_counts[g] = count;
+        if (count)
+            for (uint32_t k = lane; k < windows; k += 32) P.group_bits[(size_t)g * kWindowsPerWarp + k] = bits[k];
+        if (P.span_vis) {
+            const uint2 w = bit_field64(bits, gs.off, gs.n);
+            reinterpret_cast<uint2*>(P.span_vis)[(size_t)g * 32u + lane] = w;
+        }
+        __syncwarp();
+    }
+}
+
+// ── Phase 6: emission, per view, in the canonical order ───────────────────────
+__device__ void phase_emit(const BatchParams& P, uint32_t groups) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const VgSceneDev& S = P.scene;
+    const uint32_t gw = blockIdx.x * (kBatchThreads / 32) + warp, GW = gridDim.x * (kBatchThreads / 32);
+    for (uint32_t base = gw * 32u; base < groups; base += GW * 32u) {
+        const uint32_t gl = base + lane;
+        const uint32_t cnt = gl < groups ? ld_cg(P.group_counts + gl) : 0u;
+        uint32_t mask = __ballot_sync(0xffffffffu, cnt != 0u);
+        while (mask) {
+            const uint32_t g = base + (__ffs(mask) - 1);
+            mask &= mask - 1u;
+            const GroupSpans gs = load_group(P, g);
+            if (gs.view >= P.view_count) continue;
+            const BatchViewDev& V = P.views[gs.view];
+            const uint32_t first_group = ld_cg(P.view_span_start + gs.view) >> 5;
+            const uint32_t count = ld_cg(P.group_counts + g);
+            uint32_t slot0 = ld_cg(P.group_offs + g) - ld_cg(P.group_offs + first_group);
+            const uint32_t cap = V.capacity;
+            if (lane == 0) {
+                atomicAdd(V.counters + 0, count);
+                const unsigned long long end = (unsigned long long)slot0 + count;
+                const unsigned long long lo = slot0 > cap ? slot0 : cap;
+                if (end > lo) atomicAdd(V.counters + 1, (uint32_t)(end - lo));
+            }
+            const uint32_t windows = (gs.total + 31u) >> 5;
+            const uint32_t* gbits = P.group_bits + (size_t)g * kWindowsPerWarp;
+            for (uint32_t win = 0; win < windows; ++win) {
+                const uint32_t b = ld_cg(gbits + win);
+                if (b == 0u) continue;
+                const uint32_t s = win * 32u + lane;
+                const int j = owner_lane(gs.off, s);
+                const uint32_t j_off = __shfl_sync(0xffffffffu, gs.off, j);
+                const uint32_t j_first = __shfl_sync(0xffffffffu, gs.first, j);
+                const uint32_t j_inst = __shfl_sync(0xffffffffu, gs.inst, j);
+                const uint32_t j_lod = __shfl_sync(0xffffffffu, gs.lod, j);
+                if ((b >> lane) & 1u) {
+                    const uint32_t slot = slot0 + __popc(b & ((1u << lane) - 1u));
+                    if (slot < cap) {
+                        const uint32_t mi = j_first + (s - j_off);
+                        const uint4 d = __ldg(S.m_draw + mi);
+                        uint32_t* out = reinterpret_cast<uint32_t*>(V.indirect + slot);
+                        out[0] = d.y;
+                        out[1] = 1u;
+                        out[2] = d.x;
+                        out[3] = d.z;
+                        out[4] = slot;
+                        reinterpret_cast<uint4*>(V.draws)[slot] = make_uint4(j_inst, mi, j_lod, 0u);
+                    }
+                }
+                slot0 += __popc(b);
+            }
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kBatchThreads, 3) batch_kernel(BatchParams P) {
+    extern __shared__ __align__(16) char sm[];
+    uint32_t* s_tmp = reinterpret_cast<uint32_t*>(sm + kSmMisc);
+
+    phase_setup(P);
+    grid_sync(P);
+
+    // Phase 1: Hi-Z tiles and object chunks share one work list.
+    {
+        SelView* s_sv = reinterpret_cast<SelView*>(sm + kSmSelViews);
+        for (uint32_t k = threadIdx.x; k < P.view_count; k += kBatchThreads) {
+            const CullView* cvp = P.cviews + k;
+            SelView sv;
+            const uint4* src = reinterpret_cast<const uint4*>(&cvp->planes);
+            uint4* dst = reinterpret_cast<uint4*>(&sv.planes);
+            for (int w = 0; w < 6; ++w) dst[w] = __ldcg(src + w);
+            sv.pos_near = __ldcg(&cvp->pos_near);
+            sv.focal = __ldcg(&cvp->focal);
+            sv.thr = __ldcg(&cvp->lod_threshold_px);
+            sv.pad[0] = sv.pad[1] = 0u;
+            s_sv[k] = sv;
+        }
+        __syncthreads();
+        const uint32_t units = P.hiz_tiles + P.object_chunks;
+        for (uint32_t u = blockIdx.x; u < units; u += gridDim.x) {
+            if (u < P.hiz_tiles) phase_hiz_tile(P, u, sm);
+            else phase_select_chunk(P, u - P.hiz_tiles, sm);
+        }
+    }
+    grid_sync(P);
+
+    grid_exclusive_scan(P, P.chunk_counts, P.chunk_offs, P.view_count * P.object_chunks, s_tmp);
+    phase_expand(P, sm);
+    grid_sync(P);
+
+    const uint32_t total_spans = min(ld_cg(P.view_span_start + P.view_count), P.span_capacity);
+    const uint32_t groups = total_spans >> 5;
+    phase_test(P, groups, sm);
+    grid_sync(P);
+
+    grid_exclusive_scan(P, P.group_counts, P.group_offs, groups, s_tmp);
+    phase_emit(P, groups);
+}
+
+}  // namespace
+
+size_t batch_dynamic_smem() { return kSmTotal; }
+
+uint32_t batch_max_grid() {
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaFuncSetAttribute(batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmTotal);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel, kBatchThreads, kSmTotal);
+    return (uint32_t)(sms * per_sm);
+}
+
+cudaError_t launch_batch(const BatchParams& p, uint32_t grid, cudaStream_t stream) {
+    cudaError_t e = cudaFuncSetAttribute(batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmTotal);
+    if (e != cudaSuccess) return e;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(kBatchThreads);
+    cfg.dynamicSmemBytes = kSmTotal;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    helio_launch_begin("batch_cull", stream);
+    e = cudaLaunchKernelEx(&cfg, batch_kernel, p);
+    helio_launch_end(stream);
+    return e;
+}
+
+}  // namespace helio

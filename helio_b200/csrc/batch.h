@@ -1,0 +1,72 @@
+// batch.h — the persistent multi-view visibility kernel (one cooperative launch
+// culls every view of a batch against one device-resident scene).
+#pragma once
+
+#include "common.cuh"
+#include "kernels.h"
+#include "vg.h"
+
+namespace helio {
+
+constexpr uint32_t kBatchMaxViews = 128;
+constexpr uint32_t kBatchThreads = 256;
+constexpr uint32_t kBatchChunk = 256;  // objects per select unit and per count chunk
+
+// Per view, in device memory; filled by the host except where noted. 16-byte
+// aligned: the camera matrices are read with 128-bit loads.
+struct alignas(16) BatchViewDev {
+    HelioGpuCameraUniforms camera;
+    HizJob hiz;
+    uint32_t width, height;
+    uint32_t hiz_mip_count;  // mip_levels(width, height), unclamped (rendering.rs:828-829)
+    float lod_threshold_px;
+    uint32_t capacity;       // publication capacity of this view
+    uint32_t pad;
+    HelioDrawIndexedIndirectArgs* indirect;  // [capacity]
+    HelioGpuVgDraw* draws;                   // [capacity]
+    uint32_t* counters;                      // [16]; layout of the VG counters
+};
+
+static_assert(sizeof(BatchViewDev) % 16 == 0, "view table entries stay 16-byte aligned");
+
+// An active span: up to 64 meshlets of the selected LOD of one object in one view.
+// x = first meshlet, y = n | lod << 8 | view << 16, z = instance, w = object.
+using ActiveSpan = uint4;
+
+__host__ __device__ inline uint32_t span_n(const ActiveSpan& s) { return s.y & 0x7Fu; }
+__host__ __device__ inline uint32_t span_lod(const ActiveSpan& s) { return (s.y >> 8) & 0xFu; }
+__host__ __device__ inline uint32_t span_view(const ActiveSpan& s) { return s.y >> 16; }
+
+enum : uint32_t { kBatchErrTimeout = 1u, kBatchErrSpanCapacity = 2u };
+
+struct BatchParams {
+    VgSceneDev scene;
+    BatchViewDev* views;      // [view_count]
+    CullView* cviews;         // [view_count], written by phase 0
+    uint8_t* lod;             // [view_count * object_count]: LOD + 1 per (view, object), 0 = culled
+    uint32_t view_count;
+    uint32_t object_chunks;   // ceil(object_count / kBatchChunk)
+    uint32_t hiz_tiles;       // Hi-Z tiles of all views
+    uint32_t* hiz_tickets;    // [view_count], zero before the launch
+    uint32_t* barrier;        // [2] arrival count (zero before the launch), generation
+    uint32_t* error;          // [1] kBatchErr* bits, zero before the launch
+    uint32_t* chunk_counts;   // [view_count * object_chunks] active spans per (view, chunk)
+    uint32_t* chunk_offs;     // [view_count * object_chunks + 1]
+    uint32_t* seg_totals;     // [gridDim.x]
+    uint32_t* view_span_start;  // [view_count + 1] first span of each view (views padded to 32)
+    ActiveSpan* spans;        // [span_capacity]
+    uint32_t span_capacity;   // multiple of 32
+    uint32_t* group_counts;   // [span_capacity / 32] visible meshlets per group of 32 spans
+    uint32_t* group_offs;     // [span_capacity / 32 + 1]
+    uint32_t* group_bits;     // [span_capacity / 32 * kWindowsPerWarp] window ballots
+    uint32_t* span_vis;       // [span_capacity * 2] per-span visibility words, or null
+};
+
+// Dynamic shared memory of the persistent kernel (bytes).
+size_t batch_dynamic_smem();
+// Launches the cooperative kernel with `grid` CTAs (all co-resident) on `stream`.
+cudaError_t launch_batch(const BatchParams& p, uint32_t grid, cudaStream_t stream);
+// Largest co-resident grid for this device.
+uint32_t batch_max_grid();
+
+}  // namespace helio

@@ -1,0 +1,354 @@
+// batch_api.cu — host side of the device-resident scene and of the batched
+// multi-view cull (include/helio_cull.h, "Batched multi-view culling").
+
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "batch.h"
+#include "host_util.h"
+#include "kernels.h"
+#include "vg.h"
+
+using helio::as_stream;
+using helio::DevBuf;
+
+struct helio_vg_scene {
+    DevBuf m_bounds, m_cone, m_axis, m_draw, objects, instances, cull, staging;
+    uint32_t meshlet_count = 0, object_count = 0;
+    uint64_t lod0_meshlets = 0, max_spans = 0, max_draw_count = 0;
+    uint64_t version = 0, instance_version = 0;
+    bool have = false;
+
+    helio::VgSceneDev dev() const {
+        helio::VgSceneDev s{};
+        s.m_bounds = m_bounds.as<float4>();
+        s.m_cone = m_cone.as<float4>();
+        s.m_axis = m_axis.as<float4>();
+        s.m_draw = m_draw.as<uint4>();
+        s.objects = objects.as<HelioGpuVgObject>();
+        s.instances = instances.as<HelioGpuInstanceData>();
+        s.cull = cull.as<HelioInstanceCullData>();
+        s.items = nullptr;
+        s.meshlet_count = meshlet_count;
+        s.object_count = object_count;
+        s.instance_count = object_count;
+        s.work_item_count = 0;
+        return s;
+    }
+};
+
+struct helio_batch {
+    helio_batch_config cfg{};
+    const helio_vg_scene* scene = nullptr;
+    uint32_t view_count = 0;
+    std::vector<helio::BatchViewDev> host_views;
+    DevBuf views, cviews, lod, levels, out_indirect, out_draws, clear, chunk_counts, chunk_offs, seg_totals,
+        view_span_start, spans, group_counts, group_offs, group_bits, span_vis;
+    size_t clear_bytes = 0;
+    uint32_t grid = 0, object_chunks = 0, hiz_tiles = 0, span_capacity = 0;
+    std::vector<size_t> out_offset;  // first draw of each view in out_indirect / out_draws
+    bool prepared = false;
+
+    uint32_t* counters(uint32_t v) const { return clear.as<uint32_t>() + 16u * v; }
+    uint32_t* tickets() const { return clear.as<uint32_t>() + 16u * view_count; }
+    uint32_t* barrier() const { return tickets() + view_count; }
+    uint32_t* error() const { return barrier() + 2; }
+};
+
+namespace {
+
+int32_t copy_in(void* dst, const void* src, size_t bytes, uint32_t memory, cudaStream_t s) {
+    if (!bytes) return HELIO_OK;
+    HELIO_ARG(src, "frame data array missing");
+    HELIO_CK(cudaMemcpyAsync(dst, src, bytes,
+                             memory == HELIO_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
+    return HELIO_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t helio_vg_scene_create(helio_vg_scene** out) {
+    HELIO_ARG(out, "null pointer");
+    *out = new (std::nothrow) helio_vg_scene();
+    return *out ? HELIO_OK : helio_fail(HELIO_ERR_RESOURCE, "out of host memory");
+}
+
+int32_t helio_vg_scene_upload(helio_vg_scene* sc, const helio_vg_frame_data* f, void* stream) {
+    HELIO_ARG(sc && f, "null pointer");
+    HELIO_ARG(f->memory == HELIO_MEM_HOST || f->memory == HELIO_MEM_DEVICE, "unknown memory space");
+    cudaStream_t s = as_stream(stream);
+    int32_t st;
+    if (!sc->have || f->buffer_version != sc->version) {
+        const size_t M = f->meshlet_count, O = f->object_count;
+        HELIO_CK(sc->m_bounds.ensure(M * 16));
+        HELIO_CK(sc->m_cone.ensure(M * 16));
+        HELIO_CK(sc->m_axis.ensure(M * 16));
+        HELIO_CK(sc->m_draw.ensure(M * 16));
+        HELIO_CK(sc->objects.ensure(O * sizeof(HelioGpuVgObject)));
+        HELIO_CK(sc->instances.ensure(O * sizeof(HelioGpuInstanceData)));
+        HELIO_CK(sc->cull.ensure(O * sizeof(HelioInstanceCullData)));
+        const HelioGpuMeshletEntry* aos = f->meshlets;
+        if (M) {
+            if (f->memory == HELIO_MEM_HOST) {
+                HELIO_CK(sc->staging.ensure(M * sizeof(HelioGpuMeshletEntry)));
+                if ((st = copy_in(sc->staging.ptr, f->meshlets, M * sizeof(HelioGpuMeshletEntry), f->memory, s)))
+                    return st;
+                aos = sc->staging.as<HelioGpuMeshletEntry>();
+            }
+            HELIO_ARG(aos, "meshlet array missing");
+            helio::launch_pack_meshlets(aos, (uint32_t)M, sc->m_bounds.as<float4>(), sc->m_cone.as<float4>(),
+                                        sc->m_axis.as<float4>(), sc->m_draw.as<uint4>(), s);
+            HELIO_CK(cudaGetLastError());
+        }
+        if ((st = copy_in(sc->objects.ptr, f->objects, O * sizeof(HelioGpuVgObject), f->memory, s))) return st;
+        if ((st = copy_in(sc->instances.ptr, f->instances, O * sizeof(HelioGpuInstanceData), f->memory, s)))
+            return st;
+        helio::launch_instance_cull_data(sc->instances.as<HelioGpuInstanceData>(), (uint32_t)O,
+                                         sc->cull.as<HelioInstanceCullData>(), s);
+        HELIO_CK(cudaGetLastError());
+        // Per-object span bound and LOD0 size, for capacities and the metric.
+        std::vector<HelioGpuVgObject> objs(O);
+        if (O) {
+            HELIO_CK(cudaMemcpyAsync(objs.data(), sc->objects.ptr, O * sizeof(HelioGpuVgObject),
+                                     cudaMemcpyDeviceToHost, s));
+        }
+        HELIO_CK(cudaStreamSynchronize(s));
+        if (f->memory == HELIO_MEM_HOST) sc->staging.release();
+        uint64_t lod0 = 0, spans = 0, maxd = 0;
+        for (const HelioGpuVgObject& o : objs) {
+            lod0 += o.lod_meshlet_counts[0];
+            uint32_t mx = 0;
+            for (uint32_t l = 0; l < HELIO_VG_LOD_LEVELS && l < o.lod_count; ++l)
+                mx = o.lod_meshlet_counts[l] > mx ? o.lod_meshlet_counts[l] : mx;
+            spans += (mx + 63u) / 64u;
+            maxd += mx;
+        }
+        sc->meshlet_count = f->meshlet_count;
+        sc->object_count = f->object_count;
+        sc->lod0_meshlets = lod0;
+        sc->max_spans = spans;
+        sc->max_draw_count = maxd;
+        sc->version = f->buffer_version;
+        sc->instance_version = f->instance_version;
+        sc->have = true;
+    } else if (f->instance_version != sc->instance_version) {
+        const uint64_t start = f->instance_dirty_start, count = f->instance_dirty_count;
+        HELIO_ARG(count > 0 && start + count <= sc->object_count, "invalid dirty instance range");
+        if ((st = copy_in(sc->instances.as<HelioGpuInstanceData>() + start, f->instances + start,
+                          count * sizeof(HelioGpuInstanceData), f->memory, s)))
+            return st;
+        helio::launch_instance_cull_data(sc->instances.as<HelioGpuInstanceData>() + start, (uint32_t)count,
+                                         sc->cull.as<HelioInstanceCullData>() + start, s);
+        HELIO_CK(cudaGetLastError());
+        sc->instance_version = f->instance_version;
+    }
+    return HELIO_OK;
+}
+
+int32_t helio_vg_scene_info_get(const helio_vg_scene* sc, helio_vg_scene_info* out) {
+    HELIO_ARG(sc && out, "null pointer");
+    out->meshlet_count = sc->meshlet_count;
+    out->object_count = sc->object_count;
+    out->lod0_meshlets = sc->lod0_meshlets;
+    out->max_spans = sc->max_spans;
+    out->device_bytes = sc->m_bounds.bytes + sc->m_cone.bytes + sc->m_axis.bytes + sc->m_draw.bytes +
+                        sc->objects.bytes + sc->instances.bytes + sc->cull.bytes;
+    return HELIO_OK;
+}
+
+void helio_vg_scene_destroy(helio_vg_scene* sc) { delete sc; }
+
+int32_t helio_batch_create(const helio_batch_config* cfg, helio_batch** out) {
+    HELIO_ARG(cfg && out, "null pointer");
+    HELIO_ARG(cfg->max_views >= 1 && cfg->max_views <= HELIO_BATCH_MAX_VIEWS, "max_views must be 1..128");
+    helio_batch* b = new (std::nothrow) helio_batch();
+    if (!b) return helio_fail(HELIO_ERR_RESOURCE, "out of host memory");
+    b->cfg = *cfg;
+    *out = b;
+    return HELIO_OK;
+}
+
+int32_t helio_batch_prepare(helio_batch* b, const helio_vg_scene* sc, uint32_t n, const helio_batch_view* views,
+                            void* stream) {
+    HELIO_ARG(b && sc && views, "null pointer");
+    HELIO_ARG(sc->have, "scene not uploaded");
+    HELIO_ARG(n >= 1 && n <= b->cfg.max_views, "view count must be 1..max_views");
+    cudaStream_t s = as_stream(stream);
+    b->prepared = false;
+    b->scene = sc;
+    b->view_count = n;
+    b->host_views.assign(n, helio::BatchViewDev{});
+
+    // Pyramids (one buffer for every view) and Hi-Z jobs.
+    std::vector<size_t> level_off(n);
+    size_t level_floats = 0;
+    uint32_t tiles = 0;
+    for (uint32_t v = 0; v < n; ++v) {
+        const helio_batch_view& in = views[v];
+        HELIO_ARG(in.depth && in.width > 0 && in.height > 0 && in.width <= 32768 && in.height <= 32768,
+                  "view depth missing or size out of 1..32768");
+        const uint32_t pitch = in.depth_pitch ? in.depth_pitch : in.width;
+        HELIO_ARG(pitch >= in.width, "depth pitch smaller than width");
+        helio::BatchViewDev& d = b->host_views[v];
+        const size_t need = helio::hiz_layout(in.width, in.height, pitch, (in.flags & HELIO_HIZ_ALIAS_MIP0) == 0u,
+                                              &d.hiz);
+        level_off[v] = level_floats;
+        level_floats += (need + 3u) & ~(size_t)3u;
+        d.hiz.tile_begin = tiles;
+        tiles += d.hiz.tiles_x * d.hiz.tiles_y;
+    }
+    HELIO_CK(b->levels.ensure(level_floats * sizeof(float)));
+    // Per-view outputs.
+    const uint64_t default_cap = sc->max_draw_count < HELIO_VG_DEFAULT_PUBLICATION_LIMIT
+                                     ? sc->max_draw_count
+                                     : (uint64_t)HELIO_VG_DEFAULT_PUBLICATION_LIMIT;
+    b->out_offset.assign(n + 1, 0);
+    for (uint32_t v = 0; v < n; ++v) {
+        const uint32_t cap = views[v].draw_capacity ? views[v].draw_capacity : (uint32_t)default_cap;
+        b->host_views[v].capacity = cap;
+        b->out_offset[v + 1] = b->out_offset[v] + (cap ? cap : 1);
+    }
+    HELIO_CK(b->out_indirect.ensure(b->out_offset[n] * sizeof(HelioDrawIndexedIndirectArgs)));
+    HELIO_CK(b->out_draws.ensure(b->out_offset[n] * sizeof(HelioGpuVgDraw)));
+    // Cleared region: counters (16 words per view) | Hi-Z tickets | barrier (2) | error (1).
+    b->clear_bytes = ((size_t)16 * n + n + 3) * sizeof(uint32_t);
+    HELIO_CK(b->clear.ensure(b->clear_bytes));
+    HELIO_CK(cudaMemsetAsync(b->clear.ptr, 0, b->clear_bytes, s));
+    // Scratch.
+    const uint32_t O = sc->object_count;
+    b->object_chunks = (O + helio::kBatchChunk - 1) / helio::kBatchChunk;
+    b->hiz_tiles = tiles;
+    uint64_t span_cap = b->cfg.max_spans ? b->cfg.max_spans : (uint64_t)n * sc->max_spans + 32ull * n;
+    span_cap = (span_cap + 31u) & ~31ull;
+    HELIO_ARG(span_cap <= 0x7FFFFFE0ull, "span capacity exceeds 2^31");
+    b->span_capacity = (uint32_t)span_cap;
+    const size_t units = (size_t)n * b->object_chunks;
+    const uint32_t groups = b->span_capacity / 32u;
+    b->grid = helio::batch_max_grid();
+    HELIO_ARG(b->grid > 0, "the batch kernel does not fit on this device");
+    HELIO_CK(b->views.ensure(n * sizeof(helio::BatchViewDev)));
+    HELIO_CK(b->cviews.ensure(n * sizeof(helio::CullView)));
+    HELIO_CK(b->lod.ensure((size_t)n * (O ? O : 1)));
+    HELIO_CK(b->chunk_counts.ensure((units + 1) * 4));
+    HELIO_CK(b->chunk_offs.ensure((units + 1) * 4));
+    HELIO_CK(b->seg_totals.ensure((size_t)b->grid * 4));
+    HELIO_CK(b->view_span_start.ensure((size_t)(n + 1) * 4));
+    HELIO_CK(b->spans.ensure((size_t)b->span_capacity * sizeof(helio::ActiveSpan)));
+    HELIO_CK(b->group_counts.ensure((size_t)(groups + 1) * 4));
+    HELIO_CK(b->group_offs.ensure((size_t)(groups + 1) * 4));
+    HELIO_CK(b->group_bits.ensure((size_t)(groups + 1) * helio::kWindowsPerWarp * 4));
+    if (b->cfg.flags & HELIO_BATCH_SPAN_VISIBILITY) HELIO_CK(b->span_vis.ensure((size_t)b->span_capacity * 8));
+    // View table.
+    for (uint32_t v = 0; v < n; ++v) {
+        const helio_batch_view& in = views[v];
+        helio::BatchViewDev& d = b->host_views[v];
+        d.camera = in.camera;
+        helio::hiz_assign(&d.hiz, in.depth, b->levels.as<float>() + level_off[v]);
+        d.width = in.width;
+        d.height = in.height;
+        d.hiz_mip_count = helio::host_mip_levels(in.width, in.height);
+        d.lod_threshold_px = in.lod_error_threshold_px > 0.0f ? in.lod_error_threshold_px : 2.0f;
+        d.indirect = b->out_indirect.as<HelioDrawIndexedIndirectArgs>() + b->out_offset[v];
+        d.draws = b->out_draws.as<HelioGpuVgDraw>() + b->out_offset[v];
+        d.counters = b->counters(v);
+    }
+    HELIO_CK(cudaMemcpyAsync(b->views.ptr, b->host_views.data(), n * sizeof(helio::BatchViewDev),
+                             cudaMemcpyHostToDevice, s));
+    HELIO_CK(cudaStreamSynchronize(s));
+    b->prepared = true;
+    return HELIO_OK;
+}
+
+int32_t helio_batch_set_cameras(helio_batch* b, uint32_t n, const HelioGpuCameraUniforms* cams, void* stream) {
+    HELIO_ARG(b && cams, "null pointer");
+    HELIO_ARG(b->prepared && n == b->view_count, "camera count differs from the prepared views");
+    cudaStream_t s = as_stream(stream);
+    for (uint32_t v = 0; v < n; ++v) {
+        b->host_views[v].camera = cams[v];
+        HELIO_CK(cudaMemcpyAsync(b->views.as<helio::BatchViewDev>() + v, &b->host_views[v].camera,
+                                 sizeof(HelioGpuCameraUniforms), cudaMemcpyHostToDevice, s));
+    }
+    return HELIO_OK;
+}
+
+int32_t helio_batch_execute(helio_batch* b, void* stream) {
+    HELIO_ARG(b, "null pointer");
+    if (!b->prepared) return helio_fail(HELIO_ERR_RESOURCE, "batch executed before prepare");
+    cudaStream_t s = as_stream(stream);
+    HELIO_CK(cudaMemsetAsync(b->clear.ptr, 0, b->clear_bytes, s));
+    if (b->scene->object_count == 0) return HELIO_OK;
+    helio::BatchParams P{};
+    P.scene = b->scene->dev();
+    P.views = b->views.as<helio::BatchViewDev>();
+    P.cviews = b->cviews.as<helio::CullView>();
+    P.lod = b->lod.as<uint8_t>();
+    P.view_count = b->view_count;
+    P.object_chunks = b->object_chunks;
+    P.hiz_tiles = b->hiz_tiles;
+    P.hiz_tickets = b->tickets();
+    P.barrier = b->barrier();
+    P.error = b->error();
+    P.chunk_counts = b->chunk_counts.as<uint32_t>();
+    P.chunk_offs = b->chunk_offs.as<uint32_t>();
+    P.seg_totals = b->seg_totals.as<uint32_t>();
+    P.view_span_start = b->view_span_start.as<uint32_t>();
+    P.spans = b->spans.as<helio::ActiveSpan>();
+    P.span_capacity = b->span_capacity;
+    P.group_counts = b->group_counts.as<uint32_t>();
+    P.group_offs = b->group_offs.as<uint32_t>();
+    P.group_bits = b->group_bits.as<uint32_t>();
+    P.span_vis = (b->cfg.flags & HELIO_BATCH_SPAN_VISIBILITY) ? b->span_vis.as<uint32_t>() : nullptr;
+    HELIO_CK(helio::launch_batch(P, b->grid, s));
+    return HELIO_OK;
+}
+
+int32_t helio_batch_get_view_outputs(const helio_batch* b, uint32_t v, helio_batch_view_outputs* out) {
+    HELIO_ARG(b && out, "null pointer");
+    HELIO_ARG(b->prepared && v < b->view_count, "view index out of range");
+    const helio::BatchViewDev& d = b->host_views[v];
+    std::memset(out, 0, sizeof(*out));
+    out->indirect = d.indirect;
+    out->draws = d.draws;
+    out->counters = d.counters;
+    out->lod = b->lod.as<uint8_t>() + (size_t)v * b->scene->object_count;
+    out->capacity = d.capacity;
+    out->object_count = b->scene->object_count;
+    out->pyramid.mip_count = d.hiz.mip_count;
+    for (uint32_t l = 0; l < d.hiz.mip_count; ++l) {
+        out->pyramid.width[l] = d.hiz.lw[l];
+        out->pyramid.height[l] = d.hiz.lh[l];
+        out->pyramid.pitch[l] = d.hiz.lpitch[l];
+        out->pyramid.levels[l] = d.hiz.levels[l];
+    }
+    return HELIO_OK;
+}
+
+int32_t helio_batch_get_spans(const helio_batch* b, helio_batch_span_list* out) {
+    HELIO_ARG(b && out, "null pointer");
+    HELIO_ARG(b->prepared, "batch not prepared");
+    out->spans = b->spans.as<uint32_t>();
+    out->visibility = (b->cfg.flags & HELIO_BATCH_SPAN_VISIBILITY) ? b->span_vis.as<uint32_t>() : nullptr;
+    out->view_span_start = b->view_span_start.as<uint32_t>();
+    out->span_capacity = b->span_capacity;
+    out->view_count = b->view_count;
+    return HELIO_OK;
+}
+
+int32_t helio_batch_status(helio_batch* b, void* stream) {
+    HELIO_ARG(b, "null pointer");
+    if (!b->prepared) return HELIO_OK;
+    uint32_t err = 0;
+    HELIO_CK(cudaMemcpyAsync(&err, b->error(), 4, cudaMemcpyDeviceToHost, as_stream(stream)));
+    HELIO_CK(cudaStreamSynchronize(as_stream(stream)));
+    if (err & helio::kBatchErrTimeout) return helio_fail(HELIO_ERR_TIMEOUT, "a grid barrier of the batch timed out");
+    if (err & helio::kBatchErrSpanCapacity)
+        return helio_fail(HELIO_ERR_CAPACITY, "active spans exceeded the batch's max_spans; outputs incomplete");
+    return HELIO_OK;
+}
+
+void helio_batch_destroy(helio_batch* b) { delete b; }
+
+}  // extern "C"

@@ -15,6 +15,7 @@
 #include <string>
 
 #include "common.cuh"
+#include "host_util.h"
 #include "instance_cull.h"
 #include "kernels.h"
 #include "vg.h"
@@ -99,53 +100,21 @@ int32_t fail(int32_t code, const char* fmt, ...) {
 
 int32_t helio_report_error(int32_t code, const char* message) { return fail(code, "%s", message); }
 
+int32_t helio_fail(int32_t code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    return fail(code, "%s", buf);
+}
+
+using helio::as_stream;
+using helio::DevBuf;
+
 namespace {
 
-#define HELIO_CK(call)                                                                          \
-    do {                                                                                        \
-        cudaError_t e_ = (call);                                                                \
-        if (e_ != cudaSuccess) return fail(HELIO_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
-    } while (0)
-
-#define HELIO_ARG(cond, msg)                                     \
-    do {                                                         \
-        if (!(cond)) return fail(HELIO_ERR_INVALID_ARG, "%s", msg); \
-    } while (0)
-
-inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
-
-// Owned device allocation with grow-only semantics.
-struct DevBuf {
-    void* ptr = nullptr;
-    size_t bytes = 0;
-    ~DevBuf() { release(); }
-    void release() {
-        if (ptr) cudaFree(ptr);
-        ptr = nullptr;
-        bytes = 0;
-    }
-    cudaError_t ensure(size_t need) {
-        if (need <= bytes && ptr) return cudaSuccess;
-        release();
-        if (need == 0) need = 16;
-        cudaError_t e = cudaMalloc(&ptr, need);
-        if (e == cudaSuccess) bytes = need;
-        return e;
-    }
-    template <typename T>
-    T* as() const {
-        return reinterpret_cast<T*>(ptr);
-    }
-};
-
-uint32_t mip_levels(uint32_t w, uint32_t h) {
-    uint32_t m = w > h ? w : h, bits = 0;
-    while (m) {
-        ++bits;
-        m >>= 1;
-    }
-    return bits ? bits : 1u;
-}
+uint32_t mip_levels(uint32_t w, uint32_t h) { return helio::host_mip_levels(w, h); }
 
 helio::HizView to_view(const helio_hiz_pyramid& p) {
     helio::HizView v{};

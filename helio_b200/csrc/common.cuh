@@ -102,6 +102,9 @@ __device__ __forceinline__ void copy_hiz(const HizView& src, HizView& dst) {
     dst.mip_count = src.mip_count;
 }
 
+// kCoherent: the pyramid was written earlier in the same launch, so it is read
+// through L2 (ld.global.cg) instead of the read-only path.
+template <bool kCoherent = false>
 __device__ __forceinline__ float hiz_sample(const HizView& hz, float u, float v, uint32_t mip) {
     uint32_t l = min(mip, hz.mip_count - 1u);
     uint32_t w = hz.width[l], h = hz.height[l];
@@ -110,7 +113,8 @@ __device__ __forceinline__ float hiz_sample(const HizView& hz, float u, float v,
     int iy = (int)floorf(fmul(v, (float)h));
     ix = min(max(ix, 0), (int)w - 1);
     iy = min(max(iy, 0), (int)h - 1);
-    return __ldg(hz.levels[l] + (size_t)iy * hz.pitch[l] + ix);
+    const float* p = hz.levels[l] + (size_t)iy * hz.pitch[l] + ix;
+    return kCoherent ? __ldcg(p) : __ldg(p);
 }
 
 // Frustum planes as published by vg_cull.wgsl:266-280 (GPU form, no length guard).

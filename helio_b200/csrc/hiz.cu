@@ -1,103 +1,17 @@
 // hiz.cu — fused multi-level Hi-Z pyramid build (HiZBuildPass).
 //
-// Reference: crates/helio-pass-hiz/shaders/hiz_depth_copy.wgsl:13-19 (level 0 copy)
-// and hiz_build.wgsl:12-23 (one dispatch per level; dst = max(1, dim >> (m+1));
-// the +1 neighbours are clamped to src_size - 1, so odd sizes drop the last
-// row / column). The reference runs mip_count dispatches separated by barriers
-// (crates/helio-pass-hiz/src/lib.rs:503-531); here one launch builds every level:
-//
-//   * a CTA owns a 64x64 tile of level 0: each thread loads a 4x4 block with
-//     128-bit loads, reduces it in registers to levels 1 and 2, warp shuffles give
-//     level 3, shared memory + one warp give levels 4..6;
-//   * the last CTA of a view to finish (atomic ticket after a fence) builds the
-//     remaining levels 7.. from level 6 in shared memory.
-//
-// Every level-l texel is exactly max() over a rectangle of level 0 (max is exact),
-// and each 2x2 step applies the reference's clamp rule (a source dimension of 1
-// reuses the same texel), so the result is bit-identical to the per-level chain.
+// The reference runs one depth-copy dispatch and then mip_count-1 dispatches
+// separated by barriers (crates/helio-pass-hiz/src/lib.rs:503-531). Here one launch
+// builds every level of one or several views: one CTA per 64x64 tile of level 0
+// (hiz_tile.cuh), and the last CTA of each view finishes the levels above 6.
 
 #include "common.cuh"
+#include "hiz_tile.cuh"
 #include "kernels.h"
 
 namespace helio {
 
 namespace {
-
-// One 2x2 step of hiz_build.wgsl: a=(2x,2y) b=(2x+1,2y) c=(2x,2y+1) d=(2x+1,2y+1);
-// a source dimension of 1 clamps the +1 neighbour back onto the same texel.
-__device__ __forceinline__ float red4(float a, float b, float c, float d, bool xc, bool yc) {
-    if (xc) {
-        b = a;
-        d = c;
-    }
-    if (yc) {
-        c = a;
-        d = b;
-    }
-    return fmaxf(fmaxf(a, b), fmaxf(c, d));
-}
-
-constexpr int kTailBuf = 2304;  // floats per shared tail buffer
-
-// Levels 7.. of one pyramid, built by one warp (lane = threadIdx.x & 31) of the
-// CTA that finished the view's last tile. A source level that lives only in
-// global memory is read in batches of 8 texels per lane (32 loads in flight);
-// levels that fit are kept in shared memory for the next step.
-__device__ void hiz_tail_warp(const HizJob& J) {
-    __shared__ float bufA[kTailBuf];
-    __shared__ float bufB[kTailBuf];
-    const uint32_t lane = threadIdx.x & 31u;
-    float* cur = nullptr;  // shared copy of the current source level (or null)
-    float* nxt = bufA;
-    for (uint32_t l = 7; l < J.mip_count; ++l) {
-        const uint32_t sw = J.lw[l - 1], sh = J.lh[l - 1], sp = J.lpitch[l - 1];
-        const uint32_t dw = J.lw[l], dh = J.lh[l], dp = J.lpitch[l];
-        const float* __restrict__ src = J.levels[l - 1];
-        float* __restrict__ dst = J.levels[l];
-        const uint32_t n = dw * dh;
-        const bool fits = (size_t)n <= (size_t)kTailBuf;
-        for (uint32_t base = lane; base < n; base += 32u * 8u) {
-            float s[8][4];
-#pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                const uint32_t i = base + 32u * j;
-                if (i < n) {
-                    const uint32_t y = i / dw, x = i - y * dw;
-                    const uint32_t x0 = 2 * x, y0 = 2 * y;
-                    const uint32_t x1 = min(x0 + 1, sw - 1), y1 = min(y0 + 1, sh - 1);
-                    if (cur) {
-                        s[j][0] = cur[y0 * sw + x0];
-                        s[j][1] = cur[y0 * sw + x1];
-                        s[j][2] = cur[y1 * sw + x0];
-                        s[j][3] = cur[y1 * sw + x1];
-                    } else {
-                        s[j][0] = __ldcg(src + (size_t)y0 * sp + x0);
-                        s[j][1] = __ldcg(src + (size_t)y0 * sp + x1);
-                        s[j][2] = __ldcg(src + (size_t)y1 * sp + x0);
-                        s[j][3] = __ldcg(src + (size_t)y1 * sp + x1);
-                    }
-                }
-            }
-#pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                const uint32_t i = base + 32u * j;
-                if (i < n) {
-                    const uint32_t y = i / dw, x = i - y * dw;
-                    const float v = fmaxf(fmaxf(s[j][0], s[j][1]), fmaxf(s[j][2], s[j][3]));
-                    dst[(size_t)y * dp + x] = v;
-                    if (fits) nxt[i] = v;
-                }
-            }
-        }
-        __syncwarp();
-        if (fits) {
-            cur = nxt;
-            nxt = (nxt == bufA) ? bufB : bufA;
-        } else {
-            cur = nullptr;
-        }
-    }
-}
 
 // `single` is used when jobs == nullptr (one view, job passed by value);
 // otherwise jobs[] holds n_jobs views. The job is copied to shared memory so
@@ -108,8 +22,7 @@ __global__ void __launch_bounds__(256) hiz_build_kernel(HizJob single, const Hiz
     __shared__ HizJob s_J;
     __shared__ uint32_t s_job;
     const uint32_t tile = blockIdx.x;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    if (tid == 0) {
+    if (threadIdx.x == 0) {
         uint32_t lo = 0;
         if (jobs) {
             uint32_t hi = n_jobs - 1;
@@ -125,149 +38,7 @@ __global__ void __launch_bounds__(256) hiz_build_kernel(HizJob single, const Hiz
         s_job = lo;
     }
     __syncthreads();
-    const HizJob& J = s_J;
-    const uint32_t local = tile - J.tile_begin;
-    const uint32_t tile_y = local / J.tiles_x, tile_x = local - tile_y * J.tiles_x;
-    const uint32_t X0 = tile_x * kHizTile, Y0 = tile_y * kHizTile;
-    const uint32_t W = J.lw[0], H = J.lh[0];
-    const int tx4 = lane & 15, ty4 = warp * 2 + (lane >> 4);
-    const uint32_t bx = X0 + 4 * tx4, by = Y0 + 4 * ty4;
-
-    // Level 0: 4x4 block per thread.
-    float v[4][4];
-    const bool aligned = ((J.depth_pitch & 3u) == 0u) && ((reinterpret_cast<uintptr_t>(J.depth) & 15u) == 0u);
-    if (aligned && bx + 4 <= W && by + 4 <= H) {
-#pragma unroll
-        for (int r = 0; r < 4; ++r) {
-            float4 q = __ldcs(reinterpret_cast<const float4*>(J.depth + (size_t)(by + r) * J.depth_pitch + bx));
-            v[r][0] = q.x;
-            v[r][1] = q.y;
-            v[r][2] = q.z;
-            v[r][3] = q.w;
-        }
-    } else {
-#pragma unroll
-        for (int r = 0; r < 4; ++r)
-#pragma unroll
-            for (int c = 0; c < 4; ++c)
-                v[r][c] = (bx + c < W && by + r < H) ? __ldcs(J.depth + (size_t)(by + r) * J.depth_pitch + bx + c) : 0.0f;
-    }
-    if (J.copy_mip0) {
-        float* L0 = J.levels[0];
-        const uint32_t p0 = J.lpitch[0];
-        const bool al0 = ((p0 & 3u) == 0u) && ((reinterpret_cast<uintptr_t>(L0) & 15u) == 0u);
-#pragma unroll
-        for (int r = 0; r < 4; ++r) {
-            if (by + r >= H) break;
-            float* row = L0 + (size_t)(by + r) * p0 + bx;
-            if (al0 && bx + 4 <= W) {
-                *reinterpret_cast<float4*>(row) = make_float4(v[r][0], v[r][1], v[r][2], v[r][3]);
-            } else {
-#pragma unroll
-                for (int c = 0; c < 4; ++c)
-                    if (bx + c < W) row[c] = v[r][c];
-            }
-        }
-    }
-    if (J.mip_count <= 1) return;
-
-    // Level 1: 2x2 per thread.
-    float m1[2][2];
-    {
-        const bool xc = J.lw[0] == 1u, yc = J.lh[0] == 1u;
-#pragma unroll
-        for (int j = 0; j < 2; ++j)
-#pragma unroll
-            for (int i = 0; i < 2; ++i)
-                m1[j][i] = red4(v[2 * j][2 * i], v[2 * j][2 * i + 1], v[2 * j + 1][2 * i], v[2 * j + 1][2 * i + 1], xc, yc);
-        const uint32_t x1 = (X0 >> 1) + 2 * tx4, y1 = (Y0 >> 1) + 2 * ty4;
-        float* L1 = J.levels[1];
-        const uint32_t p1 = J.lpitch[1];
-#pragma unroll
-        for (int j = 0; j < 2; ++j) {
-            if (y1 + j >= J.lh[1]) break;
-            float* row = L1 + (size_t)(y1 + j) * p1 + x1;
-            if (x1 + 2 <= J.lw[1] && ((p1 & 1u) == 0u)) {
-                *reinterpret_cast<float2*>(row) = make_float2(m1[j][0], m1[j][1]);
-            } else {
-                if (x1 < J.lw[1]) row[0] = m1[j][0];
-                if (x1 + 1 < J.lw[1]) row[1] = m1[j][1];
-            }
-        }
-    }
-    if (J.mip_count <= 2) return;
-
-    // Level 2: one texel per thread.
-    const float m2 = red4(m1[0][0], m1[0][1], m1[1][0], m1[1][1], J.lw[1] == 1u, J.lh[1] == 1u);
-    {
-        const uint32_t x2 = (X0 >> 2) + tx4, y2 = (Y0 >> 2) + ty4;
-        if (x2 < J.lw[2] && y2 < J.lh[2]) J.levels[2][(size_t)y2 * J.lpitch[2] + x2] = m2;
-    }
-    if (J.mip_count <= 3) return;
-
-    // Level 3: 2x2 across lanes (x: lane^1, y: lane^16).
-    {
-        float b = __shfl_xor_sync(0xffffffffu, m2, 1);
-        float c = __shfl_xor_sync(0xffffffffu, m2, 16);
-        float d = __shfl_xor_sync(0xffffffffu, m2, 17);
-        float m3 = red4(m2, b, c, d, J.lw[2] == 1u, J.lh[2] == 1u);
-        if ((lane & 17) == 0) {
-            const int lx = tx4 >> 1, ly = warp;  // ty4 >> 1 == warp
-            s_m3[ly][lx] = m3;
-            const uint32_t x3 = (X0 >> 3) + lx, y3 = (Y0 >> 3) + ly;
-            if (x3 < J.lw[3] && y3 < J.lh[3]) J.levels[3][(size_t)y3 * J.lpitch[3] + x3] = m3;
-        }
-    }
-    __syncthreads();
-    if (warp != 0) return;  // levels 4.. and the tail need only warp 0
-    // Levels 4..6: warp 0.
-    if (J.mip_count > 4) {
-        const int x4 = lane & 3, y4 = (lane >> 2) & 3;
-        float m4 = red4(s_m3[2 * y4][2 * x4], s_m3[2 * y4][2 * x4 + 1], s_m3[2 * y4 + 1][2 * x4],
-                        s_m3[2 * y4 + 1][2 * x4 + 1], J.lw[3] == 1u, J.lh[3] == 1u);
-        if (lane < 16) {
-            const uint32_t gx = (X0 >> 4) + x4, gy = (Y0 >> 4) + y4;
-            if (gx < J.lw[4] && gy < J.lh[4]) J.levels[4][(size_t)gy * J.lpitch[4] + gx] = m4;
-        }
-        if (J.mip_count > 5) {
-            float b = __shfl_xor_sync(0xffffffffu, m4, 1);
-            float c = __shfl_xor_sync(0xffffffffu, m4, 4);
-            float d = __shfl_xor_sync(0xffffffffu, m4, 5);
-            float m5 = red4(m4, b, c, d, J.lw[4] == 1u, J.lh[4] == 1u);
-            if (lane < 16 && (lane & 5) == 0) {
-                const uint32_t gx = (X0 >> 5) + (x4 >> 1), gy = (Y0 >> 5) + (y4 >> 1);
-                if (gx < J.lw[5] && gy < J.lh[5]) J.levels[5][(size_t)gy * J.lpitch[5] + gx] = m5;
-            }
-            if (J.mip_count > 6) {
-                float b6 = __shfl_sync(0xffffffffu, m5, 2);
-                float c6 = __shfl_sync(0xffffffffu, m5, 8);
-                float d6 = __shfl_sync(0xffffffffu, m5, 10);
-                float m6 = red4(m5, b6, c6, d6, J.lw[5] == 1u, J.lh[5] == 1u);
-                if (lane == 0) {
-                    const uint32_t gx = X0 >> 6, gy = Y0 >> 6;
-                    if (gx < J.lw[6] && gy < J.lh[6]) J.levels[6][(size_t)gy * J.lpitch[6] + gx] = m6;
-                }
-            }
-        }
-    }
-    if (warp != 0 || J.mip_count <= 7) return;
-
-    // Tail: level 6 is written by warp 0 only, so warp 0 alone takes the ticket;
-    // the warp of the last CTA of this job builds levels 7.. from level 6.
-    __threadfence();
-    __syncwarp();
-    uint32_t last = 0u;
-    if (lane == 0) {
-        const uint32_t tiles = J.tiles_x * J.tiles_y;
-        const uint32_t t = atomicAdd(&tickets[s_job], 1u);
-        last = (t + 1 == tiles) ? 1u : 0u;
-        if (last) tickets[s_job] = 0u;  // every other CTA of this job has already taken its ticket
-    }
-    last = __shfl_sync(0xffffffffu, last, 0);
-    if (last) {
-        __threadfence();
-        hiz_tail_warp(J);
-    }
+    hiz_tile(s_J, s_job, tile - s_J.tile_begin, tickets, s_m3);
 }
 
 }  // namespace

@@ -23,6 +23,7 @@
 #include "common.cuh"
 #include "kernels.h"
 #include "vg.h"
+#include "vg_device.cuh"
 
 namespace helio {
 
@@ -87,16 +88,6 @@ __global__ void instance_cull_data_kernel(const HelioGpuInstanceData* __restrict
     }
 }
 
-__device__ __forceinline__ HelioInstanceCullData load_cull(const HelioInstanceCullData* p) {
-    const uint4 q = __ldg(reinterpret_cast<const uint4*>(p));
-    HelioInstanceCullData r;
-    r.max_scale = __uint_as_float(q.x);
-    r.min_scale = __uint_as_float(q.y);
-    r.cone_cull_enabled = q.z;
-    r.valid_transform = q.w;
-    return r;
-}
-
 // ── View constants (one warp per launch) ──────────────────────────────────────
 
 __global__ void __launch_bounds__(32) vg_view_setup_kernel(ViewSetupParams P) {
@@ -118,13 +109,6 @@ __global__ void __launch_bounds__(32) vg_view_setup_kernel(ViewSetupParams P) {
         v.pad[0] = v.pad[1] = 0u;
         *P.out = v;
     }
-}
-
-// Cooperative copy of the view constants into shared memory (16-byte words).
-__device__ __forceinline__ void load_view(const CullView* src, CullView& dst, int tid, int nthreads) {
-    const uint4* s = reinterpret_cast<const uint4*>(src);
-    uint4* d = reinterpret_cast<uint4*>(&dst);
-    for (int k = tid; k < (int)(sizeof(CullView) / 16); k += nthreads) d[k] = __ldg(s + k);
 }
 
 // ── Object select: cs_select_objects (vg_cull.wgsl:282-352) ───────────────────
@@ -200,83 +184,6 @@ __global__ void __launch_bounds__(256) vg_select_kernel(VgSelectParams P) {
 }
 
 // ── Meshlet cull ──────────────────────────────────────────────────────────────
-
-// cull_meshlet decision part (vg_cull.wgsl:143-240): true = emit a draw.
-__device__ __forceinline__ bool meshlet_visible(const VgSceneDev& S, const CullView& C, uint32_t mi,
-                                                const Mat4& model, const HelioInstanceCullData& cd,
-                                                const HelioGpuInstanceData* inst) {
-    const Planes& pl = C.planes;
-    const HizView& hz = C.hiz;
-    const uint32_t screen_h = C.screen_height, hiz_mip_count = C.hiz_mip_count;
-    if (cd.valid_transform == 0u) return false;
-    const float4 b = __ldg(S.m_bounds + mi);
-    const F3 c = mat4_point3(model, f3(b.x, b.y, b.z));
-    const float wr = fmaxf(fmul(b.w, cd.max_scale), 0.0f);
-    const F3 cam = f3(C.pos_near.x, C.pos_near.y, C.pos_near.z);
-    const F3 ctc = sub3(c, cam);
-    if (!sphere_visible_vg(pl, c, wr)) return false;
-    // Perspective normal-cone test (:159-182).
-    if (cd.cone_cull_enabled != 0u) {
-        const float4 cone = __ldg(S.m_cone + mi);
-        const float cam_dist_sq = dot3(ctc, ctc);
-        const float guard = fmul(wr, 1.5f);
-        if (cam_dist_sq > fmul(guard, guard) && cone.w <= 1.0f) {
-            const float4 ax = __ldg(S.m_axis + mi);
-            const float4* nm = reinterpret_cast<const float4*>(inst->normal_mat);
-            const F3 a = mat3_vec(__ldg(nm), __ldg(nm + 1), __ldg(nm + 2), f3(ax.x, ax.y, ax.z));
-            const F3 axis_ws = divs3(a, fsqrt(dot3(a, a)));
-            const F3 apex = mat4_point3(model, f3(cone.x, cone.y, cone.z));
-            const F3 cta = sub3(apex, cam);
-            const float ads = dot3(cta, cta);
-            if (ads > 1.0e-12f && dot3(divs3(cta, fsqrt(ads)), axis_ws) >= cone.w) return false;
-        }
-    }
-    // Conservative Hi-Z test (:184-240).
-    const float4 clip = mat4_point4(C.vp, c);
-    if (clip.w > 0.0f) {
-        const float ndc_x = fdiv(clip.x, clip.w), ndc_y = fdiv(clip.y, clip.w);
-        const float uv_x = fadd(fmul(ndc_x, 0.5f), 0.5f), uv_y = fadd(fmul(ndc_y, -0.5f), 0.5f);
-        const float nvd = fsub(clip.w, wr);
-        if (nvd > C.pos_near.w) {
-            const float ndc_r = fmaxf(fabsf(fdiv(fmul(wr, C.p00), nvd)), fabsf(fdiv(fmul(wr, C.p11), nvd)));
-            const float uvr = fmul(ndc_r, 0.5f);
-            const float u0 = fsub(uv_x, uvr), v0 = fsub(uv_y, uvr), u1 = fadd(uv_x, uvr), v1 = fadd(uv_y, uvr);
-            if (u0 >= 0.0f && v0 >= 0.0f && u1 <= 1.0f && v1 <= 1.0f) {
-                const float dist_sq = dot3(ctc, ctc);
-                float near_z = 0.0f;
-                if (dist_sq > fmul(wr, wr)) {
-                    const F3 dir = divs3(ctc, fsqrt(dist_sq));
-                    const F3 nws = sub3(c, muls3(dir, wr));
-                    const float4 nc = mat4_point4(C.vp, nws);
-                    if (nc.w > 0.0f) near_z = clampf(fdiv(nc.z, nc.w), 0.0f, 1.0f);
-                }
-                const float half_h = fmul((float)screen_h, 0.5f);
-                const float dpx = fmaxf(fmul(fmul(ndc_r, half_h), 2.0f), 1.0f);
-                const uint32_t mip = min(ceil_log2_exact(dpx), hiz_mip_count - 1u);
-                const float h00 = hiz_sample(hz, u0, v0, mip);
-                const float h01 = hiz_sample(hz, u1, v0, mip);
-                const float h10 = hiz_sample(hz, u0, v1, mip);
-                const float h11 = hiz_sample(hz, u1, v1, mip);
-                const float hzv = fmaxf(fmaxf(h00, h01), fmaxf(h10, h11));
-                if (near_z > fadd(hzv, 1.0f / 65536.0f)) return false;
-            }
-        }
-    }
-    return true;
-}
-
-// Largest lane j whose exclusive offset is <= s (for s below the warp total this
-// is the item that owns window slot s; empty items are skipped because they share
-// their offset with the next item).
-__device__ __forceinline__ int owner_lane(uint32_t off, uint32_t s) {
-    int lo = 0;
-#pragma unroll
-    for (int step = 16; step > 0; step >>= 1) {
-        const uint32_t o = __shfl_sync(0xffffffffu, off, lo + step);
-        if (o <= s) lo += step;
-    }
-    return lo;
-}
 
 // The 32 work items of one warp (lane = item): active meshlet range and packing offsets.
 struct WarpItems {

@@ -132,6 +132,33 @@ class VgOutputs(C.Structure):
                 ("capacity", u32), ("counter_count", u32), ("work_item_count", u32), ("object_count", u32)]
 
 
+class VgSceneInfo(C.Structure):
+    _fields_ = [("meshlet_count", u32), ("object_count", u32), ("lod0_meshlets", u64), ("max_spans", u64),
+                ("device_bytes", u64)]
+
+
+class BatchConfig(C.Structure):
+    _fields_ = [("max_views", u32), ("flags", u32), ("max_spans", u64)]
+
+
+class BatchView(C.Structure):
+    _fields_ = [("camera", GpuCameraUniforms), ("depth", vp), ("depth_pitch", u32), ("width", u32), ("height", u32),
+                ("lod_error_threshold_px", f32), ("draw_capacity", u32), ("flags", u32)]
+
+
+class BatchViewOutputs(C.Structure):
+    _fields_ = [("indirect", vp), ("draws", vp), ("counters", vp), ("lod", vp), ("capacity", u32),
+                ("object_count", u32), ("pyramid", HizPyramid)]
+
+
+class BatchSpanList(C.Structure):
+    _fields_ = [("spans", vp), ("visibility", vp), ("view_span_start", vp), ("span_capacity", u32),
+                ("view_count", u32)]
+
+
+HELIO_BATCH_MAX_VIEWS = 128
+HELIO_BATCH_SPAN_VISIBILITY = 1
+
 _SIZES = {GpuCameraUniforms: 368, GpuInstanceData: 144, GpuInstanceAabb: 32, GpuDrawCall: 20,
           DrawIndexedIndirectArgs: 20, GpuMeshletEntry: 64, GpuVgObject: 128, GpuVgDraw: 16, GpuVgWorkItem: 8,
           InstanceCullData: 16, VgFrameData: 80}
@@ -182,6 +209,18 @@ CULL_EXPORTS = {
     "helio_vg_publish": (i32, [vp, C.POINTER(VgOutputs)]),
     "helio_vg_device_status": (i32, [vp, vp]),
     "helio_vg_destroy": (None, [vp]),
+    "helio_vg_scene_create": (i32, [C.POINTER(vp)]),
+    "helio_vg_scene_upload": (i32, [vp, C.POINTER(VgFrameData), vp]),
+    "helio_vg_scene_info_get": (i32, [vp, C.POINTER(VgSceneInfo)]),
+    "helio_vg_scene_destroy": (None, [vp]),
+    "helio_batch_create": (i32, [C.POINTER(BatchConfig), C.POINTER(vp)]),
+    "helio_batch_prepare": (i32, [vp, vp, u32, C.POINTER(BatchView), vp]),
+    "helio_batch_set_cameras": (i32, [vp, u32, C.POINTER(GpuCameraUniforms), vp]),
+    "helio_batch_execute": (i32, [vp, vp]),
+    "helio_batch_get_view_outputs": (i32, [vp, u32, C.POINTER(BatchViewOutputs)]),
+    "helio_batch_get_spans": (i32, [vp, C.POINTER(BatchSpanList)]),
+    "helio_batch_status": (i32, [vp, vp]),
+    "helio_batch_destroy": (None, [vp]),
 }
 
 _cull = None

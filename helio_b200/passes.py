@@ -216,6 +216,96 @@ def fused_instance_cull(frustum: IndirectDispatchPass, occlusion: OcclusionCullP
                                                   _stream_ptr(stream)))
 
 
+class VgScene:
+    """Device-resident virtual-geometry scene shared by batches (helio_vg_scene)."""
+
+    def __init__(self):
+        self._lib = N.cull_lib()
+        h = C.c_void_p()
+        N.check(self._lib.helio_vg_scene_create(C.byref(h)))
+        self._h = h
+
+    def upload(self, frame: N.VgFrameData, stream=None) -> None:
+        N.check(self._lib.helio_vg_scene_upload(self._h, C.byref(frame), _stream_ptr(stream)))
+
+    def info(self) -> N.VgSceneInfo:
+        out = N.VgSceneInfo()
+        N.check(self._lib.helio_vg_scene_info_get(self._h, C.byref(out)))
+        return out
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            self._lib.helio_vg_scene_destroy(h)
+            self._h = None
+
+
+class BatchedCull:
+    """Every view of a batch culled against one VgScene in one cooperative launch
+    (Hi-Z of each view, object LOD select for every (object, view), meshlet cull and
+    per-view deterministic compaction)."""
+
+    def __init__(self, max_views: int = N.HELIO_BATCH_MAX_VIEWS, span_visibility: bool = False, max_spans: int = 0):
+        self._lib = N.cull_lib()
+        cfg = N.BatchConfig(max_views, N.HELIO_BATCH_SPAN_VISIBILITY if span_visibility else 0, max_spans)
+        h = C.c_void_p()
+        N.check(self._lib.helio_batch_create(C.byref(cfg), C.byref(h)))
+        self._h = h
+        self._keep = None
+        self.view_count = 0
+
+    def prepare(self, scene: VgScene, views: list, stream=None) -> None:
+        """views: sequence of dicts with camera (GpuCameraUniforms), depth (device
+        float32 tensor H x W), optional lod_threshold_px, draw_capacity, alias_mip0."""
+        arr = (N.BatchView * len(views))()
+        for i, v in enumerate(views):
+            d = v["depth"]
+            assert d.is_cuda and d.dtype == torch.float32 and d.stride(1) == 1
+            arr[i].camera = v["camera"]
+            arr[i].depth = d.data_ptr()
+            arr[i].depth_pitch = d.stride(0)
+            arr[i].height, arr[i].width = d.shape
+            arr[i].lod_error_threshold_px = v.get("lod_threshold_px", 0.0)
+            arr[i].draw_capacity = v.get("draw_capacity", 0)
+            arr[i].flags = N.HELIO_HIZ_ALIAS_MIP0 if v.get("alias_mip0", False) else 0
+        self._keep = (scene, [v["depth"] for v in views])
+        N.check(self._lib.helio_batch_prepare(self._h, scene._h, len(views), arr, _stream_ptr(stream)))
+        self.view_count = len(views)
+
+    def set_cameras(self, cameras: list, stream=None) -> None:
+        arr = (N.GpuCameraUniforms * len(cameras))(*cameras)
+        N.check(self._lib.helio_batch_set_cameras(self._h, len(cameras), arr, _stream_ptr(stream)))
+
+    def execute(self, stream=None) -> None:
+        N.check(self._lib.helio_batch_execute(self._h, _stream_ptr(stream)))
+
+    def status(self, stream=None) -> None:
+        N.check(self._lib.helio_batch_status(self._h, _stream_ptr(stream)))
+
+    def view_outputs(self, v: int) -> dict:
+        o = N.BatchViewOutputs()
+        N.check(self._lib.helio_batch_get_view_outputs(self._h, v, C.byref(o)))
+        cap = max(o.capacity, 1)
+        return {"indirect": device_view(o.indirect, (cap, 5)), "draws": device_view(o.draws, (cap, 4)),
+                "counters": device_view(o.counters, (11,)), "lod": device_view(o.lod, (max(o.object_count, 1),), "|u1"),
+                "capacity": o.capacity, "pyramid": o.pyramid}
+
+    def spans(self) -> dict:
+        s = N.BatchSpanList()
+        N.check(self._lib.helio_batch_get_spans(self._h, C.byref(s)))
+        out = {"spans": device_view(s.spans, (s.span_capacity, 4)),
+               "view_span_start": device_view(s.view_span_start, (s.view_count + 1,))}
+        if s.visibility:
+            out["visibility"] = device_view(s.visibility, (s.span_capacity, 2))
+        return out
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            self._lib.helio_batch_destroy(h)
+            self._h = None
+
+
 class VirtualGeometryPass:
     """Virtual-geometry cull: object LOD select + meshlet cull + deterministic compaction."""
 

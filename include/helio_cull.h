@@ -418,6 +418,92 @@ int32_t helio_vg_publish(const helio_vg_pass* pass, helio_vg_outputs* out);
 int32_t helio_vg_device_status(helio_vg_pass* pass, void* stream);
 void helio_vg_destroy(helio_vg_pass* pass);
 
+/* ════════════════════════════════════════════════════════════════════════════
+ * Batched multi-view culling (no single reference counterpart: it performs, for
+ * every view of a batch, what HiZBuildPass + VirtualGeometryPass's cull half do
+ * for one view, against one device-resident scene, in one cooperative launch).
+ * ════════════════════════════════════════════════════════════════════════════ */
+
+/* A device-resident virtual-geometry scene shared by batches. Upload follows the
+ * VgFrameData version rules of helio_vg_prepare (rendering.rs:708-819). Work items
+ * are not used: a batch derives the 64-meshlet spans of each object's selected LOD. */
+typedef struct helio_vg_scene helio_vg_scene;
+typedef struct helio_vg_scene_info {
+    uint32_t meshlet_count;
+    uint32_t object_count;
+    uint64_t lod0_meshlets; /* sum over objects of lod_meshlet_counts[0] */
+    uint64_t max_spans;     /* sum over objects of ceil(max_meshlet_count / 64) */
+    uint64_t device_bytes;
+} helio_vg_scene_info;
+int32_t helio_vg_scene_create(helio_vg_scene** out);
+int32_t helio_vg_scene_upload(helio_vg_scene* scene, const helio_vg_frame_data* frame, void* stream);
+int32_t helio_vg_scene_info_get(const helio_vg_scene* scene, helio_vg_scene_info* out);
+void helio_vg_scene_destroy(helio_vg_scene* scene);
+
+#define HELIO_BATCH_MAX_VIEWS 128u
+/* helio_batch_config.flags: also write per-span visibility words. */
+#define HELIO_BATCH_SPAN_VISIBILITY 1u
+
+typedef struct helio_batch_config {
+    uint32_t max_views; /* <= HELIO_BATCH_MAX_VIEWS */
+    uint32_t flags;
+    uint64_t max_spans; /* capacity of the active-span list; 0 = every view at LOD 0 */
+} helio_batch_config;
+
+/* One view of a batch. */
+typedef struct helio_batch_view {
+    HelioGpuCameraUniforms camera; /* host copy, uploaded by prepare / set_cameras */
+    const float* depth;            /* device, width x height floats, row pitch depth_pitch */
+    uint32_t depth_pitch;          /* floats; 0 = width */
+    uint32_t width;                /* render size (Hi-Z size, CullUniforms.screen_*) */
+    uint32_t height;
+    float lod_error_threshold_px;  /* 0 = LodQuality::Medium (2 px) */
+    uint32_t draw_capacity;        /* 0 = min(sum of max_meshlet_count, 262144) */
+    uint32_t flags;                /* HELIO_HIZ_ALIAS_MIP0: level 0 is the depth buffer itself */
+} helio_batch_view;
+
+/* Per-view results (device pointers owned by the batch). indirect / draws hold
+ * min(counters[0], capacity) draws in (object, span, lane) order, first_instance = slot;
+ * counters use the 11-word VG layout; lod[o] = selected LOD + 1 of object o (0 = culled). */
+typedef struct helio_batch_view_outputs {
+    HelioDrawIndexedIndirectArgs* indirect;
+    HelioGpuVgDraw* draws;
+    uint32_t* counters;
+    uint8_t* lod;
+    uint32_t capacity;
+    uint32_t object_count;
+    helio_hiz_pyramid pyramid;
+} helio_batch_view_outputs;
+
+/* The active spans of the last execute: spans[4 * k + 0..3] = first meshlet,
+ * n | lod << 8 | view << 16, instance, object; view v owns spans
+ * [view_span_start[v], view_span_start[v + 1]) (padded with n = 0 to a multiple of 32).
+ * visibility (if enabled) holds 2 words per span: bit l = meshlet l of the span visible. */
+typedef struct helio_batch_span_list {
+    const uint32_t* spans;
+    const uint32_t* visibility;
+    const uint32_t* view_span_start;
+    uint32_t span_capacity;
+    uint32_t view_count;
+} helio_batch_span_list;
+
+typedef struct helio_batch helio_batch;
+int32_t helio_batch_create(const helio_batch_config* config, helio_batch** out);
+/* Binds a scene and a set of views; (re)allocates pyramids, outputs and scratch. */
+int32_t helio_batch_prepare(helio_batch* batch, const helio_vg_scene* scene, uint32_t view_count,
+                            const helio_batch_view* views, void* stream);
+/* Replaces the cameras of the prepared views (no allocation). */
+int32_t helio_batch_set_cameras(helio_batch* batch, uint32_t view_count, const HelioGpuCameraUniforms* cameras,
+                                void* stream);
+/* Clears the counters and runs the persistent cooperative kernel on `stream`. */
+int32_t helio_batch_execute(helio_batch* batch, void* stream);
+int32_t helio_batch_get_view_outputs(const helio_batch* batch, uint32_t view, helio_batch_view_outputs* out);
+int32_t helio_batch_get_spans(const helio_batch* batch, helio_batch_span_list* out);
+/* Synchronises `stream`; HELIO_ERR_TIMEOUT if a bounded grid barrier gave up,
+ * HELIO_ERR_CAPACITY if the active spans exceeded max_spans (outputs incomplete). */
+int32_t helio_batch_status(helio_batch* batch, void* stream);
+void helio_batch_destroy(helio_batch* batch);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

@@ -1,0 +1,145 @@
+"""Batched multi-view cull (one cooperative launch) vs the oracle, view by view:
+pyramid levels, selected LOD per object, counters, indirect args and draw metadata in
+the canonical (object, span, lane) order, and the per-span visibility words."""
+import numpy as np
+import pytest
+
+from helpers import benchmark_scene, cull_dtype, u32
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def run_batch(scene, views, span_visibility=True, alias=False, capacities=None, repeats=1):
+    import torch
+    from helio_b200 import scene as S
+    from helio_b200.passes import BatchedCull, VgScene
+
+    vs = VgScene()
+    vs.upload(S.frame_data(scene))
+    depths = [torch.from_numpy(np.ascontiguousarray(v.depth)).cuda() for v in views]
+    b = BatchedCull(len(views), span_visibility=span_visibility)
+    specs = []
+    for i, (v, d) in enumerate(zip(views, depths)):
+        spec = {"camera": v.camera, "depth": d, "alias_mip0": alias, "lod_threshold_px": v.lod_threshold_px}
+        if capacities:
+            spec["draw_capacity"] = capacities[i]
+        specs.append(spec)
+    b.prepare(vs, specs)
+    for _ in range(repeats):
+        b.execute()
+    torch.cuda.synchronize()
+    b.status()
+    return b, vs, depths
+
+
+def gather(b, v, n_objects):
+    from helio_b200.passes import device_view
+
+    o = b.view_outputs(v)
+    counters = u32(o["counters"])
+    n = int(min(counters[0], o["capacity"]))
+    p = o["pyramid"]
+    levels = [device_view(p.levels[l], (p.height[l], p.width[l]), "<f4", (p.pitch[l] * 4, 4)).cpu().numpy()
+              for l in range(p.mip_count)]
+    return {"counters": counters, "indirect": u32(o["indirect"])[:n], "draws": u32(o["draws"])[:n],
+            "lod": o["lod"].cpu().numpy()[:n_objects].astype(np.uint32), "levels": levels, "capacity": o["capacity"]}
+
+
+def check_view(scene, view, got, spans_view, vis_view, cap):
+    levels = O.hiz_build(view.depth)
+    for l, (a, r) in enumerate(zip(got["levels"], levels)):
+        np.testing.assert_array_equal(a.view(np.uint32), r.view(np.uint32), err_msg=f"level {l}")
+    ref = O.run_view(scene, view.camera, view.width, view.height, levels, view.lod_threshold_px, cap, 11, 4,
+                     cull_dtype())
+    np.testing.assert_array_equal(got["lod"], ref["selected"], err_msg="selected LOD + 1")
+    np.testing.assert_array_equal(got["counters"], ref["counters"], err_msg="counters")
+    np.testing.assert_array_equal(got["indirect"], ref["indirect"], err_msg="indirect")
+    np.testing.assert_array_equal(got["draws"], ref["draws"], err_msg="draws")
+    if spans_view is not None:
+        # active work items (span base below the selected LOD's count), in order
+        items = scene.work_items
+        sel = ref["selected"][items["object_index"]]
+        lod = np.maximum(sel.astype(np.int64) - 1, 0)
+        cnt = np.where(sel > 0, scene.objects["lod_meshlet_counts"][items["object_index"], lod], 0)
+        active = items["local_meshlet_base"] < cnt
+        real = spans_view[(spans_view[:, 1] & 0x7F) > 0]
+        assert len(real) == int(active.sum())
+        np.testing.assert_array_equal(real[:, 3], items["object_index"][active], err_msg="span objects")
+        if vis_view is not None:
+            np.testing.assert_array_equal(vis_view[(spans_view[:, 1] & 0x7F) > 0], ref["visibility"][active],
+                                          err_msg="span visibility")
+
+
+def _check_batch(w, views, **kw):
+    b, vs, _ = run_batch(w.scene, views, **kw)
+    sp = b.spans()
+    spans = u32(sp["spans"])
+    start = u32(sp["view_span_start"])
+    vis = u32(sp["visibility"]) if "visibility" in sp else None
+    for i, v in enumerate(views):
+        got = gather(b, i, len(w.scene.objects))
+        sv = spans[start[i]:start[i + 1]]
+        check_view(w.scene, v, got, sv, vis[start[i]:start[i + 1]] if vis is not None else None, got["capacity"])
+    return b
+
+
+def test_batch_85_views_matches_oracle(cuda):
+    from helio_b200 import scene as S
+
+    w = S.config(3, scale=0.02)
+    assert len(w.views) == 85
+    _check_batch(w, w.views)
+
+
+@pytest.mark.parametrize("cfg,scale,nviews", [(0, 1.0, 1), (1, 0.2, 1), (2, 0.05, 1)])
+def test_batch_single_view_equals_plain_pipeline(cuda, cfg, scale, nviews):
+    from helio_b200 import scene as S
+
+    w = S.config(cfg, scale=scale)
+    _check_batch(w, w.views[:nviews])
+
+
+def test_batch_mixed_views_alias_and_capacity(cuda):
+    """A cfg2-shaped scene seen by the 85-view mix at a small scale, level 0 aliased
+    to the depth, and a small per-view capacity that overflows."""
+    from helio_b200 import scene as S
+
+    w = S.config(2, scale=0.03)
+    views = S.multiview_set(S.SEED_BASE + 2, True, 0.04)[:24]
+    b, vs, _ = run_batch(w.scene, views, alias=True, capacities=[50] * len(views))
+    for i, v in enumerate(views):
+        got = gather(b, i, len(w.scene.objects))
+        check_view(w.scene, v, got, None, None, 50)
+
+
+def test_batch_repeat_and_camera_update(cuda):
+    import torch
+    from helio_b200 import scene as S
+
+    w = S.config(3, scale=0.02)
+    views = w.views[:10]
+    b, vs, depths = run_batch(w.scene, views, repeats=3)
+    for i, v in enumerate(views):
+        check_view(w.scene, v, gather(b, i, len(w.scene.objects)), None, None, gather(b, i, 1)["capacity"])
+    # Move every camera and re-run without re-preparing.
+    moved = []
+    for v in views:
+        cam = S.perspective(tuple(np.array(v.camera.position_near[:3]) + 7.0), (0, 0, -300), (0, 1, 0), 70.0,
+                            v.width / v.height)
+        moved.append(S.View(cam, v.width, v.height, v.depth, v.kind, v.lod_threshold_px))
+    b.set_cameras([m.camera for m in moved])
+    b.execute()
+    torch.cuda.synchronize()
+    b.status()
+    for i, v in enumerate(moved):
+        check_view(w.scene, v, gather(b, i, len(w.scene.objects)), None, None, gather(b, i, 1)["capacity"])
+
+
+def test_batch_benchmark_scene(cuda):
+    """Every meshlet of the constant benchmark scene is emitted (meshlet_cull_benchmark.rs:284-294)."""
+    sc, v = benchmark_scene(64, 1024)
+    b, vs, _ = run_batch(sc, [v], span_visibility=False, capacities=[64 * 1024])
+    got = gather(b, 0, len(sc.objects))
+    assert got["counters"][0] == 64 * 1024 and got["counters"][1] == 0
+    np.testing.assert_array_equal(got["indirect"][:, 4], np.arange(64 * 1024))
