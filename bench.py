@@ -4,20 +4,26 @@
     python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME] [--impl ours|reference]
 
 A step is one pass of the hot path over one synthetic frame: Hi-Z pyramid build
-from the frame's depth, object LOD select, meshlet cull and deterministic draw
-compaction, for every view of the workload. The metric counts (view, LOD0 scene
-meshlet) pairs per second. Inputs are resident in HBM for `value`; `e2e` runs
-the same step through the C-ABI with host buffers (depth and camera copied in,
-counters and visible draws copied out) inside the timed region.
+from each view's depth, object LOD select, meshlet frustum / cone / Hi-Z cull and
+deterministic draw compaction, for every view of the workload. The metric counts
+(view, LOD0 scene meshlet) pairs per second.
 
-Workloads: plain2 (default; 100,000 instances x 100 meshlets = 10M LOD0 meshlets,
-3840x2160, one view), plain1 (1M meshlets, 1920x1080), plain0 (262,144 meshlets,
-1024x1024).
+Workloads
+  batched3 (default)  one scene of 200,000 instances x 50 LOD0 meshlets (10M), 85 views
+                      (1 main 3840x2160, 4 orthographic cascades 2048^2, 16 spot 512^2,
+                      64 probes 128^2), culled in ONE persistent cooperative launch; the
+                      85 plain per-view pipelines are timed beside it (same inputs).
+  plain2              100,000 instances x 100 LOD0 meshlets (10M), one 3840x2160 view.
+  plain1 / plain0     1M meshlets at 1920x1080 / 262,144 meshlets at 1024x1024.
 
-Multi-GPU (torchrun): every rank runs its own replica of the workload on its own
-GPU (independent frames, no collective on the data path): weak scaling, time =
-max over ranks. `--impl reference` times the CPU restatement of the reference
-shaders (the oracle) on the host cores, on rank 0 only.
+`value` is measured with inputs resident in HBM, the step replayed as a CUDA graph,
+CUDA events on the launching stream, L2 flushed between timed steps. `e2e` runs the
+same step through the C-ABI with host buffers: every view's depth and camera copied
+in from pinned memory and the counters and visible draws copied out, inside the
+timed region. Multi-GPU (torchrun): every rank runs its own replica of the workload
+(independent frames, no collective on the data path): weak scaling, time = max over
+ranks. `--impl reference` times the CPU restatement of the reference shaders (the
+oracle) on the host cores, on rank 0 only.
 """
 from __future__ import annotations
 
@@ -38,6 +44,7 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
+SLEEP_CYCLES = 400_000      # on-device delay queued ahead of each timed step
 
 
 def parse_args():
@@ -45,9 +52,10 @@ def parse_args():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
-    ap.add_argument("--workload", default="plain2", choices=["plain2", "plain1", "plain0"])
+    ap.add_argument("--workload", default="batched3", choices=["batched3", "plain2", "plain1", "plain0"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-plain", action="store_true", help="batched3: skip the per-view plain comparison")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="bound of the CPU baseline sample")
     return ap.parse_args()
 
@@ -89,11 +97,8 @@ class Clocks:
         time.sleep(0.25)
         self.proc.terminate()
         self.proc.wait()
-        rows = []
-        for line in Path(self.path).read_text().splitlines():
-            parts = [x.strip() for x in line.split(",")]
-            if len(parts) >= 9:
-                rows.append(parts)
+        rows = [[x.strip() for x in line.split(",")] for line in Path(self.path).read_text().splitlines()]
+        rows = [r for r in rows if len(r) >= 9]
         os.unlink(self.path)
         if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
@@ -105,176 +110,351 @@ class Clocks:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def build_workload(name: str):
-    from helio_b200 import scene as S
-
-    cfg = {"plain2": 2, "plain1": 1, "plain0": 0}[name]
-    return S.config(cfg)
-
-
 def hiz_bytes(w: int, h: int, copy: bool) -> int:
+    """Depth read, level-0 copy (unless aliased), and every level above 0 written."""
     b = 4 * w * h * (2 if copy else 1)
-    m = min(int(max(w, h)).bit_length(), 12)
-    for l in range(1, m):
+    for l in range(1, min(int(max(w, h)).bit_length(), 12)):
         b += 4 * max(w >> l, 1) * max(h >> l, 1)
     return b
 
 
-def vg_algorithmic_bytes(scene, selected: np.ndarray, visible: int) -> dict:
-    """Bytes an ideal implementation must move per launch, from the step's own outputs.
-    select: per object 64 B (head, local bounds, LOD errors) + 64 B model + 16 B
-    InstanceCullData + 4 B selected-LOD write + 16 B selected range record.
-    cull: per work item 8 B item + 8 B selected range + 8 B visibility bitmask; per
-    active work item 80 B (model + cull data); per tested meshlet 44 B (centre, radius,
-    cone apex, cutoff, axis as f32); per visible meshlet 12 B read + 20 B + 16 B written."""
+def active_spans(scene, lod_plus_one: np.ndarray) -> tuple[int, int]:
+    """(active 64-meshlet spans, tested meshlets) of one view's selected LODs."""
     obj = scene.objects
-    items = scene.work_items
-    O, W = len(obj), len(items)
-    sp1 = selected.astype(np.int64)
-    lod = np.maximum(sp1 - 1, 0)
-    cnt = np.where(sp1 > 0, obj["lod_meshlet_counts"][np.arange(O), lod], 0)
-    oi = items["object_index"].astype(np.int64)
-    valid = oi < O
-    c = np.zeros(W, np.int64)
-    c[valid] = cnt[oi[valid]]
-    base = items["local_meshlet_base"].astype(np.int64)
-    n = np.clip(c - base, 0, 64)
-    tested = int(n.sum())
-    active = int((n > 0).sum())
-    return {"select": 164 * O, "cull_test": 24 * W + 80 * active + 44 * tested, "cull_emit": 48 * visible,
-            "tested_meshlets": tested, "active_items": active}
+    sel = lod_plus_one.astype(np.int64)
+    lod = np.maximum(sel - 1, 0)
+    cnt = np.where(sel > 0, obj["lod_meshlet_counts"][np.arange(len(obj)), lod], 0).astype(np.int64)
+    return int(((cnt + 63) // 64).sum()), int(cnt.sum())
+
+
+def union_meshlets(scene, lods: np.ndarray) -> int:
+    """Meshlets of the union over views of each object's selected LOD range."""
+    obj = scene.objects
+    total = 0
+    counts = obj["lod_meshlet_counts"].astype(np.int64)
+    for l in range(8):
+        used = (lods == l + 1).any(axis=0)
+        total += int(counts[used, l].sum())
+    return total
+
+
+# ── Workloads ─────────────────────────────────────────────────────────────────
+
+class PlainWorkload:
+    """Single view through HiZBuildPass + VirtualGeometryPass (the drop-in passes)."""
+
+    def __init__(self, name, dev):
+        import torch
+        from helio_b200 import scene as S
+        from helio_b200.passes import HiZBuildPass, VirtualGeometryPass, camera_bytes
+
+        self.name = name
+        self.wl = S.config({"plain2": 2, "plain1": 1, "plain0": 0}[name])
+        self.scene = self.wl.scene
+        self.views = self.wl.views
+        self.units = self.scene.lod0_total * len(self.views)
+        self.passes = []
+        for v in self.views:
+            depth = torch.from_numpy(v.depth).to(dev)
+            cam = torch.from_numpy(camera_bytes(v.camera)).to(dev)
+            hz = HiZBuildPass(v.width, v.height)
+            hz.prepare(depth)
+            vg = VirtualGeometryPass(v.width, v.height)
+            vg.prepare(S.frame_data(self.scene))
+            self.passes.append((v, depth, cam, hz, vg))
+
+    def step(self):
+        for v, depth, cam, hz, vg in self.passes:
+            hz.execute()
+            vg.execute(cam, hz.publish())
+
+    def describe(self):
+        v = self.views[0]
+        return (f"{self.name}: {len(self.scene.objects)} instances x {self.scene.lod0_meshlets} LOD0 meshlets, "
+                f"1 view {v.width}x{v.height}")
+
+    def kernel_bytes(self) -> tuple[dict, int]:
+        """Bytes an ideal implementation must move per launch, from the step's outputs:
+        hiz_build = depth read + level-0 copy + levels 1.. written; vg_select = 164 B per
+        object (64 B head / bounds / LOD errors, 64 B model, 16 B InstanceCullData, 4 B
+        selected-LOD write, 16 B selected-range record); vg_cull_test = 24 B per work item
+        (item, selected range, visibility words) + 80 B per active item (model + cull
+        data) + 44 B per tested meshlet (centre, radius, cone apex, cutoff, axis);
+        vg_cull_emit = 48 B per visible draw (12 B read, 36 B written)."""
+        v, depth, cam, hz, vg = self.passes[0]
+        o = vg.outputs()
+        counters = o["counters"].cpu().numpy().view(np.uint32)
+        selected = o["objects"].cpu().numpy().view(np.uint32)[: len(self.scene.objects), 3]
+        visible = int(min(counters[0], o["capacity"]))
+        obj, items = self.scene.objects, self.scene.work_items
+        sp1 = selected.astype(np.int64)
+        cnt = np.where(sp1 > 0, obj["lod_meshlet_counts"][np.arange(len(obj)), np.maximum(sp1 - 1, 0)], 0)
+        n = np.clip(cnt[items["object_index"].astype(np.int64)] - items["local_meshlet_base"].astype(np.int64), 0, 64)
+        tested, active = int(n.sum()), int((n > 0).sum())
+        return {"hiz_build": hiz_bytes(v.width, v.height, True), "vg_select": 164 * len(obj),
+                "vg_cull_test": 24 * len(items) + 80 * active + 44 * tested, "vg_cull_emit": 48 * visible}, visible
+
+    def e2e(self):
+        import torch
+
+        host_depth = [torch.from_numpy(v.depth).pin_memory() for v, *_ in self.passes]
+        host_cam = [torch.from_numpy(np.frombuffer(bytes(v.camera), np.uint8).copy()).pin_memory()
+                    for v, *_ in self.passes]
+        host_cnt = [torch.empty(11, dtype=torch.int32).pin_memory() for _ in self.passes]
+        outs = []
+        for *_, vg in self.passes:
+            cap = max(vg.outputs()["capacity"], 1)
+            outs.append((torch.empty((cap, 5), dtype=torch.int32).pin_memory(),
+                         torch.empty((cap, 4), dtype=torch.int32).pin_memory()))
+        h2d = sum(int(t.numel()) * 4 for t in host_depth) + sum(int(t.numel()) for t in host_cam)
+        stats = {"d2h": 0}
+
+        def run():
+            for i, (v, depth, cam, hz, vg) in enumerate(self.passes):
+                depth.copy_(host_depth[i], non_blocking=True)
+                cam.copy_(host_cam[i], non_blocking=True)
+                hz.execute()
+                vg.execute(cam, hz.publish())
+                host_cnt[i].copy_(vg.outputs()["counters"], non_blocking=True)
+            torch.cuda.current_stream().synchronize()
+            for i, (*_, vg) in enumerate(self.passes):
+                o = vg.outputs()
+                n = int(min(int(host_cnt[i][0]) & 0xFFFFFFFF, o["capacity"]))
+                if n:
+                    outs[i][0][:n].copy_(o["indirect"][:n], non_blocking=True)
+                    outs[i][1][:n].copy_(o["draws"][:n], non_blocking=True)
+                stats["d2h"] += 44 + 36 * n
+            torch.cuda.current_stream().synchronize()
+
+        return run, h2d, stats
+
+    def visible_draws(self) -> int:
+        tot = 0
+        for *_, vg in self.passes:
+            o = vg.outputs()
+            tot += int(min(o["counters"].cpu().numpy().view(np.uint32)[0], o["capacity"]))
+        return tot
+
+
+class BatchedWorkload:
+    """85 views against one device-resident scene in one cooperative launch."""
+
+    def __init__(self, dev, with_plain=True):
+        import torch
+        from helio_b200 import scene as S
+        from helio_b200.passes import BatchedCull, HiZBuildPass, VgScene, VirtualGeometryPass, camera_bytes
+
+        self.name = "batched3"
+        self.wl = S.config(3)
+        self.scene = self.wl.scene
+        self.views = self.wl.views
+        self.units = self.scene.lod0_total * len(self.views)
+        self.vscene = VgScene()
+        self.vscene.upload(S.frame_data(self.scene))
+        self.depths = [torch.from_numpy(v.depth).to(dev) for v in self.views]
+        self.batch = BatchedCull(len(self.views), span_visibility=True)
+        self.batch.prepare(self.vscene, [{"camera": v.camera, "depth": d, "alias_mip0": True,
+                                          "lod_threshold_px": v.lod_threshold_px}
+                                         for v, d in zip(self.views, self.depths)])
+        torch.cuda.synchronize()
+        self.plain = None
+        if with_plain:
+            # The same 85 views through the plain single-view passes, one after another.
+            self.cams = [torch.from_numpy(camera_bytes(v.camera)).to(dev) for v in self.views]
+            self.hz = []
+            for v, d in zip(self.views, self.depths):
+                hz = HiZBuildPass(v.width, v.height, alias_mip0=True)
+                hz.prepare(d)
+                self.hz.append(hz)
+            self.vg = VirtualGeometryPass(self.views[0].width, self.views[0].height)
+            self.vg.prepare(S.frame_data(self.scene))
+            torch.cuda.synchronize()
+            self.plain = self.plain_step
+
+    def step(self):
+        self.batch.execute()
+
+    def plain_step(self):
+        for v, cam, hz in zip(self.views, self.cams, self.hz):
+            hz.execute()
+            self.vg.on_resize(v.width, v.height)
+            self.vg.execute(cam, hz.publish())
+
+    def describe(self):
+        return (f"batched3: {len(self.scene.objects)} instances x {self.scene.lod0_meshlets} LOD0 meshlets "
+                f"(10M), 85 views (1x 3840x2160, 4x 2048^2 orthographic, 16x 512^2 spot, 64x 128^2 probe), "
+                f"one cooperative launch, Hi-Z level 0 = the view's depth")
+
+    def outputs(self):
+        lods, draws = [], 0
+        for i in range(len(self.views)):
+            o = self.batch.view_outputs(i)
+            c = o["counters"].cpu().numpy().view(np.uint32)
+            draws += int(min(c[0], o["capacity"]))
+            lods.append(o["lod"].cpu().numpy()[: len(self.scene.objects)])
+        return np.stack(lods), draws
+
+    def kernel_bytes(self) -> tuple[dict, int]:
+        """Algorithmic bytes of the batched kernel: per view the Hi-Z (depth read + levels
+        1.. written) and the per-object LOD byte, the scene's object stage once per batch
+        (176 B per object: 96 B object fields, 64 B model, 16 B InstanceCullData), 44 B
+        per meshlet of the union over views of each object's selected LOD range, 32 B per
+        active span (16 B written, 16 B read) plus 8 B of span visibility, and 48 B per
+        visible draw (12 B read, 36 B written)."""
+        lods, visible = self.outputs()
+        spans = sum(active_spans(self.scene, lods[v])[0] for v in range(len(self.views)))
+        b = sum(hiz_bytes(v.width, v.height, False) for v in self.views)
+        b += lods.size  # LOD bytes
+        b += 176 * len(self.scene.objects)
+        b += 44 * union_meshlets(self.scene, lods)
+        b += 40 * spans
+        b += 48 * visible
+        return {"batch_cull": b}, visible
+
+    def e2e(self):
+        import torch
+
+        host_depth = [torch.from_numpy(v.depth).pin_memory() for v in self.views]
+        cams = [v.camera for v in self.views]
+        host_cnt = torch.empty((len(self.views), 11), dtype=torch.int32).pin_memory()
+        outs = []
+        for i in range(len(self.views)):
+            cap = max(self.batch.view_outputs(i)["capacity"], 1)
+            outs.append((torch.empty((cap, 5), dtype=torch.int32).pin_memory(),
+                         torch.empty((cap, 4), dtype=torch.int32).pin_memory()))
+        views_out = [self.batch.view_outputs(i) for i in range(len(self.views))]
+        h2d = sum(int(t.numel()) * 4 for t in host_depth) + 368 * len(cams)
+        stats = {"d2h": 0}
+
+        def run():
+            for d, hd in zip(self.depths, host_depth):
+                d.copy_(hd, non_blocking=True)
+            self.batch.set_cameras(cams)
+            self.batch.execute()
+            for i, o in enumerate(views_out):
+                host_cnt[i].copy_(o["counters"], non_blocking=True)
+            torch.cuda.current_stream().synchronize()
+            for i, o in enumerate(views_out):
+                n = int(min(int(host_cnt[i][0]) & 0xFFFFFFFF, o["capacity"]))
+                if n:
+                    outs[i][0][:n].copy_(o["indirect"][:n], non_blocking=True)
+                    outs[i][1][:n].copy_(o["draws"][:n], non_blocking=True)
+                stats["d2h"] += 44 + 36 * n
+            torch.cuda.current_stream().synchronize()
+
+        return run, h2d, stats
+
+
+def build_workload(name, dev, with_plain):
+    return BatchedWorkload(dev, with_plain) if name == "batched3" else PlainWorkload(name, dev)
+
+
+# ── Timing ────────────────────────────────────────────────────────────────────
+
+class Timer:
+    def __init__(self, dev):
+        import torch
+
+        self.torch = torch
+        self.flush_w = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+        self.flush_r = torch.ones(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+        self.sink = torch.empty((), dtype=torch.float32, device=dev)
+
+    def flush(self):
+        # Write a buffer larger than L2, then read another one: the step starts with
+        # none of its inputs in L2 and no dirty line left to write back.
+        self.flush_w.fill_(1.0)
+        self.torch.sum(self.flush_r, dim=0, out=self.sink)
+
+    def graph(self, fn):
+        """fn captured as one CUDA graph (None if the capture is refused)."""
+        torch = self.torch
+        side = torch.cuda.Stream()
+        side.wait_stream(torch.cuda.current_stream())
+        g = torch.cuda.CUDAGraph()
+        try:
+            with torch.cuda.stream(side):
+                fn()
+                torch.cuda.synchronize()
+                with torch.cuda.graph(g, stream=side):
+                    fn()
+            torch.cuda.synchronize()
+            return g
+        except Exception:  # a launch that cannot be captured runs eagerly
+            torch.cuda.synchronize()
+            return None
+
+    def run(self, fn, steps, warmup, graph=True):
+        """Per-step device ms of fn (graph replay when possible)."""
+        torch = self.torch
+        g = self.graph(fn) if graph else None
+        call = g.replay if g is not None else fn
+        for _ in range(max(warmup, 3)):
+            self.flush()
+            call()
+        torch.cuda.synchronize()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        for k in range(steps):
+            self.flush()
+            torch.cuda._sleep(SLEEP_CYCLES)
+            ev[k][0].record()
+            call()
+            ev[k][1].record()
+        torch.cuda.synchronize()
+        return [a.elapsed_time(b) for a, b in ev], g is not None
+
+
+def pct(xs, q):
+    s = sorted(xs)
+    return s[min(len(s) - 1, max(0, int(math.ceil(q * len(s))) - 1))]
 
 
 def run_ours(args, rank, world, local_rank):
     import torch
+    from helio_b200 import dist as D
     from helio_b200 import native as N
-    from helio_b200 import scene as S
-    from helio_b200.passes import HiZBuildPass, VirtualGeometryPass, camera_bytes, device_view
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     lib = N.cull_lib()
-    wl = build_workload(args.workload)
-    sc = wl.scene
-    views = wl.views
-    units = sc.lod0_total * len(views)
+    wl = build_workload(args.workload, dev, not args.no_plain)
+    timer = Timer(dev)
 
-    # Device-resident state, one pass pair per view.
-    stream = torch.cuda.current_stream()
-    passes = []
-    for v in views:
-        depth = torch.from_numpy(v.depth).to(dev)
-        cam = torch.from_numpy(camera_bytes(v.camera)).to(dev)
-        hz = HiZBuildPass(v.width, v.height)
-        hz.prepare(depth)
-        vg = VirtualGeometryPass(v.width, v.height)
-        vg.prepare(S.frame_data(sc))
-        passes.append((v, depth, cam, hz, vg))
+    wl.step()
     torch.cuda.synchronize()
-
-    def step():
-        for v, depth, cam, hz, vg in passes:
-            hz.execute()
-            vg.execute(cam, hz.publish())
-
-    flush_buf = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
-    flush_read = torch.ones(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
-    flush_sink = torch.empty((), dtype=torch.float32, device=dev)
-
-    def flush():
-        # Write a buffer larger than L2, then read another one, so the timed step
-        # starts with no line of its inputs in L2 and no dirty line to write back.
-        flush_buf.fill_(1.0)
-        torch.sum(flush_read, dim=0, out=flush_sink)
-
-    for _ in range(max(args.warmup, 3)):
-        flush()
-        step()
-    torch.cuda.synchronize()
-    for v, depth, cam, hz, vg in passes:
-        vg.device_status()
     launches0 = lib.helio_kernel_launch_count()
-    step()
+    wl.step()
     torch.cuda.synchronize()
     launches_per_step = lib.helio_kernel_launch_count() - launches0
 
-    # The step as one CUDA graph (every launch of the step, replayed by one call).
-    side = torch.cuda.Stream()
-    side.wait_stream(torch.cuda.current_stream())
-    graph = torch.cuda.CUDAGraph()
-    with torch.cuda.stream(side):
-        step()  # first launches outside capture
-        torch.cuda.synchronize()
-        with torch.cuda.graph(graph, stream=side):
-            step()
-    torch.cuda.synchronize()
-
-    def queued():
-        # A short on-device delay ahead of each timed step: the host queues the
-        # whole step meanwhile, so the events time the GPU, not the enqueue.
-        torch.cuda._sleep(200_000)
-
-    for _ in range(max(args.warmup, 3)):
-        flush()
-        graph.replay()
-    torch.cuda.synchronize()
-
-    # Timed region: K graph replays, each bracketed by events, L2 flushed in between.
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     clocks = Clocks(local_rank)
     if world > 1:
         torch.distributed.barrier()
     clocks.start()
-    torch.cuda.synchronize()
-    for k in range(args.steps):
-        flush()
-        queued()
-        ev[k][0].record()
-        graph.replay()
-        ev[k][1].record()
-    torch.cuda.synchronize()
-    launches = launches_per_step * args.steps
+    step_ms, graphed = timer.run(wl.step, args.steps, args.warmup)
     clk = clocks.stop()
-    step_ms = [a.elapsed_time(b) for a, b in ev]
-    total_ms = float(sum(step_ms))
-    if world > 1:
-        t = torch.tensor([total_ms], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t.item())
-        torch.distributed.barrier()
-    value = units * args.steps * world / (total_ms / 1e3)
+    total_ms = D.max_over_ranks(sum(step_ms), dev)
+    value = wl.units * args.steps * world / (total_ms / 1e3)
 
-    # Per-kernel device time (event profiler, same steps, separate pass).
+    # Per-kernel device time (event profiler around every launch, eager, queued ahead).
     lib.helio_profiler_reset()
     lib.helio_profiler_enable(1)
     for _ in range(args.steps):
-        flush()
-        queued()
-        step()
+        timer.flush()
+        torch.cuda._sleep(SLEEP_CYCLES)
+        wl.step()
     torch.cuda.synchronize()
     lib.helio_profiler_enable(0)
     prof = N.profiler_collect()
     lib.helio_profiler_reset()
-
-    # Algorithmic bytes per launch from the step's own outputs.
-    outs = []
-    for v, depth, cam, hz, vg in passes:
-        o = vg.outputs()
-        counters = o["counters"].cpu().numpy().view(np.uint32)
-        selected = o["objects"].cpu().numpy().view(np.uint32)[:, 3]
-        visible = int(min(counters[0], o["capacity"]))
-        outs.append((vg_algorithmic_bytes(sc, selected, visible), visible, v))
-    kb = {"hiz_build": [hiz_bytes(v.width, v.height, True) for _, _, v in outs],
-          "vg_select": [a["select"] for a, _, _ in outs],
-          "vg_cull_test": [a["cull_test"] for a, _, _ in outs], "vg_cull_emit": [a["cull_emit"] for a, _, _ in outs]}
+    kb, visible = wl.kernel_bytes()
     kernels = {}
     tot_prof = sum(ms for _, ms in prof.values()) or 1.0
     for name, (n, ms) in prof.items():
         entry = {"launches": n, "avg_us": 1e3 * ms / max(n, 1), "share": ms / tot_prof}
         if name in kb:
-            per_launch = float(np.mean(kb[name]))
-            entry["algorithmic_bytes_per_launch"] = per_launch
-            entry["achieved_gbs"] = per_launch / (ms / max(n, 1) / 1e3) / 1e9
+            entry["algorithmic_bytes_per_launch"] = float(kb[name])
+            entry["achieved_gbs"] = kb[name] / (ms / max(n, 1) / 1e3) / 1e9
         kernels[name] = entry
     dom = max((k for k in kernels if "achieved_gbs" in kernels[k]), key=lambda k: kernels[k]["share"])
     peak, peak_kind = peaks()
@@ -286,140 +466,120 @@ def run_ours(args, rank, world, local_rank):
                 "peak_kind": peak_kind, "unit": "GB/s", "frac": kernels[dom]["achieved_gbs"] / peak,
                 "traffic": traffic}
 
-    # End to end through the C-ABI with host buffers.
+    extra = {}
+    if hasattr(wl, "batch"):
+        timer.flush()
+        torch.cuda._sleep(SLEEP_CYCLES)
+        wl.step()
+        extra["phases_us"] = wl.batch.phase_times()
+    if getattr(wl, "plain", None) is not None:
+        plain_ms, plain_graphed = timer.run(wl.plain, max(3, args.steps // 4), args.warmup)
+        pm = D.max_over_ranks(sum(plain_ms), dev) / len(plain_ms)
+        extra["plain_per_view"] = {"ms_per_step": pm, "value": wl.units / (pm / 1e3), "unit": "meshlets/s",
+                                   "graph": plain_graphed, "views": len(wl.views),
+                                   "batched_speedup": pm / (total_ms / args.steps)}
+
     e2e = None
     if not args.no_e2e:
-        host_depth = [torch.from_numpy(v.depth).pin_memory() for v, *_ in passes]
-        host_cam = [torch.from_numpy(camera_bytes(v.camera)).pin_memory() for v, *_ in passes]
-        host_cnt = [torch.empty(11, dtype=torch.int32).pin_memory() for _ in passes]
-        host_out = []
-        for _, _, _, _, vg in passes:
-            cap = vg.outputs()["capacity"]
-            host_out.append((torch.empty((max(cap, 1), 5), dtype=torch.int32).pin_memory(),
-                             torch.empty((max(cap, 1), 4), dtype=torch.int32).pin_memory()))
-        h2d = sum(int(t.numel()) * 4 for t in host_depth) + sum(int(t.numel()) for t in host_cam)
-        d2h_total = 0
-
-        def e2e_step():
-            nonlocal d2h_total
-            for i, (v, depth, cam, hz, vg) in enumerate(passes):
-                depth.copy_(host_depth[i], non_blocking=True)
-                cam.copy_(host_cam[i], non_blocking=True)
-                hz.execute()
-                vg.execute(cam, hz.publish())
-                o = vg.outputs()
-                host_cnt[i].copy_(o["counters"], non_blocking=True)
-            torch.cuda.current_stream().synchronize()
-            for i, (v, depth, cam, hz, vg) in enumerate(passes):
-                o = vg.outputs()
-                n = int(min(int(host_cnt[i][0]) & 0xFFFFFFFF, o["capacity"]))
-                if n:
-                    host_out[i][0][:n].copy_(o["indirect"][:n], non_blocking=True)
-                    host_out[i][1][:n].copy_(o["draws"][:n], non_blocking=True)
-                d2h_total += 44 + 36 * n
-            torch.cuda.current_stream().synchronize()
-
+        run, h2d, stats = wl.e2e()
         for _ in range(max(args.warmup, 3)):
-            e2e_step()
-        d2h_total = 0
+            run()
+        stats["d2h"] = 0
         ee = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
         for k in range(args.steps):
-            flush()
+            timer.flush()
             ee[k][0].record()
-            e2e_step()
+            run()
             ee[k][1].record()
         torch.cuda.synchronize()
-        e2e_ms = float(sum(a.elapsed_time(b) for a, b in ee))
-        if world > 1:
-            t = torch.tensor([e2e_ms], device=dev)
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            e2e_ms = float(t.item())
-        e2e = {"value": units * args.steps * world / (e2e_ms / 1e3), "unit": "meshlets/s",
-               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": int(d2h_total / args.steps),
+        e2e_ms = D.max_over_ranks(float(sum(a.elapsed_time(b) for a, b in ee)), dev)
+        e2e = {"value": wl.units * args.steps * world / (e2e_ms / 1e3), "unit": "meshlets/s",
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": int(stats["d2h"] / args.steps),
                "ms_per_step": e2e_ms / args.steps}
 
-    cpu = None
-    if rank == 0 and world == 1:
-        cpu = cpu_baseline(wl, args.cpu_seconds)
-
-    srt = sorted(step_ms)
+    cpu = cpu_baseline(wl.wl, args.cpu_seconds) if (rank == 0 and world == 1) else None
     line = {
         "metric": "meshlets culled/s", "value": value, "unit": "meshlets/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator)",
-        "config": {"workload": f"{args.workload}: {wl_desc(wl)}", "views": len(views),
-                   "lod0_meshlets_per_view": sc.lod0_total,
+        "config": {"workload": wl.describe(), "views": len(wl.views), "lod0_meshlets_per_view": wl.scene.lod0_total,
                    "l2": "flushed between timed steps (256 MB write, then 256 MB read)",
-                   "timing": "CUDA-graph replay of the whole step, CUDA events on the launching stream",
+                   "timing": ("CUDA-graph replay of the whole step" if graphed else "eager launches") +
+                             ", CUDA events on the launching stream",
                    "parallelism": f"replica x{world}" if world > 1 else "single GPU"},
-        "latency_ms": {"p50": srt[len(srt) // 2], "p99": srt[min(len(srt) - 1, int(math.ceil(0.99 * len(srt))) - 1)]},
+        "latency_ms": {"p50": pct(step_ms, 0.5), "p99": pct(step_ms, 0.99)},
         "roofline": roofline, "kernels": kernels, "cpu_baseline": cpu, "e2e": e2e,
-        "gpu_launches": int(launches), "clocks": clk,
-        "visible_draws_per_step": int(sum(vis for _, vis, _ in outs)),
+        "gpu_launches": int(launches_per_step * args.steps), "clocks": clk, "visible_draws_per_step": visible,
     }
+    line.update(extra)
     return line
 
 
-def wl_desc(wl) -> str:
-    sc = wl.scene
-    v = wl.views[0]
-    return (f"{len(sc.objects)} instances x {sc.lod0_meshlets} LOD0 meshlets, {len(wl.views)} view(s), "
-            f"first {v.width}x{v.height}")
+# ── CPU baseline / reference arm (the oracle) ────────────────────────────────
 
-
-def oracle_step(wl, threads: int):
+def oracle_views(wl, views, threads: int) -> int:
     from oracle import oracle as O
     from helio_b200 import native as N
 
     cd = np.dtype(N.InstanceCullData)
     vis = 0
-    for v in wl.views:
+    for v in views:
         levels = O.hiz_build(v.depth)
         r = O.run_view(wl.scene, v.camera, v.width, v.height, levels, v.lod_threshold_px, None, 11, threads, cd)
         vis += int(r["counters"][0])
     return vis
 
 
+def sample_views(wl, k: int):
+    """Every 5th view (offset by k) of a many-view workload; all views otherwise."""
+    return wl.views if len(wl.views) < 10 else wl.views[k % 5::5]
+
+
 def cpu_baseline(wl, seconds: float) -> dict:
-    """The oracle timed on this host on a bounded sample (whole steps, repeated until
-    `seconds` elapse, at least one)."""
     threads = max(1, os.cpu_count() or 1)
     t0 = time.perf_counter()
-    n = 0
+    n_units = 0
+    k = 0
     while True:
-        oracle_step(wl, threads)
-        n += 1
-        if time.perf_counter() - t0 >= seconds or n >= 50:
+        views = sample_views(wl, k)
+        oracle_views(wl, views, threads)
+        n_units += wl.scene.lod0_total * len(views)
+        k += 1
+        if time.perf_counter() - t0 >= seconds or k >= 50:
             break
     dt = time.perf_counter() - t0
-    units = wl.scene.lod0_total * len(wl.views) * n
-    return {"value": units / dt, "unit": "meshlets/s", "cores": threads, "kind": "port",
-            "sample": f"{n} full step(s) of the same workload (Hi-Z + select + cull, multi-threaded select/cull)",
-            "seconds": dt}
+    return {"value": n_units / dt, "unit": "meshlets/s", "cores": threads, "kind": "port",
+            "sample": f"{k} step(s) of {len(sample_views(wl, 0))} view(s) each (Hi-Z + select + cull per view, "
+                      f"multi-threaded select / cull), {dt:.1f} s", "seconds": dt}
 
 
 def run_reference(args):
-    wl = build_workload(args.workload)
+    from helio_b200 import scene as S
+
+    cfg = {"batched3": 3, "plain2": 2, "plain1": 1, "plain0": 0}[args.workload]
+    wl = S.config(cfg)
     threads = max(1, os.cpu_count() or 1)
-    for _ in range(args.warmup):
-        oracle_step(wl, threads)
-    times = []
-    for _ in range(args.steps):
+    for k in range(args.warmup):
+        oracle_views(wl, sample_views(wl, k), threads)
+    times, units = [], 0
+    for k in range(args.steps):
+        views = sample_views(wl, k)
         t0 = time.perf_counter()
-        oracle_step(wl, threads)
+        oracle_views(wl, views, threads)
         times.append(time.perf_counter() - t0)
-    units = wl.scene.lod0_total * len(wl.views)
-    value = units * len(times) / sum(times)
+        units += wl.scene.lod0_total * len(views)
+    value = units / sum(times)
+    sample = (f"each step: {len(sample_views(wl, 0))} of {len(wl.views)} views (every 5th, rotating) of the same "
+              f"workload" if len(wl.views) >= 10 else "each step: the full workload")
     return {
         "metric": "meshlets culled/s", "value": value, "unit": "meshlets/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded generator)", "impl": "reference",
-        "config": {"workload": f"{args.workload}: {wl_desc(wl)}", "views": len(wl.views),
-                   "lod0_meshlets_per_view": wl.scene.lod0_total},
+        "config": {"workload": args.workload, "views": len(wl.views), "lod0_meshlets_per_view": wl.scene.lod0_total},
         "cpu_baseline": {"value": value, "unit": "meshlets/s", "cores": threads, "kind": "port",
-                         "sample": f"{args.steps} full steps on the host cores (CPU restatement of the reference "
-                                   f"shaders; the WGSL itself cannot run on this machine)"},
+                         "sample": sample + "; CPU restatement of the reference shaders (the WGSL itself cannot "
+                                            "run on this machine)"},
         "e2e": {"value": value, "unit": "meshlets/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 
@@ -434,13 +594,9 @@ def main():
             print(json.dumps(run_reference(args)), flush=True)
         return 0
     if world > 1:
-        import datetime
+        from helio_b200 import dist as D
 
-        import torch
-
-        torch.cuda.set_device(local_rank)
-        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                             device_id=torch.device("cuda", local_rank))
+        D.init("nccl", timeout_s=120)
     line = run_ours(args, rank, world, local_rank)
     if rank == 0:
         print(json.dumps(line), flush=True)

@@ -34,8 +34,7 @@ namespace {
 struct SelView {
     Planes planes;
     float4 pos_near;
-    float focal, thr;
-    uint32_t pad[2];
+    float focal, thr, thr_lo, thr_hi;  // thr_lo / thr_hi: QuotientBound margins of thr
 };
 static_assert(sizeof(SelView) == 128, "SelView layout");
 
@@ -47,7 +46,8 @@ constexpr size_t kSmSelMax = kSmSelHist + 32 * kBatchMaxViews;                //
 constexpr size_t kSmHizJob = kSmSelMax + 4 * kBatchMaxViews;                  // HizJob
 constexpr size_t kSmHizM3 = kSmHizJob + ((sizeof(HizJob) + 15) / 16) * 16;    // float[8][9]
 constexpr size_t kSmMisc = kSmHizM3 + 8 * 9 * 4;                              // u32[64]
-constexpr size_t kSmTotal = kSmMisc + 64 * 4;
+constexpr size_t kSmTileBegin = kSmMisc + 64 * 4;                             // u32[kBatchMaxViews]
+constexpr size_t kSmTotal = kSmTileBegin + 4 * kBatchMaxViews;
 // Phases 2..6 reuse the region from offset 0.
 constexpr size_t kSmTestViews = 0;                                       // CullView per warp
 constexpr size_t kSmTestBits = kSmTestViews + sizeof(CullView) * 8;      // u32[8][66]
@@ -183,93 +183,124 @@ __device__ void phase_setup(const BatchParams& P) {
     }
 }
 
-// ── Phase 1a: one Hi-Z tile ───────────────────────────────────────────────────
+// ── Phase 1a: one Hi-Z tile (levels 0..6; the tails follow the phase barrier) ─
+// The view's HizJob stays in shared memory while consecutive tiles of a CTA
+// belong to the same view (s_job holds its index, ~0u before the first tile).
+__device__ void load_hiz_job(const BatchParams& P, uint32_t v, char* sm) {
+    // Warp 0 copies the job word by word.
+    uint32_t* dst = reinterpret_cast<uint32_t*>(sm + kSmHizJob);
+    const uint32_t* src = reinterpret_cast<const uint32_t*>(&P.views[v].hiz);
+    for (uint32_t w = threadIdx.x & 31u; w < sizeof(HizJob) / 4; w += 32u) dst[w] = __ldg(src + w);
+}
+
 __device__ void phase_hiz_tile(const BatchParams& P, uint32_t tile, char* sm) {
-    HizJob& J = *reinterpret_cast<HizJob*>(sm + kSmHizJob);
-    uint32_t* s_job = reinterpret_cast<uint32_t*>(sm + kSmMisc);
+    const HizJob& J = *reinterpret_cast<const HizJob*>(sm + kSmHizJob);
+    volatile uint32_t* s_job = reinterpret_cast<volatile uint32_t*>(sm + kSmMisc);
+    const uint32_t* s_tb = reinterpret_cast<const uint32_t*>(sm + kSmTileBegin);
     __syncthreads();  // the previous unit's warp 0 may still read s_m3 / J
-    if (threadIdx.x == 0) {
+    if (threadIdx.x < 32) {
         uint32_t lo = 0, hi = P.view_count - 1;
         while (lo < hi) {
             const uint32_t mid = (lo + hi + 1) >> 1;
-            if (P.views[mid].hiz.tile_begin <= tile) lo = mid;
+            if (s_tb[mid] <= tile) lo = mid;
             else hi = mid - 1;
         }
-        J = P.views[lo].hiz;
-        *s_job = lo;
+        if (*s_job != lo) {
+            load_hiz_job(P, lo, sm);
+            __syncwarp();
+            if (threadIdx.x == 0) *s_job = lo;
+        }
     }
     __syncthreads();
-    hiz_tile(J, *s_job, tile - J.tile_begin, P.hiz_tickets, reinterpret_cast<float(*)[9]>(sm + kSmHizM3));
+    hiz_tile(J, *s_job, tile - J.tile_begin, nullptr, reinterpret_cast<float(*)[9]>(sm + kSmHizM3));
 }
 
-// ── Phase 1b: object select against every view (vg_cull.wgsl:282-352) ────────
-__device__ void phase_select_chunk(const BatchParams& P, uint32_t chunk, char* sm) {
+// ── Phase 1b: object select against a group of views (vg_cull.wgsl:282-352) ──
+// Unit = (256-object chunk, group of kSelectViews views): the object is loaded once
+// per unit and tested against each view of the group.
+constexpr uint32_t kSelectViews = 16;
+
+__device__ void phase_select_chunk(const BatchParams& P, uint32_t chunk, uint32_t v_begin, uint32_t v_end, char* sm) {
     const SelView* s_sv = reinterpret_cast<const SelView*>(sm + kSmSelViews);
     uint32_t* s_cnt = reinterpret_cast<uint32_t*>(sm + kSmSelCnt);
     uint32_t* s_hist = reinterpret_cast<uint32_t*>(sm + kSmSelHist);
     uint32_t* s_max = reinterpret_cast<uint32_t*>(sm + kSmSelMax);
-    const uint32_t V = P.view_count, tid = threadIdx.x;
+    const uint32_t tid = threadIdx.x, nv = v_end - v_begin;
     __syncthreads();
-    for (uint32_t k = tid; k < V * 10u; k += kBatchThreads) {
-        if (k < V) s_cnt[k] = 0u;
-        else if (k < 9u * V) s_hist[k - V] = 0u;
-        else s_max[k - 9u * V] = 0u;
+    for (uint32_t k = tid; k < nv * 10u; k += kBatchThreads) {
+        const uint32_t v = v_begin + k % nv, f = k / nv;  // f: 0 count, 1..8 histogram, 9 max
+        if (f == 0) s_cnt[v] = 0u;
+        else if (f <= 8) s_hist[v * 8u + (f - 1u)] = 0u;
+        else s_max[v] = 0u;
     }
     __syncthreads();
     const VgSceneDev& S = P.scene;
-    const uint32_t o = chunk * kBatchChunk + tid;
-    if (o < S.object_count) {
-        const HelioGpuVgObject* obj = S.objects + o;
-        const uint4 head = __ldg(reinterpret_cast<const uint4*>(obj));
-        const float4 lb = __ldg(reinterpret_cast<const float4*>(obj->local_bounds));
-        const float4 e0 = __ldg(reinterpret_cast<const float4*>(obj->lod_errors));
-        const float4 e1 = __ldg(reinterpret_cast<const float4*>(obj->lod_errors + 4));
-        const uint4 c0 = __ldg(reinterpret_cast<const uint4*>(obj->lod_meshlet_counts));
-        const uint4 c1 = __ldg(reinterpret_cast<const uint4*>(obj->lod_meshlet_counts + 4));
-        const uint32_t lod_count = min(head.y, 8u), ii = head.x;
-        bool valid = false;
-        F3 c = f3(0.f, 0.f, 0.f);
-        float wr = 0.0f, max_scale = 0.0f;
-        if (lod_count > 0u && ii < S.instance_count) {
-            const HelioInstanceCullData cd = load_cull(S.cull + ii);
-            const Mat4 model = ldg_mat4(S.instances[ii].model);
-            if (cd.valid_transform != 0u) {
-                valid = true;
-                max_scale = cd.max_scale;
-                c = mat4_point3(model, f3(lb.x, lb.y, lb.z));
-                wr = fmaxf(fmul(lb.w, cd.max_scale), 0.0f);
+    const uint32_t o = chunk * kBatchChunk + tid, lane = tid & 31u;
+    // Lanes past the last object take part in the warp reductions as invisible.
+    const bool in_range = o < S.object_count;
+    const HelioGpuVgObject* obj = S.objects + (in_range ? o : 0u);
+    const uint4 head = __ldg(reinterpret_cast<const uint4*>(obj));
+    const float4 lb = __ldg(reinterpret_cast<const float4*>(obj->local_bounds));
+    const float4 e0 = __ldg(reinterpret_cast<const float4*>(obj->lod_errors));
+    const float4 e1 = __ldg(reinterpret_cast<const float4*>(obj->lod_errors + 4));
+    const uint4 c0 = __ldg(reinterpret_cast<const uint4*>(obj->lod_meshlet_counts));
+    const uint4 c1 = __ldg(reinterpret_cast<const uint4*>(obj->lod_meshlet_counts + 4));
+    const uint32_t lod_count = min(head.y, 8u), ii = head.x;
+    bool valid = false;
+    F3 c = f3(0.f, 0.f, 0.f);
+    float wr = 0.0f, max_scale = 0.0f;
+    if (in_range && lod_count > 0u && ii < S.instance_count) {
+        const HelioInstanceCullData cd = load_cull(S.cull + ii);
+        const Mat4 model = ldg_mat4(S.instances[ii].model);
+        if (cd.valid_transform != 0u) {
+            valid = true;
+            max_scale = cd.max_scale;
+            c = mat4_point3(model, f3(lb.x, lb.y, lb.z));
+            wr = fmaxf(fmul(lb.w, cd.max_scale), 0.0f);
+        }
+    }
+    const float err[8] = {e0.x, e0.y, e0.z, e0.w, e1.x, e1.y, e1.z, e1.w};
+    const uint32_t cnts[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
+    uint8_t* lod_col = P.lod + o;
+    for (uint32_t v = v_begin; v < v_end; ++v) {
+        const bool vis = valid && sphere_visible_vg(s_sv[v].planes, c, wr);
+        uint32_t lod = 0, cnt = c0.x;
+        if (vis) {
+            const float4 pn = s_sv[v].pos_near;
+            const F3 d = sub3(c, f3(pn.x, pn.y, pn.z));
+            const float dist = fsqrt(dot3(d, d));
+            const float closest = fmaxf(fsub(dist, wr), fmaxf(pn.w, 1.0e-4f));
+            const float focal = s_sv[v].focal;
+            const QuotientBound qb{s_sv[v].thr, s_sv[v].thr_lo, s_sv[v].thr_hi};
+            const float r = quotient_rcp(closest);
+#pragma unroll
+            for (uint32_t level = 1; level < 8; ++level) {
+                if (level >= lod_count) break;
+                // px = err * max_scale * focal / closest; px <= threshold keeps the level.
+                if (quotient_le(fmul(fmul(err[level], max_scale), focal), closest, r, qb)) {
+                    lod = level;
+                    cnt = cnts[level];
+                } else {
+                    break;
+                }
             }
         }
-        const float err[8] = {e0.x, e0.y, e0.z, e0.w, e1.x, e1.y, e1.z, e1.w};
-        const uint32_t cnts[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
-        uint8_t* lod_col = P.lod + o;
-        for (uint32_t v = 0; v < V; ++v) {
-            uint32_t sel = 0;
-            if (valid && sphere_visible_vg(s_sv[v].planes, c, wr)) {
-                const float4 pn = s_sv[v].pos_near;
-                const F3 d = sub3(c, f3(pn.x, pn.y, pn.z));
-                const float dist = fsqrt(dot3(d, d));
-                const float closest = fmaxf(fsub(dist, wr), fmaxf(pn.w, 1.0e-4f));
-                const float focal = s_sv[v].focal, thr = s_sv[v].thr;
-                uint32_t lod = 0;
-#pragma unroll
-                for (uint32_t level = 1; level < 8; ++level) {
-                    if (level >= lod_count) break;
-                    const float px = fdiv(fmul(fmul(err[level], max_scale), focal), closest);
-                    if (px <= thr) lod = level;
-                    else break;
-                }
-                sel = lod + 1u;
-                const uint32_t spans = (cnts[lod] + 63u) >> 6;
+        if (in_range) lod_col[(size_t)v * S.object_count] = (uint8_t)(vis ? lod + 1u : 0u);
+        if (__any_sync(0xffffffffu, vis)) {
+            const uint32_t spans = __reduce_add_sync(0xffffffffu, vis ? (cnt + 63u) >> 6 : 0u);
+            // lod_count - 1 + 1: 0 means no visible object
+            const uint32_t top = __reduce_max_sync(0xffffffffu, vis ? lod_count : 0u);
+            const uint32_t key = vis ? lod : 8u;
+            const uint32_t peers = __match_any_sync(0xffffffffu, key);
+            if (key < 8u && lane == (uint32_t)(__ffs(peers) - 1)) atomicAdd(s_hist + v * 8u + key, __popc(peers));
+            if (lane == 0) {
                 if (spans) atomicAdd(s_cnt + v, spans);
-                atomicAdd(s_hist + v * 8u + lod, 1u);
-                atomicMax(s_max + v, lod_count);  // lod_count - 1 + 1: 0 means no visible object
+                atomicMax(s_max + v, top);
             }
-            lod_col[(size_t)v * S.object_count] = (uint8_t)sel;
         }
     }
     __syncthreads();
-    for (uint32_t v = tid; v < V; v += kBatchThreads) {
+    for (uint32_t v = v_begin + tid; v < v_end; v += kBatchThreads) {
         P.chunk_counts[(size_t)v * P.object_chunks + chunk] = s_cnt[v];
         uint32_t* counters = P.views[v].counters;
         for (uint32_t l = 0; l < 8u; ++l)
@@ -284,6 +315,18 @@ __device__ void phase_expand(const BatchParams& P, char* sm) {
     uint32_t* s_tmp = reinterpret_cast<uint32_t*>(sm + kSmMisc);
     const uint32_t V = P.view_count, C = P.object_chunks, tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
+    // Hi-Z levels 7.. of each view, by warp 0 of CTA v (mod grid), from the level 6
+    // that phase 1 wrote; the test phase reads them after the next barrier.
+    if (warp == 0) {
+        const HizJob& J = *reinterpret_cast<const HizJob*>(sm + kSmHizJob);
+        for (uint32_t v = blockIdx.x; v < V; v += gridDim.x) {
+            if (P.views[v].hiz.mip_count <= 7u) continue;
+            load_hiz_job(P, v, sm);
+            __syncwarp();
+            hiz_tail_warp(J);
+            __syncwarp();
+        }
+    }
     // Padded first span of every view (a multiple of 32).
     {
         uint32_t padded = 0;
@@ -303,36 +346,49 @@ __device__ void phase_expand(const BatchParams& P, char* sm) {
     const VgSceneDev& S = P.scene;
     const uint32_t n_units = V * C;
     const uint32_t gw = blockIdx.x * (kBatchThreads / 32) + warp, GW = gridDim.x * (kBatchThreads / 32);
-    for (uint32_t base = gw * 32u; base < n_units; base += GW * 32u) {
-        const uint32_t u = base + lane;
+    // Units are dealt out strided (lane k of warp w looks at unit w + k * W) so that the
+    // heavy consecutive chunks of a large view spread over many warps.
+    for (uint32_t k0 = 0; gw + (size_t)k0 * GW < n_units; k0 += 32u) {
+        const size_t u = gw + (size_t)(k0 + lane) * GW;
         const uint32_t cnt = u < n_units ? ld_cg(P.chunk_counts + u) : 0u;
         uint32_t mask = __ballot_sync(0xffffffffu, cnt != 0u);
         while (mask) {
-            const uint32_t uu = base + (__ffs(mask) - 1);
+            const uint32_t uu = gw + (k0 + (__ffs(mask) - 1)) * GW;
             mask &= mask - 1u;
             const uint32_t v = uu / C, ch = uu - v * C;
             uint32_t pos = s_vstart[v] + (ld_cg(P.chunk_offs + uu) - ld_cg(P.chunk_offs + (size_t)v * C));
-            for (uint32_t r = 0; r < kBatchChunk / 32u; ++r) {
+            // All loads of the chunk's 256 objects are issued before any is used: one
+            // round trip for the LOD bytes, one for the objects' selected ranges.
+            constexpr int R = kBatchChunk / 32;
+            const uint8_t* lrow = P.lod + (size_t)v * S.object_count;
+            uint32_t sel[R], count[R], first[R], inst[R];
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
                 const uint32_t o = ch * kBatchChunk + r * 32u + lane;
-                uint32_t ns = 0, first = 0, count = 0, inst = 0, lod = 0;
-                if (o < S.object_count) {
-                    const uint32_t sel = __ldcg(P.lod + (size_t)v * S.object_count + o);
-                    if (sel) {
-                        lod = sel - 1u;
-                        const HelioGpuVgObject* obj = S.objects + o;
-                        count = __ldg(&obj->lod_meshlet_counts[lod]);
-                        first = __ldg(&obj->lod_first_meshlets[lod]);
-                        inst = __ldg(&obj->instance_index);
-                        ns = (count + 63u) >> 6;
-                    }
+                sel[r] = o < S.object_count ? (uint32_t)__ldcg(lrow + o) : 0u;
+            }
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                count[r] = first[r] = inst[r] = 0u;
+                if (sel[r]) {
+                    const HelioGpuVgObject* obj = S.objects + (ch * kBatchChunk + r * 32u + lane);
+                    count[r] = __ldg(&obj->lod_meshlet_counts[sel[r] - 1u]);
+                    first[r] = __ldg(&obj->lod_first_meshlets[sel[r] - 1u]);
+                    inst[r] = __ldg(&obj->instance_index);
                 }
+            }
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const uint32_t o = ch * kBatchChunk + r * 32u + lane;
+                const uint32_t lod = sel[r] ? sel[r] - 1u : 0u;
+                const uint32_t ns = (count[r] + 63u) >> 6;
                 const uint32_t inc = warp_inclusive(ns);
                 const uint32_t total = __shfl_sync(0xffffffffu, inc, 31);
                 uint32_t p = pos + inc - ns;
                 for (uint32_t j = 0; j < ns; ++j, ++p) {
                     if (p < P.span_capacity) {
-                        const uint32_t n = min(64u, count - 64u * j);
-                        P.spans[p] = make_uint4(first + 64u * j, n | (lod << 8) | (v << 16), inst, o);
+                        const uint32_t n = min(64u, count[r] - 64u * j);
+                        P.spans[p] = make_uint4(first[r] + 64u * j, n | (lod << 8) | (v << 16), inst[r], o);
                     }
                 }
                 pos += total;
@@ -420,59 +476,98 @@ __device__ void phase_test(const BatchParams& P, uint32_t groups, char* sm) {
     }
 }
 
+// Visible meshlets of a group: the set bits of all its window ballots (lane k holds
+// windows k and k + 32).
+__device__ __forceinline__ uint32_t cnt_of(uint32_t lo, uint32_t hi) {
+    uint32_t c = __popc(lo) + __popc(hi);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    return c;
+}
+
 // ── Phase 6: emission, per view, in the canonical order ───────────────────────
 __device__ void phase_emit(const BatchParams& P, uint32_t groups) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const VgSceneDev& S = P.scene;
     const uint32_t gw = blockIdx.x * (kBatchThreads / 32) + warp, GW = gridDim.x * (kBatchThreads / 32);
-    for (uint32_t base = gw * 32u; base < groups; base += GW * 32u) {
-        const uint32_t gl = base + lane;
+    // Groups are dealt out strided (lane k of warp w looks at group w + k * W): the heavy
+    // consecutive groups of a large view spread over many warps.
+    for (uint32_t k0 = 0; gw + (size_t)k0 * GW < groups; k0 += 32u) {
+        const size_t gl = gw + (size_t)(k0 + lane) * GW;
         const uint32_t cnt = gl < groups ? ld_cg(P.group_counts + gl) : 0u;
         uint32_t mask = __ballot_sync(0xffffffffu, cnt != 0u);
         while (mask) {
-            const uint32_t g = base + (__ffs(mask) - 1);
+            const uint32_t g = gw + (k0 + (__ffs(mask) - 1)) * GW;
             mask &= mask - 1u;
+            // Round trip 1: the group's spans and its scan offset.
+            const uint32_t goff = ld_cg(P.group_offs + g);
             const GroupSpans gs = load_group(P, g);
             if (gs.view >= P.view_count) continue;
+            // Round trip 2: the view's first group, its table entry and every window's ballot.
             const BatchViewDev& V = P.views[gs.view];
             const uint32_t first_group = ld_cg(P.view_span_start + gs.view) >> 5;
-            const uint32_t count = ld_cg(P.group_counts + g);
-            uint32_t slot0 = ld_cg(P.group_offs + g) - ld_cg(P.group_offs + first_group);
             const uint32_t cap = V.capacity;
-            if (lane == 0) {
-                atomicAdd(V.counters + 0, count);
-                const unsigned long long end = (unsigned long long)slot0 + count;
-                const unsigned long long lo = slot0 > cap ? slot0 : cap;
-                if (end > lo) atomicAdd(V.counters + 1, (uint32_t)(end - lo));
-            }
+            HelioDrawIndexedIndirectArgs* indirect = V.indirect;
+            HelioGpuVgDraw* draws = V.draws;
+            uint32_t* counters = V.counters;
             const uint32_t windows = (gs.total + 31u) >> 5;
             const uint32_t* gbits = P.group_bits + (size_t)g * kWindowsPerWarp;
-            for (uint32_t win = 0; win < windows; ++win) {
-                const uint32_t b = ld_cg(gbits + win);
-                if (b == 0u) continue;
-                const uint32_t s = win * 32u + lane;
-                const int j = owner_lane(gs.off, s);
-                const uint32_t j_off = __shfl_sync(0xffffffffu, gs.off, j);
-                const uint32_t j_first = __shfl_sync(0xffffffffu, gs.first, j);
-                const uint32_t j_inst = __shfl_sync(0xffffffffu, gs.inst, j);
-                const uint32_t j_lod = __shfl_sync(0xffffffffu, gs.lod, j);
-                if ((b >> lane) & 1u) {
-                    const uint32_t slot = slot0 + __popc(b & ((1u << lane) - 1u));
-                    if (slot < cap) {
-                        const uint32_t mi = j_first + (s - j_off);
-                        const uint4 d = __ldg(S.m_draw + mi);
-                        uint32_t* out = reinterpret_cast<uint32_t*>(V.indirect + slot);
-                        out[0] = d.y;
-                        out[1] = 1u;
-                        out[2] = d.x;
-                        out[3] = d.z;
-                        out[4] = slot;
-                        reinterpret_cast<uint4*>(V.draws)[slot] = make_uint4(j_inst, mi, j_lod, 0u);
-                    }
+            const uint32_t bits_lo = (uint32_t)lane < windows ? ld_cg(gbits + lane) : 0u;
+            const uint32_t bits_hi = (uint32_t)lane + 32u < windows ? ld_cg(gbits + lane + 32) : 0u;
+            const uint32_t count = cnt_of(bits_lo, bits_hi);
+            uint32_t slot0 = goff - ld_cg(P.group_offs + first_group);
+            if (lane == 0) {
+                atomicAdd(counters + 0, count);
+                const unsigned long long end = (unsigned long long)slot0 + count;
+                const unsigned long long lo = slot0 > cap ? slot0 : cap;
+                if (end > lo) atomicAdd(counters + 1, (uint32_t)(end - lo));
+            }
+            // Windows in groups of 4: the draw records of 4 windows are loaded before
+            // any of them is written.
+            for (uint32_t w0 = 0; w0 < windows; w0 += 4) {
+                uint4 d[4];
+                uint32_t b[4], mi[4], ji[4], jl[4];
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const uint32_t win = w0 + k;
+                    const uint32_t src = win < 32u ? bits_lo : bits_hi;
+                    b[k] = win < windows ? __shfl_sync(0xffffffffu, src, win & 31u) : 0u;
+                    const uint32_t s = win * 32u + lane;
+                    const int j = owner_lane(gs.off, s);
+                    const uint32_t j_off = __shfl_sync(0xffffffffu, gs.off, j);
+                    const uint32_t j_first = __shfl_sync(0xffffffffu, gs.first, j);
+                    ji[k] = __shfl_sync(0xffffffffu, gs.inst, j);
+                    jl[k] = __shfl_sync(0xffffffffu, gs.lod, j);
+                    mi[k] = j_first + (s - j_off);
+                    if ((b[k] >> lane) & 1u) d[k] = __ldg(S.m_draw + mi[k]);
                 }
-                slot0 += __popc(b);
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    if ((b[k] >> lane) & 1u) {
+                        const uint32_t slot = slot0 + __popc(b[k] & ((1u << lane) - 1u));
+                        if (slot < cap) {
+                            uint32_t* out = reinterpret_cast<uint32_t*>(indirect + slot);
+                            out[0] = d[k].y;
+                            out[1] = 1u;
+                            out[2] = d[k].x;
+                            out[3] = d[k].z;
+                            out[4] = slot;
+                            reinterpret_cast<uint4*>(draws)[slot] = make_uint4(ji[k], mi[k], jl[k], 0u);
+                        }
+                    }
+                    slot0 += __popc(b[k]);
+                }
             }
         }
+    }
+}
+
+// Block 0 records the global timer after each phase (tracing; a few stores per launch).
+__device__ __forceinline__ void stamp(const BatchParams& P, int k) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        unsigned long long t;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+        P.phase_ns[k] = t;
     }
 }
 
@@ -480,8 +575,10 @@ __global__ void __launch_bounds__(kBatchThreads, 3) batch_kernel(BatchParams P) 
     extern __shared__ __align__(16) char sm[];
     uint32_t* s_tmp = reinterpret_cast<uint32_t*>(sm + kSmMisc);
 
+    stamp(P, 0);
     phase_setup(P);
     grid_sync(P);
+    stamp(P, 1);
 
     // Phase 1: Hi-Z tiles and object chunks share one work list.
     {
@@ -495,29 +592,84 @@ __global__ void __launch_bounds__(kBatchThreads, 3) batch_kernel(BatchParams P) 
             sv.pos_near = __ldcg(&cvp->pos_near);
             sv.focal = __ldcg(&cvp->focal);
             sv.thr = __ldcg(&cvp->lod_threshold_px);
-            sv.pad[0] = sv.pad[1] = 0u;
+            const QuotientBound qb = quotient_bound(sv.thr);
+            sv.thr_lo = qb.lo;
+            sv.thr_hi = qb.hi;
             s_sv[k] = sv;
+            reinterpret_cast<uint32_t*>(sm + kSmTileBegin)[k] = P.views[k].hiz.tile_begin;
+        }
+        // Hi-Z tiles (memory bound) and select units (arithmetic bound) alternate in
+        // one work queue, so that the CTAs sharing an SM overlap the two kinds of work
+        // and CTAs that draw cheap units draw more of them. Thread 0 claims the next
+        // unit while the block works on the current one.
+        const uint32_t vgroups = (P.view_count + kSelectViews - 1) / kSelectViews;
+        const uint32_t sel_units = P.object_chunks * vgroups;
+        const uint32_t pair = min(P.hiz_tiles, sel_units);
+        const uint32_t units = P.hiz_tiles + sel_units;
+        volatile uint32_t* s_unit = s_tmp + 8;
+        if (threadIdx.x == 0) {
+            *s_unit = atomicAdd(P.work, 1u);
+            s_tmp[0] = ~0u;  // no HizJob in shared memory yet
         }
         __syncthreads();
-        const uint32_t units = P.hiz_tiles + P.object_chunks;
-        for (uint32_t u = blockIdx.x; u < units; u += gridDim.x) {
-            if (u < P.hiz_tiles) phase_hiz_tile(P, u, sm);
-            else phase_select_chunk(P, u - P.hiz_tiles, sm);
+        unsigned long long t_hiz = 0, t_sel = 0, t0, t1;
+        for (;;) {
+            const uint32_t u = *s_unit;
+            if (u >= units) break;
+            uint32_t next = 0;
+            if (threadIdx.x == 0) next = atomicAdd(P.work, 1u);
+            bool is_hiz;
+            uint32_t k;
+            if (u < 2 * pair) {
+                is_hiz = (u & 1u) == 0u;
+                k = u >> 1;
+            } else {
+                is_hiz = P.hiz_tiles > sel_units;
+                k = u - pair;
+            }
+            asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+            if (is_hiz) {
+                phase_hiz_tile(P, k, sm);
+            } else {
+                const uint32_t chunk = k / vgroups, vg = k - chunk * vgroups;
+                phase_select_chunk(P, chunk, vg * kSelectViews, min(P.view_count, (vg + 1) * kSelectViews), sm);
+            }
+            asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t1));
+            (is_hiz ? t_hiz : t_sel) += t1 - t0;
+            __syncthreads();  // every thread has read *s_unit
+            if (threadIdx.x == 0) *s_unit = next;
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) {
+            atomicMax(P.phase_ns + 8, t_hiz);
+            atomicMax(P.phase_ns + 9, t_sel);
         }
     }
     grid_sync(P);
+    stamp(P, 2);
 
     grid_exclusive_scan(P, P.chunk_counts, P.chunk_offs, P.view_count * P.object_chunks, s_tmp);
+    stamp(P, 3);
     phase_expand(P, sm);
     grid_sync(P);
+    stamp(P, 4);
 
     const uint32_t total_spans = min(ld_cg(P.view_span_start + P.view_count), P.span_capacity);
     const uint32_t groups = total_spans >> 5;
     phase_test(P, groups, sm);
     grid_sync(P);
+    stamp(P, 5);
 
     grid_exclusive_scan(P, P.group_counts, P.group_offs, groups, s_tmp);
+    stamp(P, 6);
     phase_emit(P, groups);
+    // End of the launch: the latest block end (no barrier needed).
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long t;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+        atomicMax(P.phase_ns + 7, t);
+    }
 }
 
 }  // namespace

@@ -47,9 +47,9 @@ struct BatchParams {
     uint32_t view_count;
     uint32_t object_chunks;   // ceil(object_count / kBatchChunk)
     uint32_t hiz_tiles;       // Hi-Z tiles of all views
-    uint32_t* hiz_tickets;    // [view_count], zero before the launch
     uint32_t* barrier;        // [2] arrival count (zero before the launch), generation
     uint32_t* error;          // [1] kBatchErr* bits, zero before the launch
+    uint32_t* work;           // [1] phase-1 work queue head, zero before the launch
     uint32_t* chunk_counts;   // [view_count * object_chunks] active spans per (view, chunk)
     uint32_t* chunk_offs;     // [view_count * object_chunks + 1]
     uint32_t* seg_totals;     // [gridDim.x]
@@ -60,7 +60,12 @@ struct BatchParams {
     uint32_t* group_offs;     // [span_capacity / 32 + 1]
     uint32_t* group_bits;     // [span_capacity / 32 * kWindowsPerWarp] window ballots
     uint32_t* span_vis;       // [span_capacity * 2] per-span visibility words, or null
+    unsigned long long* phase_ns;  // [kBatchPhaseStamps] %globaltimer at launch and after each phase
 };
+
+// [0..7] phase boundaries, [8] / [9] largest per-CTA time spent on Hi-Z tiles /
+// object chunks in phase 1 (ns).
+constexpr uint32_t kBatchPhaseStamps = 10;
 
 // Dynamic shared memory of the persistent kernel (bytes).
 size_t batch_dynamic_smem();

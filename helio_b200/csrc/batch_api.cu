@@ -50,10 +50,16 @@ struct helio_batch {
     std::vector<size_t> out_offset;  // first draw of each view in out_indirect / out_draws
     bool prepared = false;
 
+    // Cleared region: counters (16 words per view) | barrier (2) | error (1) |
+    // work queue (1) | phase stamps (u64, 8-byte aligned).
     uint32_t* counters(uint32_t v) const { return clear.as<uint32_t>() + 16u * v; }
-    uint32_t* tickets() const { return clear.as<uint32_t>() + 16u * view_count; }
-    uint32_t* barrier() const { return tickets() + view_count; }
+    uint32_t* barrier() const { return clear.as<uint32_t>() + 16u * view_count; }
     uint32_t* error() const { return barrier() + 2; }
+    uint32_t* work() const { return barrier() + 3; }
+    size_t stamps_offset() const { return ((16u * view_count + 4u) * 4u + 7u) & ~(size_t)7u; }
+    unsigned long long* stamps() const {
+        return reinterpret_cast<unsigned long long*>(clear.as<char>() + stamps_offset());
+    }
 };
 
 namespace {
@@ -213,8 +219,8 @@ int32_t helio_batch_prepare(helio_batch* b, const helio_vg_scene* sc, uint32_t n
     }
     HELIO_CK(b->out_indirect.ensure(b->out_offset[n] * sizeof(HelioDrawIndexedIndirectArgs)));
     HELIO_CK(b->out_draws.ensure(b->out_offset[n] * sizeof(HelioGpuVgDraw)));
-    // Cleared region: counters (16 words per view) | Hi-Z tickets | barrier (2) | error (1).
-    b->clear_bytes = ((size_t)16 * n + n + 3) * sizeof(uint32_t);
+    b->view_count = n;
+    b->clear_bytes = b->stamps_offset() + helio::kBatchPhaseStamps * sizeof(unsigned long long);
     HELIO_CK(b->clear.ensure(b->clear_bytes));
     HELIO_CK(cudaMemsetAsync(b->clear.ptr, 0, b->clear_bytes, s));
     // Scratch.
@@ -288,9 +294,9 @@ int32_t helio_batch_execute(helio_batch* b, void* stream) {
     P.view_count = b->view_count;
     P.object_chunks = b->object_chunks;
     P.hiz_tiles = b->hiz_tiles;
-    P.hiz_tickets = b->tickets();
     P.barrier = b->barrier();
     P.error = b->error();
+    P.work = b->work();
     P.chunk_counts = b->chunk_counts.as<uint32_t>();
     P.chunk_offs = b->chunk_offs.as<uint32_t>();
     P.seg_totals = b->seg_totals.as<uint32_t>();
@@ -301,7 +307,23 @@ int32_t helio_batch_execute(helio_batch* b, void* stream) {
     P.group_offs = b->group_offs.as<uint32_t>();
     P.group_bits = b->group_bits.as<uint32_t>();
     P.span_vis = (b->cfg.flags & HELIO_BATCH_SPAN_VISIBILITY) ? b->span_vis.as<uint32_t>() : nullptr;
+    P.phase_ns = b->stamps();
     HELIO_CK(helio::launch_batch(P, b->grid, s));
+    return HELIO_OK;
+}
+
+int32_t helio_batch_get_phase_times(helio_batch* b, double* us_out, uint32_t capacity, uint32_t* count,
+                                    void* stream) {
+    HELIO_ARG(b && count && (capacity == 0 || us_out), "null pointer");
+    HELIO_ARG(b->prepared, "batch not prepared");
+    unsigned long long t[helio::kBatchPhaseStamps] = {0};
+    HELIO_CK(cudaMemcpyAsync(t, b->stamps(), sizeof(t), cudaMemcpyDeviceToHost, as_stream(stream)));
+    HELIO_CK(cudaStreamSynchronize(as_stream(stream)));
+    const uint32_t n = 9;
+    for (uint32_t k = 0; k < 7 && k < capacity; ++k)
+        us_out[k] = (t[k + 1] >= t[k] && t[k] != 0) ? (double)(t[k + 1] - t[k]) * 1e-3 : 0.0;
+    for (uint32_t k = 7; k < n && k < capacity; ++k) us_out[k] = (double)t[k + 1] * 1e-3;
+    *count = n;
     return HELIO_OK;
 }
 

@@ -39,6 +39,42 @@ __device__ __forceinline__ float dot3(F3 a, F3 b) {
 }
 __device__ __forceinline__ float clampf(float x, float lo, float hi) { return fminf(fmaxf(x, lo), hi); }
 
+// ── Exact `a / b <= thr` without the correctly rounded division in clear cases ──
+// r = rcp.approx.f32(b) has at most 1 ulp of error (PTX ISA), so q = RN(a * r)
+// lies within 2^-22 (relative) of a / b. With margins of |thr| * 2^-18 on either
+// side of thr, q below the lower margin proves RN(a / b) <= thr and q above the
+// upper margin proves RN(a / b) > thr; everything in between (and NaN) takes the
+// correctly rounded division. The margins are -inf / +inf (always exact) unless
+// 2^-60 <= |thr| <= 2^60, and r is NaN (always exact) unless 2^-64 <= b <= 2^64,
+// which keeps q clear of underflow relative to thr.
+struct QuotientBound {
+    float thr, lo, hi;
+};
+
+__device__ __forceinline__ QuotientBound quotient_bound(float thr) {
+    const float at = fabsf(thr);
+    if (at >= 0x1p-60f && at <= 0x1p60f) {
+        const float m = fmul(at, 0x1p-18f);
+        return QuotientBound{thr, fsub(thr, m), fadd(thr, m)};
+    }
+    return QuotientBound{thr, -__int_as_float(0x7f800000), __int_as_float(0x7f800000)};
+}
+
+__device__ __forceinline__ float quotient_rcp(float b) {
+    if (!(b >= 0x1p-64f && b <= 0x1p64f)) return __int_as_float(0x7fffffff);
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(b));
+    return r;
+}
+
+// RN(a / b) <= q.thr, bit-for-bit; r = quotient_rcp(b).
+__device__ __forceinline__ bool quotient_le(float a, float b, float r, const QuotientBound& q) {
+    const float approx = fmul(a, r);
+    if (approx < q.lo) return true;
+    if (approx > q.hi) return false;
+    return fdiv(a, b) <= q.thr;
+}
+
 // Column-major 4x4 matrix held as four columns.
 struct Mat4 {
     float4 c0, c1, c2, c3;

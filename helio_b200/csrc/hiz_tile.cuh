@@ -99,7 +99,8 @@ static __device__ __noinline__ void hiz_tail_warp(const HizJob& J) {
 // Tile `tile` (flat index within job J, whose ticket is tickets[job]) by all 256
 // threads of the CTA. s_m3 is an 8x9 shared scratch. Warps 1..7 return right
 // after the level-3 barrier; warp 0 finishes levels 4..6 and, if this CTA is the
-// last of the view, the tail.
+// last of the view, the tail. With tickets == nullptr the tile stops at level 6
+// and the caller builds the tail after a grid-wide barrier.
 __device__ __forceinline__ void hiz_tile(const HizJob& J, uint32_t job, uint32_t tile, uint32_t* tickets,
                                          float (*s_m3)[9]) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -227,7 +228,7 @@ __device__ __forceinline__ void hiz_tile(const HizJob& J, uint32_t job, uint32_t
             }
         }
     }
-    if (J.mip_count <= 7) return;
+    if (J.mip_count <= 7 || tickets == nullptr) return;
 
     // Tail: level 6 is written by warp 0 only, so warp 0 alone takes the ticket;
     // the warp of the last CTA of this job builds levels 7.. from level 6.

@@ -145,14 +145,15 @@ __global__ void __launch_bounds__(256) vg_select_kernel(VgSelectParams P) {
                     const float dist = fsqrt(dot3(d, d));
                     const float closest = fmaxf(fsub(dist, wr), fmaxf(pn.w, 1.0e-4f));
                     const float focal = s_view.focal;
-                    const float thr = s_view.lod_threshold_px;
+                    const QuotientBound qb = quotient_bound(s_view.lod_threshold_px);
+                    const float r = quotient_rcp(closest);
                     const float err[8] = {e0.x, e0.y, e0.z, e0.w, e1.x, e1.y, e1.z, e1.w};
                     uint32_t lod = 0;
 #pragma unroll
                     for (uint32_t level = 1; level < 8; ++level) {
                         if (level >= lod_count) break;
-                        const float px = fdiv(fmul(fmul(err[level], cd.max_scale), focal), closest);
-                        if (px <= thr) lod = level;
+                        // px = err * max_scale * focal / closest; px <= threshold keeps the level.
+                        if (quotient_le(fmul(fmul(err[level], cd.max_scale), focal), closest, r, qb)) lod = level;
                         else break;
                     }
                     selected = lod;

@@ -220,6 +220,7 @@ CULL_EXPORTS = {
     "helio_batch_get_view_outputs": (i32, [vp, u32, C.POINTER(BatchViewOutputs)]),
     "helio_batch_get_spans": (i32, [vp, C.POINTER(BatchSpanList)]),
     "helio_batch_status": (i32, [vp, vp]),
+    "helio_batch_get_phase_times": (i32, [vp, C.POINTER(C.c_double), u32, C.POINTER(u32), vp]),
     "helio_batch_destroy": (None, [vp]),
 }
 

@@ -282,6 +282,17 @@ class BatchedCull:
     def status(self, stream=None) -> None:
         N.check(self._lib.helio_batch_status(self._h, _stream_ptr(stream)))
 
+    PHASES = ("view_setup", "hiz_and_select", "span_count_scan", "span_expand", "meshlet_test",
+              "group_count_scan", "emit", "max_cta_hiz_busy", "max_cta_select_busy")
+
+    def phase_times(self, stream=None) -> dict:
+        """Device microseconds of each phase of the last execute, then the largest
+        per-CTA busy time on Hi-Z tiles and on object chunks within phase 1."""
+        arr = (C.c_double * 9)()
+        n = N.u32(0)
+        N.check(self._lib.helio_batch_get_phase_times(self._h, arr, 9, C.byref(n), _stream_ptr(stream)))
+        return {name: arr[i] for i, name in enumerate(self.PHASES[: n.value])}
+
     def view_outputs(self, v: int) -> dict:
         o = N.BatchViewOutputs()
         N.check(self._lib.helio_batch_get_view_outputs(self._h, v, C.byref(o)))

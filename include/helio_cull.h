@@ -499,6 +499,13 @@ int32_t helio_batch_set_cameras(helio_batch* batch, uint32_t view_count, const H
 int32_t helio_batch_execute(helio_batch* batch, void* stream);
 int32_t helio_batch_get_view_outputs(const helio_batch* batch, uint32_t view, helio_batch_view_outputs* out);
 int32_t helio_batch_get_spans(const helio_batch* batch, helio_batch_span_list* out);
+/* Tracing: device time (us) of the phases of the last execute, read from timer
+ * stamps the kernel takes at its grid barriers (synchronises `stream`). Order:
+ * view setup, Hi-Z + object select, span-count scan, span expansion, meshlet tests,
+ * group-count scan, emission; then the largest per-CTA busy time on Hi-Z tiles and
+ * on object chunks within the Hi-Z + select phase. */
+int32_t helio_batch_get_phase_times(helio_batch* batch, double* us_out, uint32_t capacity, uint32_t* count,
+                                    void* stream);
 /* Synchronises `stream`; HELIO_ERR_TIMEOUT if a bounded grid barrier gave up,
  * HELIO_ERR_CAPACITY if the active spans exceeded max_spans (outputs incomplete). */
 int32_t helio_batch_status(helio_batch* batch, void* stream);
