@@ -7,10 +7,15 @@
 // draws of each view compacted in the canonical (object, span, lane) order. The
 // work of all views is shared as follows (phases separated by grid barriers):
 //
-//   0  view constants (planes, camera fields, pyramid descriptor), one warp per view
+//   0  view constants (planes, camera fields, pyramid descriptor, reject box), one
+//      warp per view
 //   1  Hi-Z tiles of every view  +  object select: each object is loaded once and
-//      tested against every view; per (view, object) the selected LOD + 1 is stored
-//      and per (view, 256-object chunk) the number of active 64-meshlet spans
+//      tested against a group of views; per (view, object) the selected LOD + 1 is
+//      stored and per (view, 256-object chunk) the number of active 64-meshlet spans
+//      and of visible objects. An object whose world centre lies outside a view's
+//      reject box fails that view's sphere test for certain (see reject_box_warp)
+//      and skips it; the remaining (object, view) pairs are compacted per warp into
+//      full 32-lane batches for the exact test and the LOD choice
 //   2  exclusive scan of the (view, chunk) span counts
 //   3  expansion into one list of active spans, view-major, each view padded to a
 //      multiple of 32 spans so every group of 32 spans belongs to one view
@@ -31,19 +36,31 @@ namespace helio {
 
 namespace {
 
+// Select constants of a view in shared memory. 144 bytes (36 words): the 128-bit
+// plane loads of 8 lanes that read 8 consecutive views hit 8 different bank groups.
 struct SelView {
     Planes planes;
     float4 pos_near;
     float focal, thr, thr_lo, thr_hi;  // thr_lo / thr_hi: QuotientBound margins of thr
+    float4 pad;
 };
-static_assert(sizeof(SelView) == 128, "SelView layout");
+static_assert(sizeof(SelView) == 144, "SelView layout");
+
+struct SelBox {
+    float lo[3], hi[3];
+    uint32_t pad[2];
+};
 
 // Dynamic shared memory layout (bytes).
-constexpr size_t kSmSelViews = 0;                                            // SelView[kBatchMaxViews]
-constexpr size_t kSmSelCnt = kSmSelViews + sizeof(SelView) * kBatchMaxViews;  // u32[kBatchMaxViews]
-constexpr size_t kSmSelHist = kSmSelCnt + 4 * kBatchMaxViews;                 // u32[kBatchMaxViews][8]
-constexpr size_t kSmSelMax = kSmSelHist + 32 * kBatchMaxViews;                // u32[kBatchMaxViews]
-constexpr size_t kSmHizJob = kSmSelMax + 4 * kBatchMaxViews;                  // HizJob
+constexpr uint32_t kSelectMaxViews = 32;  // views per select unit, at most
+constexpr uint32_t kSelQueue = 64;        // candidate (view, lane) slots per warp
+constexpr size_t kSmSelViews = 0;                                               // SelView[kBatchMaxViews]
+constexpr size_t kSmSelBox = kSmSelViews + sizeof(SelView) * kBatchMaxViews;    // SelBox[kBatchMaxViews]
+constexpr size_t kSmSelLod = kSmSelBox + sizeof(SelBox) * kBatchMaxViews;       // u8[kSelectMaxViews][256]
+constexpr size_t kSmSelQueue = kSmSelLod + kSelectMaxViews * kBatchChunk;       // u16[8][kSelQueue]
+constexpr size_t kSmSelSpans = kSmSelQueue + 2 * 8 * kSelQueue;                 // u32[kSelectMaxViews]
+constexpr size_t kSmSelVis = kSmSelSpans + 4 * kSelectMaxViews;                 // u32[kSelectMaxViews]
+constexpr size_t kSmHizJob = kSmSelVis + 4 * kSelectMaxViews;                   // HizJob
 constexpr size_t kSmHizM3 = kSmHizJob + ((sizeof(HizJob) + 15) / 16) * 16;    // float[8][9]
 constexpr size_t kSmMisc = kSmHizM3 + 8 * 9 * 4;                              // u32[64]
 constexpr size_t kSmTileBegin = kSmMisc + 64 * 4;                             // u32[kBatchMaxViews]
@@ -151,6 +168,126 @@ __device__ void grid_exclusive_scan(const BatchParams& P, const uint32_t* in, ui
     grid_sync(P);
 }
 
+// ── Reject box of a view ──────────────────────────────────────────────────────
+// sphere_visible_vg rejects (c, r) when some plane gives fl(d_i) < -r, where d_i =
+// dot(n_i, c) + w_i is evaluated with 4 roundings, so |fl(d_i) - d_i| <= 5u S_i
+// (u = 2^-24, S_i = |n_i.x c.x| + |n_i.y c.y| + |n_i.z c.z| + |w_i|). For every
+// valid object of the scene r <= rmax and |c|_1 <= cl1, and the normalised plane
+// components are at most 1 + 2^-23 in magnitude, so with
+//     s_i = rmax + 2^-20 (cl1 + |w_i| + rmax)
+// a centre outside Q = { p : n_i . p + w_i + s_i >= 0 for all i } (exact
+// arithmetic on the float planes) has some d_i < -s_i, hence fl(d_i) < -rmax <= -r:
+// the sphere test fails for certain. The box is the axis-aligned bound of Q,
+// widened and rounded outward to float; a centre outside it is outside Q.
+//
+// Q is bounded and its vertices are intersections of three planes. Lane t < 20
+// solves triple t in double (Cramer's rule) and keeps the point if it satisfies
+// every constraint within a relative 1e-7. The box is disabled (infinite, so
+// nothing is rejected) when an input is not finite, when one of the eight corner
+// triples (one plane of each pair x, y, z) is ill-conditioned (relative
+// determinant below 1e-4) or infeasible, when an ill-conditioned triple (relative
+// determinant in (1e-12, 1e-4]) lands within a loose 1e-3 of Q (a vertex that
+// double precision may have misplaced), or when Q is unbounded: a recession
+// direction of Q is a cross product of two normals (lanes 0..14, both signs) that
+// no plane rejects.
+__device__ void reject_box_warp(const Planes& pl, float rmax_f, float cl1_f, float box[6]) {
+    const int lane = threadIdx.x & 31;
+    double n[6][3], w[6];
+    bool finite = isfinite(rmax_f) && isfinite(cl1_f);
+    const double rmax = rmax_f, cl1 = cl1_f;
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+        const float4 p = pl.p[i];
+        finite = finite && isfinite(p.x) && isfinite(p.y) && isfinite(p.z) && isfinite(p.w);
+        n[i][0] = p.x;
+        n[i][1] = p.y;
+        n[i][2] = p.z;
+        w[i] = (double)p.w + rmax + 0x1p-20 * (cl1 + fabs((double)p.w) + rmax);
+    }
+    auto nrm = [&](int i) { return sqrt(n[i][0] * n[i][0] + n[i][1] * n[i][1] + n[i][2] * n[i][2]); };
+    auto slack = [&](int j, double x, double y, double z) { return n[j][0] * x + n[j][1] * y + n[j][2] * z + w[j]; };
+    auto scale = [&](int j, double x, double y, double z) {
+        return (fabs(x) + fabs(y) + fabs(z)) * nrm(j) + fabs(w[j]) + 1e-30;
+    };
+    bool bad = !finite;
+    double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    if (finite && lane < 20) {
+        // lane -> (a < b < c)
+        int a = 0, b = 1, c = 2;
+        for (int k = 0; k < lane; ++k) {
+            if (++c == 6) {
+                if (++b == 5) {
+                    ++a;
+                    b = a + 1;
+                }
+                c = b + 1;
+            }
+        }
+        const double bc[3] = {n[b][1] * n[c][2] - n[b][2] * n[c][1], n[b][2] * n[c][0] - n[b][0] * n[c][2],
+                              n[b][0] * n[c][1] - n[b][1] * n[c][0]};
+        const double ca[3] = {n[c][1] * n[a][2] - n[c][2] * n[a][1], n[c][2] * n[a][0] - n[c][0] * n[a][2],
+                              n[c][0] * n[a][1] - n[c][1] * n[a][0]};
+        const double ab[3] = {n[a][1] * n[b][2] - n[a][2] * n[b][1], n[a][2] * n[b][0] - n[a][0] * n[b][2],
+                              n[a][0] * n[b][1] - n[a][1] * n[b][0]};
+        const double det = n[a][0] * bc[0] + n[a][1] * bc[1] + n[a][2] * bc[2];
+        const double rel = fabs(det) / (nrm(a) * nrm(b) * nrm(c) + 1e-300);
+        const bool corner = a < 2 && b >= 2 && b < 4 && c >= 4;
+        double p[3] = {0.0, 0.0, 0.0};
+        bool feasible = false, loose = false;
+        if (rel > 1e-12) {
+#pragma unroll
+            for (int k = 0; k < 3; ++k) p[k] = -(w[a] * bc[k] + w[b] * ca[k] + w[c] * ab[k]) / det;
+            feasible = isfinite(p[0]) && isfinite(p[1]) && isfinite(p[2]);
+            loose = feasible;
+            for (int j = 0; j < 6; ++j) {
+                const double s = slack(j, p[0], p[1], p[2]), sc = scale(j, p[0], p[1], p[2]);
+                feasible = feasible && s >= -1e-7 * sc;
+                loose = loose && s >= -1e-3 * sc;
+            }
+        }
+        if (corner && !(rel > 1e-4 && feasible)) bad = true;
+        if (!corner && rel > 1e-12 && rel <= 1e-4 && loose) bad = true;
+        if (rel > 1e-4 && feasible)
+            for (int k = 0; k < 3; ++k) lo[k] = hi[k] = p[k];
+    }
+    if (finite && lane < 15) {
+        int a = 0, b = 1;
+        for (int k = 0; k < lane; ++k)
+            if (++b == 6) {
+                ++a;
+                b = a + 1;
+            }
+        const double d[3] = {n[a][1] * n[b][2] - n[a][2] * n[b][1], n[a][2] * n[b][0] - n[a][0] * n[b][2],
+                             n[a][0] * n[b][1] - n[a][1] * n[b][0]};
+        const double len = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+        if (len > 1e-12 * nrm(a) * nrm(b)) {
+            for (int sgn = -1; sgn <= 1; sgn += 2) {
+                bool ray = true;
+                for (int j = 0; j < 6; ++j)
+                    ray = ray && sgn * (n[j][0] * d[0] + n[j][1] * d[1] + n[j][2] * d[2]) >= -1e-9 * nrm(j) * len;
+                if (ray) bad = true;
+            }
+        }
+    }
+    bad = __any_sync(0xffffffffu, bad);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            lo[k] = fmin(lo[k], __shfl_xor_sync(0xffffffffu, lo[k], o));
+            hi[k] = fmax(hi[k], __shfl_xor_sync(0xffffffffu, hi[k], o));
+        }
+        if (bad || !(lo[k] <= hi[k])) {
+            box[k] = -INFINITY;
+            box[3 + k] = INFINITY;
+        } else {
+            const double pad = 1e-6 * (fabs(lo[k]) + fabs(hi[k]) + rmax + 1.0);
+            box[k] = __double2float_rd(lo[k] - pad);
+            box[3 + k] = __double2float_ru(hi[k] + pad);
+        }
+    }
+}
+
 // ── Phase 0: view constants ──────────────────────────────────────────────────
 __device__ void phase_setup(const BatchParams& P) {
     for (uint32_t v = blockIdx.x; v < P.view_count; v += gridDim.x) {
@@ -158,7 +295,11 @@ __device__ void phase_setup(const BatchParams& P) {
         const BatchViewDev& V = P.views[v];
         __shared__ Planes s_pl;
         publish_planes_warp(V.camera.view_proj, s_pl);
+        float box[6];
+        reject_box_warp(s_pl, __uint_as_float(__ldg(P.scene_bounds)), __uint_as_float(__ldg(P.scene_bounds + 1)),
+                        box);
         if (threadIdx.x == 0) {
+            for (int k = 0; k < 6; ++k) P.views[v].reject_box[k] = box[k];
             CullView c;
             c.planes = s_pl;
             c.vp = ldg_mat4(V.camera.view_proj);
@@ -216,96 +357,128 @@ __device__ void phase_hiz_tile(const BatchParams& P, uint32_t tile, char* sm) {
 }
 
 // ── Phase 1b: object select against a group of views (vg_cull.wgsl:282-352) ──
-// Unit = (256-object chunk, group of kSelectViews views): the object is loaded once
-// per unit and tested against each view of the group.
-constexpr uint32_t kSelectViews = 16;
+// Unit = (256-object chunk, group of at most kSelectMaxViews views); lane j of warp
+// w holds object chunk * 256 + 32 w + j. For each view of the group the warp tests
+// the world centres against the view's reject box (broadcast from shared memory)
+// and queues the (view, lane) pairs the box does not reject; every 32 queued pairs
+// are tested exactly, one pair per lane (select_batch). The selected LOD + 1 of the
+// unit's pairs collects in a shared tile (zero = culled) that is written out row by
+// row; spans and visible objects per view are counted with shared atomics.
 
-__device__ void phase_select_chunk(const BatchParams& P, uint32_t chunk, uint32_t v_begin, uint32_t v_end, char* sm) {
+// Exact sphere test and LOD walk of n <= 32 queued pairs (vg_cull.wgsl:315-336).
+__device__ void select_batch(const BatchParams& P, uint32_t chunk, uint32_t v_begin, const uint16_t* queue,
+                             uint32_t n, F3 c, float wr, float max_scale, char* sm) {
     const SelView* s_sv = reinterpret_cast<const SelView*>(sm + kSmSelViews);
-    uint32_t* s_cnt = reinterpret_cast<uint32_t*>(sm + kSmSelCnt);
-    uint32_t* s_hist = reinterpret_cast<uint32_t*>(sm + kSmSelHist);
-    uint32_t* s_max = reinterpret_cast<uint32_t*>(sm + kSmSelMax);
-    const uint32_t tid = threadIdx.x, nv = v_end - v_begin;
-    __syncthreads();
-    for (uint32_t k = tid; k < nv * 10u; k += kBatchThreads) {
-        const uint32_t v = v_begin + k % nv, f = k / nv;  // f: 0 count, 1..8 histogram, 9 max
-        if (f == 0) s_cnt[v] = 0u;
-        else if (f <= 8) s_hist[v * 8u + (f - 1u)] = 0u;
-        else s_max[v] = 0u;
-    }
-    __syncthreads();
-    const VgSceneDev& S = P.scene;
-    const uint32_t o = chunk * kBatchChunk + tid, lane = tid & 31u;
-    // Lanes past the last object take part in the warp reductions as invisible.
-    const bool in_range = o < S.object_count;
-    const HelioGpuVgObject* obj = S.objects + (in_range ? o : 0u);
-    const uint4 head = __ldg(reinterpret_cast<const uint4*>(obj));
-    const float4 lb = __ldg(reinterpret_cast<const float4*>(obj->local_bounds));
+    uint8_t* s_lod = reinterpret_cast<uint8_t*>(sm + kSmSelLod);
+    uint32_t* s_spans = reinterpret_cast<uint32_t*>(sm + kSmSelSpans);
+    uint32_t* s_vis = reinterpret_cast<uint32_t*>(sm + kSmSelVis);
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const uint32_t e = lane < n ? (uint32_t)queue[lane] : lane;
+    const uint32_t j = e & 31u, k = e >> 5;
+    const F3 cj = f3(__shfl_sync(0xffffffffu, c.x, j), __shfl_sync(0xffffffffu, c.y, j),
+                     __shfl_sync(0xffffffffu, c.z, j));
+    const float wrj = __shfl_sync(0xffffffffu, wr, j), msj = __shfl_sync(0xffffffffu, max_scale, j);
+    if (lane >= n) return;
+    const SelView& sv = s_sv[v_begin + k];
+    if (!sphere_visible_vg(sv.planes, cj, wrj)) return;
+    const uint32_t slot = warp * 32u + j;
+    const HelioGpuVgObject* obj = P.scene.objects + (chunk * kBatchChunk + slot);
+    const uint32_t lod_count = min(__ldg(&obj->lod_count), 8u);
     const float4 e0 = __ldg(reinterpret_cast<const float4*>(obj->lod_errors));
     const float4 e1 = __ldg(reinterpret_cast<const float4*>(obj->lod_errors + 4));
-    const uint4 c0 = __ldg(reinterpret_cast<const uint4*>(obj->lod_meshlet_counts));
-    const uint4 c1 = __ldg(reinterpret_cast<const uint4*>(obj->lod_meshlet_counts + 4));
-    const uint32_t lod_count = min(head.y, 8u), ii = head.x;
+    const float err[8] = {e0.x, e0.y, e0.z, e0.w, e1.x, e1.y, e1.z, e1.w};
+    const F3 d = sub3(cj, f3(sv.pos_near.x, sv.pos_near.y, sv.pos_near.z));
+    const float dist = fsqrt(dot3(d, d));
+    const float closest = fmaxf(fsub(dist, wrj), fmaxf(sv.pos_near.w, 1.0e-4f));
+    const QuotientBound qb{sv.thr, sv.thr_lo, sv.thr_hi};
+    const float r = quotient_rcp(closest);
+    uint32_t lod = 0;
+#pragma unroll
+    for (uint32_t level = 1; level < 8; ++level) {
+        if (level >= lod_count) break;
+        // px = err * max_scale * focal / closest; px <= threshold keeps the level.
+        if (quotient_le(fmul(fmul(err[level], msj), sv.focal), closest, r, qb)) lod = level;
+        else break;
+    }
+    const uint32_t cnt = __ldg(&obj->lod_meshlet_counts[lod]);
+    s_lod[k * kBatchChunk + slot] = (uint8_t)(lod + 1u);
+    if (cnt) atomicAdd(s_spans + k, (cnt + 63u) >> 6);
+    atomicAdd(s_vis + k, 1u);
+}
+
+__device__ void phase_select_chunk(const BatchParams& P, uint32_t chunk, uint32_t v_begin, uint32_t v_end, char* sm) {
+    const SelBox* s_box = reinterpret_cast<const SelBox*>(sm + kSmSelBox);
+    uint4* s_lod4 = reinterpret_cast<uint4*>(sm + kSmSelLod);
+    uint32_t* s_spans = reinterpret_cast<uint32_t*>(sm + kSmSelSpans);
+    uint32_t* s_vis = reinterpret_cast<uint32_t*>(sm + kSmSelVis);
+    const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5, nv = v_end - v_begin;
+    const VgSceneDev& S = P.scene;
+    const uint32_t o = chunk * kBatchChunk + tid;
     bool valid = false;
     F3 c = f3(0.f, 0.f, 0.f);
     float wr = 0.0f, max_scale = 0.0f;
-    if (in_range && lod_count > 0u && ii < S.instance_count) {
-        const HelioInstanceCullData cd = load_cull(S.cull + ii);
-        const Mat4 model = ldg_mat4(S.instances[ii].model);
-        if (cd.valid_transform != 0u) {
-            valid = true;
-            max_scale = cd.max_scale;
-            c = mat4_point3(model, f3(lb.x, lb.y, lb.z));
-            wr = fmaxf(fmul(lb.w, cd.max_scale), 0.0f);
+    if (o < S.object_count) {
+        const HelioGpuVgObject* obj = S.objects + o;
+        const uint4 head = __ldg(reinterpret_cast<const uint4*>(obj));
+        const float4 lb = __ldg(reinterpret_cast<const float4*>(obj->local_bounds));
+        const uint32_t lod_count = min(head.y, 8u), ii = head.x;
+        if (lod_count > 0u && ii < S.instance_count) {
+            const HelioInstanceCullData cd = load_cull(S.cull + ii);
+            const Mat4 model = ldg_mat4(S.instances[ii].model);
+            if (cd.valid_transform != 0u) {
+                valid = true;
+                max_scale = cd.max_scale;
+                c = mat4_point3(model, f3(lb.x, lb.y, lb.z));
+                wr = fmaxf(fmul(lb.w, cd.max_scale), 0.0f);
+            }
         }
     }
-    const float err[8] = {e0.x, e0.y, e0.z, e0.w, e1.x, e1.y, e1.z, e1.w};
-    const uint32_t cnts[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
-    uint8_t* lod_col = P.lod + o;
-    for (uint32_t v = v_begin; v < v_end; ++v) {
-        const bool vis = valid && sphere_visible_vg(s_sv[v].planes, c, wr);
-        uint32_t lod = 0, cnt = c0.x;
-        if (vis) {
-            const float4 pn = s_sv[v].pos_near;
-            const F3 d = sub3(c, f3(pn.x, pn.y, pn.z));
-            const float dist = fsqrt(dot3(d, d));
-            const float closest = fmaxf(fsub(dist, wr), fmaxf(pn.w, 1.0e-4f));
-            const float focal = s_sv[v].focal;
-            const QuotientBound qb{s_sv[v].thr, s_sv[v].thr_lo, s_sv[v].thr_hi};
-            const float r = quotient_rcp(closest);
-#pragma unroll
-            for (uint32_t level = 1; level < 8; ++level) {
-                if (level >= lod_count) break;
-                // px = err * max_scale * focal / closest; px <= threshold keeps the level.
-                if (quotient_le(fmul(fmul(err[level], max_scale), focal), closest, r, qb)) {
-                    lod = level;
-                    cnt = cnts[level];
-                } else {
-                    break;
-                }
-            }
-        }
-        if (in_range) lod_col[(size_t)v * S.object_count] = (uint8_t)(vis ? lod + 1u : 0u);
-        if (__any_sync(0xffffffffu, vis)) {
-            const uint32_t spans = __reduce_add_sync(0xffffffffu, vis ? (cnt + 63u) >> 6 : 0u);
-            // lod_count - 1 + 1: 0 means no visible object
-            const uint32_t top = __reduce_max_sync(0xffffffffu, vis ? lod_count : 0u);
-            const uint32_t key = vis ? lod : 8u;
-            const uint32_t peers = __match_any_sync(0xffffffffu, key);
-            if (key < 8u && lane == (uint32_t)(__ffs(peers) - 1)) atomicAdd(s_hist + v * 8u + key, __popc(peers));
-            if (lane == 0) {
-                if (spans) atomicAdd(s_cnt + v, spans);
-                atomicMax(s_max + v, top);
-            }
-        }
+    __syncthreads();  // the previous unit is done with the tile and the counters
+    constexpr uint32_t kRow4 = kBatchChunk / 16;  // 16-byte words per tile row
+    for (uint32_t i = tid; i < nv * kRow4; i += kBatchThreads) s_lod4[i] = make_uint4(0u, 0u, 0u, 0u);
+    if (tid < nv) {
+        s_spans[tid] = 0u;
+        s_vis[tid] = 0u;
     }
     __syncthreads();
-    for (uint32_t v = v_begin + tid; v < v_end; v += kBatchThreads) {
-        P.chunk_counts[(size_t)v * P.object_chunks + chunk] = s_cnt[v];
-        uint32_t* counters = P.views[v].counters;
-        for (uint32_t l = 0; l < 8u; ++l)
-            if (s_hist[v * 8u + l]) atomicAdd(counters + 2 + l, s_hist[v * 8u + l]);
-        if (s_max[v]) atomicMax(counters + 10, s_max[v] - 1u);
+    uint16_t* q = reinterpret_cast<uint16_t*>(sm + kSmSelQueue) + warp * kSelQueue;
+    const uint32_t lt = (1u << lane) - 1u;
+    uint32_t qn = 0;  // warp-uniform
+    for (uint32_t k = 0; k < nv; ++k) {
+        const SelBox& b = s_box[v_begin + k];
+        // NaN centres are never rejected here; the exact test decides them.
+        const bool out = c.x < b.lo[0] || c.x > b.hi[0] || c.y < b.lo[1] || c.y > b.hi[1] || c.z < b.lo[2] ||
+                         c.z > b.hi[2];
+        const bool pass = valid && !out;
+        const uint32_t bal = __ballot_sync(0xffffffffu, pass);
+        if (pass) q[qn + __popc(bal & lt)] = (uint16_t)((k << 5) | lane);
+        qn += __popc(bal);
+        if (qn >= 32u) {
+            __syncwarp();
+            select_batch(P, chunk, v_begin, q, 32u, c, wr, max_scale, sm);
+            __syncwarp();
+            const uint32_t rest = qn - 32u;
+            const uint16_t x = lane < rest ? q[32u + lane] : (uint16_t)0;
+            __syncwarp();
+            if (lane < rest) q[lane] = x;
+            __syncwarp();
+            qn = rest;
+        }
+    }
+    if (qn) {
+        __syncwarp();
+        select_batch(P, chunk, v_begin, q, qn, c, wr, max_scale, sm);
+    }
+    __syncthreads();
+    for (uint32_t i = tid; i < nv * kRow4; i += kBatchThreads) {
+        const uint32_t k = i / kRow4, w4 = i - k * kRow4;
+        *reinterpret_cast<uint4*>(P.lod + (size_t)(v_begin + k) * P.lod_pitch + chunk * kBatchChunk + w4 * 16u) =
+            s_lod4[i];
+    }
+    if (tid < nv) {
+        const size_t u = (size_t)(v_begin + tid) * P.object_chunks + chunk;
+        P.chunk_counts[u] = s_spans[tid];
+        P.chunk_vis[u] = s_vis[tid];
     }
 }
 
@@ -350,8 +523,9 @@ __device__ void phase_expand(const BatchParams& P, char* sm) {
     // heavy consecutive chunks of a large view spread over many warps.
     for (uint32_t k0 = 0; gw + (size_t)k0 * GW < n_units; k0 += 32u) {
         const size_t u = gw + (size_t)(k0 + lane) * GW;
-        const uint32_t cnt = u < n_units ? ld_cg(P.chunk_counts + u) : 0u;
-        uint32_t mask = __ballot_sync(0xffffffffu, cnt != 0u);
+        // A unit with a visible object has spans to write or LOD statistics to count.
+        const uint32_t busy = u < n_units ? ld_cg(P.chunk_vis + u) : 0u;
+        uint32_t mask = __ballot_sync(0xffffffffu, busy != 0u);
         while (mask) {
             const uint32_t uu = gw + (k0 + (__ffs(mask) - 1)) * GW;
             mask &= mask - 1u;
@@ -360,22 +534,38 @@ __device__ void phase_expand(const BatchParams& P, char* sm) {
             // All loads of the chunk's 256 objects are issued before any is used: one
             // round trip for the LOD bytes, one for the objects' selected ranges.
             constexpr int R = kBatchChunk / 32;
-            const uint8_t* lrow = P.lod + (size_t)v * S.object_count;
+            const uint8_t* lrow = P.lod + (size_t)v * P.lod_pitch;
             uint32_t sel[R], count[R], first[R], inst[R];
 #pragma unroll
             for (int r = 0; r < R; ++r) {
                 const uint32_t o = ch * kBatchChunk + r * 32u + lane;
                 sel[r] = o < S.object_count ? (uint32_t)__ldcg(lrow + o) : 0u;
             }
+            // LOD histogram (4-bit lanes: at most R objects per lane) and the largest
+            // lod_count - 1 of the visible objects: counters 2..9 and 10 of the view.
+            uint32_t hist = 0u, top = 0u;
 #pragma unroll
             for (int r = 0; r < R; ++r) {
                 count[r] = first[r] = inst[r] = 0u;
                 if (sel[r]) {
                     const HelioGpuVgObject* obj = S.objects + (ch * kBatchChunk + r * 32u + lane);
+                    const uint2 h = __ldg(reinterpret_cast<const uint2*>(obj));  // instance_index, lod_count
                     count[r] = __ldg(&obj->lod_meshlet_counts[sel[r] - 1u]);
                     first[r] = __ldg(&obj->lod_first_meshlets[sel[r] - 1u]);
-                    inst[r] = __ldg(&obj->instance_index);
+                    inst[r] = h.x;
+                    hist += 1u << (4u * (sel[r] - 1u));
+                    top = max(top, min(h.y, 8u));  // lod_count - 1 + 1
                 }
+            }
+            {
+                uint32_t* counters = P.views[v].counters;
+#pragma unroll
+                for (uint32_t l = 0; l < 8u; ++l) {
+                    const uint32_t n = __reduce_add_sync(0xffffffffu, (hist >> (4u * l)) & 15u);
+                    if (lane == 0 && n) atomicAdd(counters + 2 + l, n);
+                }
+                top = __reduce_max_sync(0xffffffffu, top);
+                if (lane == 0 && top) atomicMax(counters + 10, top - 1u);
             }
 #pragma unroll
             for (int r = 0; r < R; ++r) {
@@ -595,16 +785,25 @@ __global__ void __launch_bounds__(kBatchThreads, 3) batch_kernel(BatchParams P) 
             const QuotientBound qb = quotient_bound(sv.thr);
             sv.thr_lo = qb.lo;
             sv.thr_hi = qb.hi;
+            sv.pad = make_float4(0.f, 0.f, 0.f, 0.f);
             s_sv[k] = sv;
+            SelBox bx;
+            for (int i = 0; i < 3; ++i) {
+                bx.lo[i] = __ldcg(&P.views[k].reject_box[i]);
+                bx.hi[i] = __ldcg(&P.views[k].reject_box[3 + i]);
+            }
+            bx.pad[0] = bx.pad[1] = 0u;
+            reinterpret_cast<SelBox*>(sm + kSmSelBox)[k] = bx;
             reinterpret_cast<uint32_t*>(sm + kSmTileBegin)[k] = P.views[k].hiz.tile_begin;
         }
-        // Hi-Z tiles (memory bound) and select units (arithmetic bound) alternate in
-        // one work queue, so that the CTAs sharing an SM overlap the two kinds of work
-        // and CTAs that draw cheap units draw more of them. Thread 0 claims the next
-        // unit while the block works on the current one.
-        const uint32_t vgroups = (P.view_count + kSelectViews - 1) / kSelectViews;
+        // Hi-Z tiles (memory bound) and select units (arithmetic bound) are spread
+        // evenly through one work queue, so that the CTAs sharing an SM overlap the two
+        // kinds of work and CTAs that draw cheap units draw more of them. Thread 0
+        // claims the next unit while the block works on the current one. Unit u is a
+        // select unit iff floor((u + 1) S / U) > floor(u S / U).
+        const uint32_t vgroups = (P.view_count + kSelectMaxViews - 1) / kSelectMaxViews;
+        const uint32_t gsize = (P.view_count + vgroups - 1) / vgroups;  // balanced view groups
         const uint32_t sel_units = P.object_chunks * vgroups;
-        const uint32_t pair = min(P.hiz_tiles, sel_units);
         const uint32_t units = P.hiz_tiles + sel_units;
         volatile uint32_t* s_unit = s_tmp + 8;
         if (threadIdx.x == 0) {
@@ -618,21 +817,14 @@ __global__ void __launch_bounds__(kBatchThreads, 3) batch_kernel(BatchParams P) 
             if (u >= units) break;
             uint32_t next = 0;
             if (threadIdx.x == 0) next = atomicAdd(P.work, 1u);
-            bool is_hiz;
-            uint32_t k;
-            if (u < 2 * pair) {
-                is_hiz = (u & 1u) == 0u;
-                k = u >> 1;
-            } else {
-                is_hiz = P.hiz_tiles > sel_units;
-                k = u - pair;
-            }
+            const uint32_t sel_before = (uint32_t)((uint64_t)u * sel_units / units);
+            const bool is_hiz = (uint32_t)((uint64_t)(u + 1) * sel_units / units) == sel_before;
             asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
             if (is_hiz) {
-                phase_hiz_tile(P, k, sm);
+                phase_hiz_tile(P, u - sel_before, sm);
             } else {
-                const uint32_t chunk = k / vgroups, vg = k - chunk * vgroups;
-                phase_select_chunk(P, chunk, vg * kSelectViews, min(P.view_count, (vg + 1) * kSelectViews), sm);
+                const uint32_t chunk = sel_before / vgroups, vg = sel_before - chunk * vgroups;
+                phase_select_chunk(P, chunk, vg * gsize, min(P.view_count, (vg + 1) * gsize), sm);
             }
             asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t1));
             (is_hiz ? t_hiz : t_sel) += t1 - t0;
@@ -672,7 +864,43 @@ __global__ void __launch_bounds__(kBatchThreads, 3) batch_kernel(BatchParams P) 
     }
 }
 
+__global__ void scene_bounds_kernel(VgSceneDev S, uint32_t* bounds) {
+    const uint32_t o = blockIdx.x * blockDim.x + threadIdx.x;
+    float wr = 0.0f, cl1 = 0.0f;
+    if (o < S.object_count) {
+        const HelioGpuVgObject* obj = S.objects + o;
+        const uint4 head = __ldg(reinterpret_cast<const uint4*>(obj));
+        const uint32_t lod_count = min(head.y, 8u), ii = head.x;
+        if (lod_count > 0u && ii < S.instance_count) {
+            const HelioInstanceCullData cd = load_cull(S.cull + ii);
+            if (cd.valid_transform != 0u) {
+                const float4 lb = __ldg(reinterpret_cast<const float4*>(obj->local_bounds));
+                const F3 c = mat4_point3(ldg_mat4(S.instances[ii].model), f3(lb.x, lb.y, lb.z));
+                wr = fmaxf(fmul(lb.w, cd.max_scale), 0.0f);
+                cl1 = fabsf(c.x) + fabsf(c.y) + fabsf(c.z);  // rounding up is not needed: 2^-20 slack
+            }
+        }
+    }
+    // Non-negative floats (and NaN above +inf) order like their bit patterns.
+    uint32_t a = __float_as_uint(wr), b = __float_as_uint(cl1);
+#pragma unroll
+    for (int k = 16; k > 0; k >>= 1) {
+        a = max(a, __shfl_xor_sync(0xffffffffu, a, k));
+        b = max(b, __shfl_xor_sync(0xffffffffu, b, k));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (a) atomicMax(bounds, a);
+        if (b) atomicMax(bounds + 1, b);
+    }
+}
+
 }  // namespace
+
+cudaError_t launch_scene_bounds(const VgSceneDev& scene, uint32_t* bounds, cudaStream_t stream) {
+    const uint32_t n = scene.object_count;
+    if (n) scene_bounds_kernel<<<(n + 255) / 256, 256, 0, stream>>>(scene, bounds);
+    return cudaGetLastError();
+}
 
 size_t batch_dynamic_smem() { return kSmTotal; }
 

@@ -25,6 +25,8 @@ struct alignas(16) BatchViewDev {
     HelioDrawIndexedIndirectArgs* indirect;  // [capacity]
     HelioGpuVgDraw* draws;                   // [capacity]
     uint32_t* counters;                      // [16]; layout of the VG counters
+    float reject_box[6];  // written by phase 0: x/y/z lower bounds, then upper bounds
+    uint32_t pad2[2];
 };
 
 static_assert(sizeof(BatchViewDev) % 16 == 0, "view table entries stay 16-byte aligned");
@@ -41,9 +43,11 @@ enum : uint32_t { kBatchErrTimeout = 1u, kBatchErrSpanCapacity = 2u };
 
 struct BatchParams {
     VgSceneDev scene;
+    const uint32_t* scene_bounds;  // [2] launch_scene_bounds output
     BatchViewDev* views;      // [view_count]
     CullView* cviews;         // [view_count], written by phase 0
-    uint8_t* lod;             // [view_count * object_count]: LOD + 1 per (view, object), 0 = culled
+    uint8_t* lod;             // [view_count * lod_pitch]: LOD + 1 per (view, object), 0 = culled
+    uint32_t lod_pitch;       // bytes per view row: object_count rounded up to kBatchChunk
     uint32_t view_count;
     uint32_t object_chunks;   // ceil(object_count / kBatchChunk)
     uint32_t hiz_tiles;       // Hi-Z tiles of all views
@@ -51,6 +55,7 @@ struct BatchParams {
     uint32_t* error;          // [1] kBatchErr* bits, zero before the launch
     uint32_t* work;           // [1] phase-1 work queue head, zero before the launch
     uint32_t* chunk_counts;   // [view_count * object_chunks] active spans per (view, chunk)
+    uint32_t* chunk_vis;      // [view_count * object_chunks] visible objects per (view, chunk)
     uint32_t* chunk_offs;     // [view_count * object_chunks + 1]
     uint32_t* seg_totals;     // [gridDim.x]
     uint32_t* view_span_start;  // [view_count + 1] first span of each view (views padded to 32)
@@ -66,6 +71,13 @@ struct BatchParams {
 // [0..7] phase boundaries, [8] / [9] largest per-CTA time spent on Hi-Z tiles /
 // object chunks in phase 1 (ns).
 constexpr uint32_t kBatchPhaseStamps = 10;
+
+// Bounds over the valid objects of a scene (an object with lod_count > 0, an
+// instance in range and a valid transform), as float bits, for the per-view reject
+// boxes: bounds[0] = largest world radius max(local_radius * max_scale, 0),
+// bounds[1] = largest |c.x| + |c.y| + |c.z| of a world centre c (computed exactly as
+// the select computes them). `bounds` must be zero before the launch.
+cudaError_t launch_scene_bounds(const VgSceneDev& scene, uint32_t* bounds, cudaStream_t stream);
 
 // Dynamic shared memory of the persistent kernel (bytes).
 size_t batch_dynamic_smem();

@@ -15,6 +15,7 @@ using helio::DevBuf;
 
 struct helio_vg_scene {
     DevBuf m_bounds, m_cone, m_axis, m_draw, objects, instances, cull, staging;
+    DevBuf bounds;  // [2] launch_scene_bounds of the current objects and instances
     uint32_t meshlet_count = 0, object_count = 0;
     uint64_t lod0_meshlets = 0, max_spans = 0, max_draw_count = 0;
     uint64_t version = 0, instance_version = 0;
@@ -43,10 +44,10 @@ struct helio_batch {
     const helio_vg_scene* scene = nullptr;
     uint32_t view_count = 0;
     std::vector<helio::BatchViewDev> host_views;
-    DevBuf views, cviews, lod, levels, out_indirect, out_draws, clear, chunk_counts, chunk_offs, seg_totals,
+    DevBuf views, cviews, lod, levels, out_indirect, out_draws, clear, chunk_counts, chunk_vis, chunk_offs, seg_totals,
         view_span_start, spans, group_counts, group_offs, group_bits, span_vis;
     size_t clear_bytes = 0;
-    uint32_t grid = 0, object_chunks = 0, hiz_tiles = 0, span_capacity = 0;
+    uint32_t grid = 0, object_chunks = 0, hiz_tiles = 0, span_capacity = 0, lod_pitch = 0;
     std::vector<size_t> out_offset;  // first draw of each view in out_indirect / out_draws
     bool prepared = false;
 
@@ -69,6 +70,13 @@ int32_t copy_in(void* dst, const void* src, size_t bytes, uint32_t memory, cudaS
     HELIO_ARG(src, "frame data array missing");
     HELIO_CK(cudaMemcpyAsync(dst, src, bytes,
                              memory == HELIO_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
+    return HELIO_OK;
+}
+
+int32_t refresh_bounds(helio_vg_scene* sc, cudaStream_t s) {
+    HELIO_CK(sc->bounds.ensure(8));
+    HELIO_CK(cudaMemsetAsync(sc->bounds.ptr, 0, 8, s));
+    HELIO_CK(helio::launch_scene_bounds(sc->dev(), sc->bounds.as<uint32_t>(), s));
     return HELIO_OK;
 }
 
@@ -140,6 +148,7 @@ int32_t helio_vg_scene_upload(helio_vg_scene* sc, const helio_vg_frame_data* f, 
         sc->version = f->buffer_version;
         sc->instance_version = f->instance_version;
         sc->have = true;
+        if ((st = refresh_bounds(sc, s))) return st;
     } else if (f->instance_version != sc->instance_version) {
         const uint64_t start = f->instance_dirty_start, count = f->instance_dirty_count;
         HELIO_ARG(count > 0 && start + count <= sc->object_count, "invalid dirty instance range");
@@ -150,6 +159,7 @@ int32_t helio_vg_scene_upload(helio_vg_scene* sc, const helio_vg_frame_data* f, 
                                          sc->cull.as<HelioInstanceCullData>() + start, s);
         HELIO_CK(cudaGetLastError());
         sc->instance_version = f->instance_version;
+        if ((st = refresh_bounds(sc, s))) return st;
     }
     return HELIO_OK;
 }
@@ -237,8 +247,10 @@ int32_t helio_batch_prepare(helio_batch* b, const helio_vg_scene* sc, uint32_t n
     HELIO_ARG(b->grid > 0, "the batch kernel does not fit on this device");
     HELIO_CK(b->views.ensure(n * sizeof(helio::BatchViewDev)));
     HELIO_CK(b->cviews.ensure(n * sizeof(helio::CullView)));
-    HELIO_CK(b->lod.ensure((size_t)n * (O ? O : 1)));
+    b->lod_pitch = (O + helio::kBatchChunk - 1) / helio::kBatchChunk * helio::kBatchChunk;
+    HELIO_CK(b->lod.ensure((size_t)n * (b->lod_pitch ? b->lod_pitch : helio::kBatchChunk)));
     HELIO_CK(b->chunk_counts.ensure((units + 1) * 4));
+    HELIO_CK(b->chunk_vis.ensure((units + 1) * 4));
     HELIO_CK(b->chunk_offs.ensure((units + 1) * 4));
     HELIO_CK(b->seg_totals.ensure((size_t)b->grid * 4));
     HELIO_CK(b->view_span_start.ensure((size_t)(n + 1) * 4));
@@ -291,6 +303,8 @@ int32_t helio_batch_execute(helio_batch* b, void* stream) {
     P.views = b->views.as<helio::BatchViewDev>();
     P.cviews = b->cviews.as<helio::CullView>();
     P.lod = b->lod.as<uint8_t>();
+    P.lod_pitch = b->lod_pitch;
+    P.scene_bounds = b->scene->bounds.as<uint32_t>();
     P.view_count = b->view_count;
     P.object_chunks = b->object_chunks;
     P.hiz_tiles = b->hiz_tiles;
@@ -298,6 +312,7 @@ int32_t helio_batch_execute(helio_batch* b, void* stream) {
     P.error = b->error();
     P.work = b->work();
     P.chunk_counts = b->chunk_counts.as<uint32_t>();
+    P.chunk_vis = b->chunk_vis.as<uint32_t>();
     P.chunk_offs = b->chunk_offs.as<uint32_t>();
     P.seg_totals = b->seg_totals.as<uint32_t>();
     P.view_span_start = b->view_span_start.as<uint32_t>();
@@ -335,7 +350,7 @@ int32_t helio_batch_get_view_outputs(const helio_batch* b, uint32_t v, helio_bat
     out->indirect = d.indirect;
     out->draws = d.draws;
     out->counters = d.counters;
-    out->lod = b->lod.as<uint8_t>() + (size_t)v * b->scene->object_count;
+    out->lod = b->lod.as<uint8_t>() + (size_t)v * b->lod_pitch;
     out->capacity = d.capacity;
     out->object_count = b->scene->object_count;
     out->pyramid.mip_count = d.hiz.mip_count;
