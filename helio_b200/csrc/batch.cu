@@ -59,8 +59,9 @@ constexpr size_t kSmSelBox = kSmSelViews + sizeof(SelView) * kBatchMaxViews;    
 constexpr size_t kSmSelLod = kSmSelBox + sizeof(SelBox) * kBatchMaxViews;       // u8[kSelectMaxViews][256]
 constexpr size_t kSmSelQueue = kSmSelLod + kSelectMaxViews * kBatchChunk;       // u16[8][kSelQueue]
 constexpr size_t kSmSelSpans = kSmSelQueue + 2 * 8 * kSelQueue;                 // u32[kSelectMaxViews]
-constexpr size_t kSmSelVis = kSmSelSpans + 4 * kSelectMaxViews;                 // u32[kSelectMaxViews]
-constexpr size_t kSmHizJob = kSmSelVis + 4 * kSelectMaxViews;                   // HizJob
+constexpr size_t kSmSelMask = kSmSelSpans + 4 * kSelectMaxViews;                // u32[kSelectMaxViews][8]
+constexpr size_t kSmSelStats = kSmSelMask + 4 * 8 * kSelectMaxViews;             // u32[kSelectMaxViews][9]
+constexpr size_t kSmHizJob = kSmSelStats + 4 * 9 * kSelectMaxViews;             // HizJob
 constexpr size_t kSmHizM3 = kSmHizJob + ((sizeof(HizJob) + 15) / 16) * 16;    // float[8][9]
 constexpr size_t kSmMisc = kSmHizM3 + 8 * 9 * 4;                              // u32[64]
 constexpr size_t kSmTileBegin = kSmMisc + 64 * 4;                             // u32[kBatchMaxViews]
@@ -69,8 +70,9 @@ constexpr size_t kSmTotal = kSmTileBegin + 4 * kBatchMaxViews;
 constexpr size_t kSmTestViews = 0;                                       // CullView per warp
 constexpr size_t kSmTestBits = kSmTestViews + sizeof(CullView) * 8;      // u32[8][66]
 constexpr int kBits = kWindowsPerWarp + 2;
+constexpr size_t kSmTestQueue = kSmTestBits + 8 * kBits * 4;            // u16[8][64]
 constexpr size_t kSmVStart = 0;                                          // u32[kBatchMaxViews + 1]
-static_assert(kSmTestBits + 8 * kBits * 4 <= kSmMisc, "test phase fits");
+static_assert(kSmTestQueue + 8 * 64 * 2 <= kSmMisc, "test phase fits");
 
 __device__ __forceinline__ uint32_t ld_cg(const uint32_t* p) { return __ldcg(p); }
 
@@ -371,7 +373,8 @@ __device__ void select_batch(const BatchParams& P, uint32_t chunk, uint32_t v_be
     const SelView* s_sv = reinterpret_cast<const SelView*>(sm + kSmSelViews);
     uint8_t* s_lod = reinterpret_cast<uint8_t*>(sm + kSmSelLod);
     uint32_t* s_spans = reinterpret_cast<uint32_t*>(sm + kSmSelSpans);
-    uint32_t* s_vis = reinterpret_cast<uint32_t*>(sm + kSmSelVis);
+    uint32_t* s_vmask = reinterpret_cast<uint32_t*>(sm + kSmSelMask);
+    uint32_t* s_stats = reinterpret_cast<uint32_t*>(sm + kSmSelStats);
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     const uint32_t e = lane < n ? (uint32_t)queue[lane] : lane;
     const uint32_t j = e & 31u, k = e >> 5;
@@ -402,15 +405,70 @@ __device__ void select_batch(const BatchParams& P, uint32_t chunk, uint32_t v_be
     }
     const uint32_t cnt = __ldg(&obj->lod_meshlet_counts[lod]);
     s_lod[k * kBatchChunk + slot] = (uint8_t)(lod + 1u);
+    atomicOr(s_vmask + k * 8u + (slot >> 5), 1u << (slot & 31u));
     if (cnt) atomicAdd(s_spans + k, (cnt + 63u) >> 6);
-    atomicAdd(s_vis + k, 1u);
+    // LOD histogram and largest lod_count of the view's visible objects, per unit.
+    atomicAdd(s_stats + k * 9u + lod, 1u);
+    atomicMax(s_stats + k * 9u + 8u, lod_count);
+}
+
+// Position of the r-th (0-based) set bit of x; x has more than r set bits.
+__device__ __forceinline__ uint32_t select_bit(uint32_t x, uint32_t r) {
+    uint32_t p = 0;
+#pragma unroll
+    for (uint32_t w = 16; w; w >>= 1) {
+        const uint32_t c = __popc(x & ((1u << w) - 1u));
+        if (r >= c) {
+            r -= c;
+            x >>= w;
+            p += w;
+        }
+    }
+    return p;
+}
+
+// The visible objects of view v in a chunk, in object order, by one warp: entry i
+// = slot | LOD << 8 of the i-th set bit of the chunk's 256-bit mask (lane i of
+// round i / 32 finds it from the words' bit counts, scanned over lanes 0..7).
+__device__ void select_write_list(const BatchParams& P, uint32_t chunk, uint32_t v, const uint8_t* row,
+                                  const uint32_t* mask, const uint32_t* stats, uint32_t spans) {
+    const uint32_t lane = threadIdx.x & 31u;
+    // The unit's share of counters 2..9 (LOD histogram) and 10 (largest lod_count - 1).
+    if (lane < 9u && stats[lane]) {
+        uint32_t* counters = P.views[v].counters;
+        if (lane < 8u) atomicAdd(counters + 2 + lane, stats[lane]);
+        else atomicMax(counters + 10, stats[8] - 1u);
+    }
+    const uint32_t word = lane < 8u ? mask[lane] : 0u;
+    const uint32_t wc = __popc(word);
+    const uint32_t winc = warp_inclusive(wc);
+    const uint32_t visible = __shfl_sync(0xffffffffu, winc, 7);
+    const size_t u = (size_t)v * P.object_chunks + chunk;
+    uint16_t* list = P.vis_list + u * kBatchChunk;
+    for (uint32_t base = 0; base < visible; base += 32u) {
+        const uint32_t i = base + lane;
+        uint32_t w = 0;  // the word of the i-th set bit: words whose inclusive count is <= i
+#pragma unroll
+        for (uint32_t q = 0; q < 8u; ++q) w += __shfl_sync(0xffffffffu, winc, q) <= i ? 1u : 0u;
+        w = min(w, 7u);
+        const uint32_t before = __shfl_sync(0xffffffffu, winc - wc, w);
+        const uint32_t wd = __shfl_sync(0xffffffffu, word, w);
+        if (i < visible) {
+            const uint32_t slot = w * 32u + select_bit(wd, i - before);
+            list[i] = (uint16_t)(slot | ((uint32_t)(row[slot] - 1u) << 8));
+        }
+    }
+    if (lane == 0) {
+        P.chunk_counts[u] = spans;
+        P.chunk_vis[u] = visible;
+    }
 }
 
 __device__ void phase_select_chunk(const BatchParams& P, uint32_t chunk, uint32_t v_begin, uint32_t v_end, char* sm) {
     const SelBox* s_box = reinterpret_cast<const SelBox*>(sm + kSmSelBox);
     uint4* s_lod4 = reinterpret_cast<uint4*>(sm + kSmSelLod);
     uint32_t* s_spans = reinterpret_cast<uint32_t*>(sm + kSmSelSpans);
-    uint32_t* s_vis = reinterpret_cast<uint32_t*>(sm + kSmSelVis);
+    uint32_t* s_vmask = reinterpret_cast<uint32_t*>(sm + kSmSelMask);
     const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5, nv = v_end - v_begin;
     const VgSceneDev& S = P.scene;
     const uint32_t o = chunk * kBatchChunk + tid;
@@ -436,10 +494,10 @@ __device__ void phase_select_chunk(const BatchParams& P, uint32_t chunk, uint32_
     __syncthreads();  // the previous unit is done with the tile and the counters
     constexpr uint32_t kRow4 = kBatchChunk / 16;  // 16-byte words per tile row
     for (uint32_t i = tid; i < nv * kRow4; i += kBatchThreads) s_lod4[i] = make_uint4(0u, 0u, 0u, 0u);
-    if (tid < nv) {
-        s_spans[tid] = 0u;
-        s_vis[tid] = 0u;
-    }
+    if (tid < nv) s_spans[tid] = 0u;
+    if (tid < nv * 8u) s_vmask[tid] = 0u;
+    uint32_t* s_stats = reinterpret_cast<uint32_t*>(sm + kSmSelStats);
+    for (uint32_t i = tid; i < nv * 9u; i += kBatchThreads) s_stats[i] = 0u;
     __syncthreads();
     uint16_t* q = reinterpret_cast<uint16_t*>(sm + kSmSelQueue) + warp * kSelQueue;
     const uint32_t lt = (1u << lane) - 1u;
@@ -475,11 +533,10 @@ __device__ void phase_select_chunk(const BatchParams& P, uint32_t chunk, uint32_
         *reinterpret_cast<uint4*>(P.lod + (size_t)(v_begin + k) * P.lod_pitch + chunk * kBatchChunk + w4 * 16u) =
             s_lod4[i];
     }
-    if (tid < nv) {
-        const size_t u = (size_t)(v_begin + tid) * P.object_chunks + chunk;
-        P.chunk_counts[u] = s_spans[tid];
-        P.chunk_vis[u] = s_vis[tid];
-    }
+    const uint8_t* s_lod = reinterpret_cast<const uint8_t*>(sm + kSmSelLod);
+    for (uint32_t k = warp; k < nv; k += kBatchThreads / 32)
+        select_write_list(P, chunk, v_begin + k, s_lod + k * kBatchChunk, s_vmask + k * 8u, s_stats + k * 9u,
+                          s_spans[k]);
 }
 
 // ── Phase 3: expansion into the view-major list of active spans ──────────────
@@ -523,65 +580,41 @@ __device__ void phase_expand(const BatchParams& P, char* sm) {
     // heavy consecutive chunks of a large view spread over many warps.
     for (uint32_t k0 = 0; gw + (size_t)k0 * GW < n_units; k0 += 32u) {
         const size_t u = gw + (size_t)(k0 + lane) * GW;
-        // A unit with a visible object has spans to write or LOD statistics to count.
+        // Units with visible objects (the only ones that can have spans).
         const uint32_t busy = u < n_units ? ld_cg(P.chunk_vis + u) : 0u;
         uint32_t mask = __ballot_sync(0xffffffffu, busy != 0u);
         while (mask) {
-            const uint32_t uu = gw + (k0 + (__ffs(mask) - 1)) * GW;
+            const uint32_t src_lane = __ffs(mask) - 1;
+            const uint32_t uu = gw + (k0 + src_lane) * GW;
+            const uint32_t vis = __shfl_sync(0xffffffffu, busy, src_lane);
             mask &= mask - 1u;
             const uint32_t v = uu / C, ch = uu - v * C;
             uint32_t pos = s_vstart[v] + (ld_cg(P.chunk_offs + uu) - ld_cg(P.chunk_offs + (size_t)v * C));
-            // All loads of the chunk's 256 objects are issued before any is used: one
-            // round trip for the LOD bytes, one for the objects' selected ranges.
-            constexpr int R = kBatchChunk / 32;
-            const uint8_t* lrow = P.lod + (size_t)v * P.lod_pitch;
-            uint32_t sel[R], count[R], first[R], inst[R];
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-                const uint32_t o = ch * kBatchChunk + r * 32u + lane;
-                sel[r] = o < S.object_count ? (uint32_t)__ldcg(lrow + o) : 0u;
-            }
-            // LOD histogram (4-bit lanes: at most R objects per lane) and the largest
-            // lod_count - 1 of the visible objects: counters 2..9 and 10 of the view.
-            uint32_t hist = 0u, top = 0u;
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-                count[r] = first[r] = inst[r] = 0u;
-                if (sel[r]) {
-                    const HelioGpuVgObject* obj = S.objects + (ch * kBatchChunk + r * 32u + lane);
-                    const uint2 h = __ldg(reinterpret_cast<const uint2*>(obj));  // instance_index, lod_count
-                    count[r] = __ldg(&obj->lod_meshlet_counts[sel[r] - 1u]);
-                    first[r] = __ldg(&obj->lod_first_meshlets[sel[r] - 1u]);
-                    inst[r] = h.x;
-                    hist += 1u << (4u * (sel[r] - 1u));
-                    top = max(top, min(h.y, 8u));  // lod_count - 1 + 1
+            // Round trip 1: the chunk's visible list (slot | LOD << 8, object order);
+            // round trip 2: the visible objects' selected ranges.
+            const uint16_t* list = P.vis_list + (size_t)uu * kBatchChunk;
+            for (uint32_t base = 0; base < vis; base += 32u) {
+                const uint32_t i = base + lane;
+                uint32_t count = 0, first = 0, inst = 0, lod = 0, o = 0;
+                if (i < vis) {
+                    const uint32_t e = __ldcg(list + i);
+                    lod = e >> 8;
+                    o = ch * kBatchChunk + (e & 0xFFu);
+                    const HelioGpuVgObject* obj = S.objects + o;
+                    count = __ldg(&obj->lod_meshlet_counts[lod]);
+                    first = __ldg(&obj->lod_first_meshlets[lod]);
+                    inst = __ldg(&obj->instance_index);
                 }
-            }
-            {
-                uint32_t* counters = P.views[v].counters;
-#pragma unroll
-                for (uint32_t l = 0; l < 8u; ++l) {
-                    const uint32_t n = __reduce_add_sync(0xffffffffu, (hist >> (4u * l)) & 15u);
-                    if (lane == 0 && n) atomicAdd(counters + 2 + l, n);
-                }
-                top = __reduce_max_sync(0xffffffffu, top);
-                if (lane == 0 && top) atomicMax(counters + 10, top - 1u);
-            }
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-                const uint32_t o = ch * kBatchChunk + r * 32u + lane;
-                const uint32_t lod = sel[r] ? sel[r] - 1u : 0u;
-                const uint32_t ns = (count[r] + 63u) >> 6;
+                const uint32_t ns = (count + 63u) >> 6;
                 const uint32_t inc = warp_inclusive(ns);
-                const uint32_t total = __shfl_sync(0xffffffffu, inc, 31);
                 uint32_t p = pos + inc - ns;
                 for (uint32_t j = 0; j < ns; ++j, ++p) {
                     if (p < P.span_capacity) {
-                        const uint32_t n = min(64u, count[r] - 64u * j);
-                        P.spans[p] = make_uint4(first[r] + 64u * j, n | (lod << 8) | (v << 16), inst[r], o);
+                        const uint32_t n = min(64u, count - 64u * j);
+                        P.spans[p] = make_uint4(first + 64u * j, n | (lod << 8) | (v << 16), inst, o);
                     }
                 }
-                pos += total;
+                pos += __shfl_sync(0xffffffffu, inc, 31);
             }
         }
     }
@@ -614,10 +647,36 @@ __device__ __forceinline__ GroupSpans load_group(const BatchParams& P, uint32_t 
 }
 
 // ── Phase 4: meshlet tests of every group of 32 spans ────────────────────────
+// Hi-Z tests of n <= 32 queued candidates of a group (lane i takes entry i, a
+// meshlet position s of the group); visible ones set bit s of the group's bits.
+__device__ void test_hiz_batch(const VgSceneDev& S, const CullView& cv, const GroupSpans& gs, const uint16_t* q,
+                               uint32_t n, uint32_t* bits) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t s = lane < n ? (uint32_t)q[lane] : 0u;
+    const int j = owner_lane(gs.off, s);
+    const uint32_t j_off = __shfl_sync(0xffffffffu, gs.off, j);
+    const uint32_t j_first = __shfl_sync(0xffffffffu, gs.first, j);
+    const uint32_t j_inst = __shfl_sync(0xffffffffu, gs.inst, j);
+    if (lane >= n) return;
+    const uint32_t mi = j_first + (s - j_off);
+    const HelioInstanceCullData cd = load_cull(S.cull + j_inst);
+    const Mat4 model = ldg_mat4(S.instances[j_inst].model);
+    F3 c;
+    float wr;
+    meshlet_sphere(S, mi, model, cd, c, wr);
+    if (meshlet_hiz_visible<true>(cv, c, wr)) atomicOr(bits + (s >> 5), 1u << (s & 31u));
+}
+
+// Per group of 32 spans, the warp runs the frustum and cone tests window by window
+// (32 meshlets packed densely across the spans) and queues the meshlets that pass;
+// every 32 queued meshlets take the Hi-Z test together, so that the costly Hi-Z
+// test runs on full warps although about half the meshlets leave earlier.
 __device__ void phase_test(const BatchParams& P, uint32_t groups, char* sm) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     CullView& cv = *reinterpret_cast<CullView*>(sm + kSmTestViews + sizeof(CullView) * warp);
     uint32_t* bits = reinterpret_cast<uint32_t*>(sm + kSmTestBits) + warp * kBits;
+    uint16_t* q = reinterpret_cast<uint16_t*>(sm + kSmTestQueue) + warp * 64;
+    const uint32_t lt = (1u << lane) - 1u;
     const VgSceneDev& S = P.scene;
     uint32_t cached_view = 0xFFFFFFFFu;
     const uint32_t gw = blockIdx.x * (kBatchThreads / 32) + warp, GW = gridDim.x * (kBatchThreads / 32);
@@ -632,29 +691,49 @@ __device__ void phase_test(const BatchParams& P, uint32_t groups, char* sm) {
         }
         for (int k = lane; k < kBits; k += 32) bits[k] = 0u;
         __syncwarp();
-        uint32_t count = 0;
         const uint32_t windows = (gs.total + 31u) >> 5;
+        uint32_t qn = 0;  // warp-uniform
         for (uint32_t win = 0; win < windows; ++win) {
             const uint32_t s = win * 32u + lane;
             const int j = owner_lane(gs.off, s);
             const uint32_t j_off = __shfl_sync(0xffffffffu, gs.off, j);
             const uint32_t j_first = __shfl_sync(0xffffffffu, gs.first, j);
             const uint32_t j_inst = __shfl_sync(0xffffffffu, gs.inst, j);
-            bool vis = false;
+            bool cand = false;
             if (s < gs.total) {
                 const uint32_t mi = j_first + (s - j_off);
                 if (mi < S.meshlet_count) {
                     const HelioGpuInstanceData* in = S.instances + j_inst;
                     const HelioInstanceCullData cd = load_cull(S.cull + j_inst);
                     const Mat4 model = ldg_mat4(in->model);
-                    vis = meshlet_visible<true>(S, cv, mi, model, cd, in);
+                    F3 c;
+                    float wr;
+                    cand = meshlet_frustum_cone(cv, load_meshlet(S, mi, in), model, cd, c, wr);
                 }
             }
-            const uint32_t b = __ballot_sync(0xffffffffu, vis);
-            if (lane == 0) bits[win] = b;
-            count += __popc(b);
+            const uint32_t b = __ballot_sync(0xffffffffu, cand);
+            if (cand) q[qn + __popc(b & lt)] = (uint16_t)s;
+            qn += __popc(b);
+            if (qn >= 32u) {
+                __syncwarp();
+                test_hiz_batch(S, cv, gs, q, 32u, bits);
+                __syncwarp();
+                const uint32_t rest = qn - 32u;
+                const uint16_t x = (uint32_t)lane < rest ? q[32 + lane] : (uint16_t)0;
+                __syncwarp();
+                if ((uint32_t)lane < rest) q[lane] = x;
+                __syncwarp();
+                qn = rest;
+            }
+        }
+        if (qn) {
+            __syncwarp();
+            test_hiz_batch(S, cv, gs, q, qn, bits);
         }
         __syncwarp();
+        uint32_t count = __popc(bits[lane]) + __popc(bits[lane + 32]);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) count += __shfl_xor_sync(0xffffffffu, count, o);
         if (lane == 0) P.group_counts[g] = count;
         if (count)
             for (uint32_t k = lane; k < windows; k += 32) P.group_bits[(size_t)g * kWindowsPerWarp + k] = bits[k];

@@ -56,6 +56,8 @@ struct BatchParams {
     uint32_t* work;           // [1] phase-1 work queue head, zero before the launch
     uint32_t* chunk_counts;   // [view_count * object_chunks] active spans per (view, chunk)
     uint32_t* chunk_vis;      // [view_count * object_chunks] visible objects per (view, chunk)
+    uint16_t* vis_list;       // [view_count * object_chunks * kBatchChunk] per (view, chunk): its
+                              // visible objects in object order, slot | LOD << 8
     uint32_t* chunk_offs;     // [view_count * object_chunks + 1]
     uint32_t* seg_totals;     // [gridDim.x]
     uint32_t* view_span_start;  // [view_count + 1] first span of each view (views padded to 32)

@@ -3,6 +3,7 @@
 
 #include <cstring>
 #include <new>
+#include <algorithm>
 #include <vector>
 
 #include "batch.h"
@@ -44,7 +45,7 @@ struct helio_batch {
     const helio_vg_scene* scene = nullptr;
     uint32_t view_count = 0;
     std::vector<helio::BatchViewDev> host_views;
-    DevBuf views, cviews, lod, levels, out_indirect, out_draws, clear, chunk_counts, chunk_vis, chunk_offs, seg_totals,
+    DevBuf views, cviews, lod, levels, out_indirect, out_draws, clear, chunk_counts, chunk_vis, vis_list, chunk_offs, seg_totals,
         view_span_start, spans, group_counts, group_offs, group_bits, span_vis;
     size_t clear_bytes = 0;
     uint32_t grid = 0, object_chunks = 0, hiz_tiles = 0, span_capacity = 0, lod_pitch = 0;
@@ -251,6 +252,7 @@ int32_t helio_batch_prepare(helio_batch* b, const helio_vg_scene* sc, uint32_t n
     HELIO_CK(b->lod.ensure((size_t)n * (b->lod_pitch ? b->lod_pitch : helio::kBatchChunk)));
     HELIO_CK(b->chunk_counts.ensure((units + 1) * 4));
     HELIO_CK(b->chunk_vis.ensure((units + 1) * 4));
+    HELIO_CK(b->vis_list.ensure(std::max<size_t>(1, units) * helio::kBatchChunk * sizeof(uint16_t)));
     HELIO_CK(b->chunk_offs.ensure((units + 1) * 4));
     HELIO_CK(b->seg_totals.ensure((size_t)b->grid * 4));
     HELIO_CK(b->view_span_start.ensure((size_t)(n + 1) * 4));
@@ -313,6 +315,7 @@ int32_t helio_batch_execute(helio_batch* b, void* stream) {
     P.work = b->work();
     P.chunk_counts = b->chunk_counts.as<uint32_t>();
     P.chunk_vis = b->chunk_vis.as<uint32_t>();
+    P.vis_list = b->vis_list.as<uint16_t>();
     P.chunk_offs = b->chunk_offs.as<uint32_t>();
     P.seg_totals = b->seg_totals.as<uint32_t>();
     P.view_span_start = b->view_span_start.as<uint32_t>();

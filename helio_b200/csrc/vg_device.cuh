@@ -24,39 +24,68 @@ __device__ __forceinline__ void load_view(const CullView* src, CullView& dst, in
     for (int k = tid; k < (int)(sizeof(CullView) / 16); k += nthreads) d[k] = __ldg(s + k);
 }
 
-// cull_meshlet decision part (vg_cull.wgsl:143-240): true = emit a draw.
-// kCoherentHiz: the pyramid was written earlier in the same launch.
-template <bool kCoherentHiz = false>
-__device__ __forceinline__ bool meshlet_visible(const VgSceneDev& S, const CullView& C, uint32_t mi,
-                                                const Mat4& model, const HelioInstanceCullData& cd,
-                                                const HelioGpuInstanceData* inst) {
-    const Planes& pl = C.planes;
-    const HizView& hz = C.hiz;
-    const uint32_t screen_h = C.screen_height, hiz_mip_count = C.hiz_mip_count;
-    if (cd.valid_transform == 0u) return false;
+// World-space bounding sphere of meshlet mi of an instance (vg_cull.wgsl:150-152).
+__device__ __forceinline__ void meshlet_sphere(const VgSceneDev& S, uint32_t mi, const Mat4& model,
+                                               const HelioInstanceCullData& cd, F3& c, float& wr) {
     const float4 b = __ldg(S.m_bounds + mi);
-    const F3 c = mat4_point3(model, f3(b.x, b.y, b.z));
-    const float wr = fmaxf(fmul(b.w, cd.max_scale), 0.0f);
-    const F3 cam = f3(C.pos_near.x, C.pos_near.y, C.pos_near.z);
-    const F3 ctc = sub3(c, cam);
-    if (!sphere_visible_vg(pl, c, wr)) return false;
+    c = mat4_point3(model, f3(b.x, b.y, b.z));
+    wr = fmaxf(fmul(b.w, cd.max_scale), 0.0f);
+}
+
+// Everything the frustum and cone tests read of one meshlet of one instance,
+// loaded in one go (one memory round trip instead of one per test).
+struct MeshletInputs {
+    float4 bounds, cone, axis;
+    float4 n0, n1, n2;  // the instance's normal matrix columns
+};
+
+__device__ __forceinline__ MeshletInputs load_meshlet(const VgSceneDev& S, uint32_t mi,
+                                                      const HelioGpuInstanceData* inst) {
+    MeshletInputs m;
+    m.bounds = __ldg(S.m_bounds + mi);
+    m.cone = __ldg(S.m_cone + mi);
+    m.axis = __ldg(S.m_axis + mi);
+    const float4* nm = reinterpret_cast<const float4*>(inst->normal_mat);
+    m.n0 = __ldg(nm);
+    m.n1 = __ldg(nm + 1);
+    m.n2 = __ldg(nm + 2);
+    return m;
+}
+
+// cull_meshlet, first part (vg_cull.wgsl:143-182): the frustum and normal-cone
+// tests. True = the meshlet is still a candidate and the Hi-Z test decides it;
+// (c, wr) is its world-space sphere.
+__device__ __forceinline__ bool meshlet_frustum_cone(const CullView& C, const MeshletInputs& m, const Mat4& model,
+                                                     const HelioInstanceCullData& cd, F3& c, float& wr) {
+    if (cd.valid_transform == 0u) return false;
+    c = mat4_point3(model, f3(m.bounds.x, m.bounds.y, m.bounds.z));
+    wr = fmaxf(fmul(m.bounds.w, cd.max_scale), 0.0f);
+    if (!sphere_visible_vg(C.planes, c, wr)) return false;
     // Perspective normal-cone test (:159-182).
     if (cd.cone_cull_enabled != 0u) {
-        const float4 cone = __ldg(S.m_cone + mi);
+        const F3 cam = f3(C.pos_near.x, C.pos_near.y, C.pos_near.z);
+        const F3 ctc = sub3(c, cam);
         const float cam_dist_sq = dot3(ctc, ctc);
         const float guard = fmul(wr, 1.5f);
-        if (cam_dist_sq > fmul(guard, guard) && cone.w <= 1.0f) {
-            const float4 ax = __ldg(S.m_axis + mi);
-            const float4* nm = reinterpret_cast<const float4*>(inst->normal_mat);
-            const F3 a = mat3_vec(__ldg(nm), __ldg(nm + 1), __ldg(nm + 2), f3(ax.x, ax.y, ax.z));
+        if (cam_dist_sq > fmul(guard, guard) && m.cone.w <= 1.0f) {
+            const F3 a = mat3_vec(m.n0, m.n1, m.n2, f3(m.axis.x, m.axis.y, m.axis.z));
             const F3 axis_ws = divs3(a, fsqrt(dot3(a, a)));
-            const F3 apex = mat4_point3(model, f3(cone.x, cone.y, cone.z));
+            const F3 apex = mat4_point3(model, f3(m.cone.x, m.cone.y, m.cone.z));
             const F3 cta = sub3(apex, cam);
             const float ads = dot3(cta, cta);
-            if (ads > 1.0e-12f && dot3(divs3(cta, fsqrt(ads)), axis_ws) >= cone.w) return false;
+            if (ads > 1.0e-12f && dot3(divs3(cta, fsqrt(ads)), axis_ws) >= m.cone.w) return false;
         }
     }
-    // Conservative Hi-Z test (:184-240).
+    return true;
+}
+
+// cull_meshlet, second part (vg_cull.wgsl:184-240): the conservative Hi-Z test of
+// the sphere (c, wr). True = visible. kCoherentHiz: the pyramid was written
+// earlier in the same launch.
+template <bool kCoherentHiz = false>
+__device__ __forceinline__ bool meshlet_hiz_visible(const CullView& C, F3 c, float wr) {
+    const HizView& hz = C.hiz;
+    const F3 ctc = sub3(c, f3(C.pos_near.x, C.pos_near.y, C.pos_near.z));
     const float4 clip = mat4_point4(C.vp, c);
     if (clip.w > 0.0f) {
         const float ndc_x = fdiv(clip.x, clip.w), ndc_y = fdiv(clip.y, clip.w);
@@ -75,9 +104,9 @@ __device__ __forceinline__ bool meshlet_visible(const VgSceneDev& S, const CullV
                     const float4 nc = mat4_point4(C.vp, nws);
                     if (nc.w > 0.0f) near_z = clampf(fdiv(nc.z, nc.w), 0.0f, 1.0f);
                 }
-                const float half_h = fmul((float)screen_h, 0.5f);
+                const float half_h = fmul((float)C.screen_height, 0.5f);
                 const float dpx = fmaxf(fmul(fmul(ndc_r, half_h), 2.0f), 1.0f);
-                const uint32_t mip = min(ceil_log2_exact(dpx), hiz_mip_count - 1u);
+                const uint32_t mip = min(ceil_log2_exact(dpx), C.hiz_mip_count - 1u);
                 const float h00 = hiz_sample<kCoherentHiz>(hz, u0, v0, mip);
                 const float h01 = hiz_sample<kCoherentHiz>(hz, u1, v0, mip);
                 const float h10 = hiz_sample<kCoherentHiz>(hz, u0, v1, mip);
@@ -88,6 +117,17 @@ __device__ __forceinline__ bool meshlet_visible(const VgSceneDev& S, const CullV
         }
     }
     return true;
+}
+
+// cull_meshlet decision part (vg_cull.wgsl:143-240): true = emit a draw.
+template <bool kCoherentHiz = false>
+__device__ __forceinline__ bool meshlet_visible(const VgSceneDev& S, const CullView& C, uint32_t mi,
+                                                const Mat4& model, const HelioInstanceCullData& cd,
+                                                const HelioGpuInstanceData* inst) {
+    F3 c;
+    float wr;
+    if (!meshlet_frustum_cone(C, load_meshlet(S, mi, inst), model, cd, c, wr)) return false;
+    return meshlet_hiz_visible<kCoherentHiz>(C, c, wr);
 }
 
 // Largest lane j whose exclusive offset is <= s (for s below the warp total this
