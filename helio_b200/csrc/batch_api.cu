@@ -52,6 +52,14 @@ struct helio_batch {
     std::vector<size_t> out_offset;  // first draw of each view in out_indirect / out_draws
     bool prepared = false;
 
+    // Buffer k of the plan's order (kBuf* below).
+    DevBuf& buf(int k) {
+        DevBuf* all[] = {&levels, &out_indirect, &out_draws, &clear, &views, &cviews, &lod, &chunk_counts,
+                         &chunk_vis, &vis_list, &chunk_offs, &seg_totals, &view_span_start, &spans,
+                         &group_counts, &group_offs, &group_bits, &span_vis};
+        return *all[k];
+    }
+
     // Cleared region: counters (16 words per view) | barrier (2) | error (1) |
     // work queue (1) | phase stamps (u64, 8-byte aligned).
     uint32_t* counters(uint32_t v) const { return clear.as<uint32_t>() + 16u * v; }
@@ -78,6 +86,81 @@ int32_t refresh_bounds(helio_vg_scene* sc, cudaStream_t s) {
     HELIO_CK(sc->bounds.ensure(8));
     HELIO_CK(cudaMemsetAsync(sc->bounds.ptr, 0, 8, s));
     HELIO_CK(helio::launch_scene_bounds(sc->dev(), sc->bounds.as<uint32_t>(), s));
+    return HELIO_OK;
+}
+
+// Device buffers of a batch, in helio_batch::buf order.
+enum {
+    kBufLevels, kBufIndirect, kBufDraws, kBufClear, kBufViews, kBufCViews, kBufLod, kBufChunkCounts, kBufChunkVis,
+    kBufVisList, kBufChunkOffs, kBufSegTotals, kBufViewSpanStart, kBufSpans, kBufGroupCounts, kBufGroupOffs,
+    kBufGroupBits, kBufSpanVis, kBatchBufs
+};
+
+// Everything helio_batch_prepare sizes for a set of views: per-buffer bytes, the
+// pyramid layout of each view (written into `dev` when given), output capacities.
+struct BatchPlan {
+    size_t need[kBatchBufs] = {};
+    std::vector<size_t> level_off, out_offset;
+    std::vector<uint32_t> capacity;
+    uint32_t tiles = 0, grid = 0, object_chunks = 0, span_capacity = 0, lod_pitch = 0;
+};
+
+int32_t plan_batch(const helio_batch_config& cfg, const helio_vg_scene* sc, uint32_t n, const helio_batch_view* views,
+                   BatchPlan& p, helio::BatchViewDev* dev) {
+    p.level_off.assign(n, 0);
+    p.out_offset.assign(n + 1, 0);
+    p.capacity.assign(n, 0);
+    size_t level_floats = 0;
+    const uint64_t default_cap = sc->max_draw_count < HELIO_VG_DEFAULT_PUBLICATION_LIMIT
+                                     ? sc->max_draw_count
+                                     : (uint64_t)HELIO_VG_DEFAULT_PUBLICATION_LIMIT;
+    for (uint32_t v = 0; v < n; ++v) {
+        const helio_batch_view& in = views[v];
+        HELIO_ARG(in.width > 0 && in.height > 0 && in.width <= 32768 && in.height <= 32768,
+                  "view size out of 1..32768");
+        const uint32_t pitch = in.depth_pitch ? in.depth_pitch : in.width;
+        HELIO_ARG(pitch >= in.width, "depth pitch smaller than width");
+        helio::HizJob job{};
+        helio::HizJob& J = dev ? dev[v].hiz : job;
+        const size_t need = helio::hiz_layout(in.width, in.height, pitch, (in.flags & HELIO_HIZ_ALIAS_MIP0) == 0u, &J);
+        p.level_off[v] = level_floats;
+        level_floats += (need + 3u) & ~(size_t)3u;
+        J.tile_begin = p.tiles;
+        p.tiles += J.tiles_x * J.tiles_y;
+        const uint32_t cap = in.draw_capacity ? in.draw_capacity : (uint32_t)default_cap;
+        p.capacity[v] = cap;
+        p.out_offset[v + 1] = p.out_offset[v] + (cap ? cap : 1);
+    }
+    const uint32_t O = sc->object_count;
+    p.object_chunks = (O + helio::kBatchChunk - 1) / helio::kBatchChunk;
+    uint64_t span_cap = cfg.max_spans ? cfg.max_spans : (uint64_t)n * sc->max_spans + 32ull * n;
+    span_cap = (span_cap + 31u) & ~31ull;
+    HELIO_ARG(span_cap <= 0x7FFFFFE0ull, "span capacity exceeds 2^31");
+    p.span_capacity = (uint32_t)span_cap;
+    p.grid = helio::batch_max_grid();
+    HELIO_ARG(p.grid > 0, "the batch kernel does not fit on this device");
+    if (cfg.max_ctas && cfg.max_ctas < p.grid) p.grid = cfg.max_ctas;
+    p.lod_pitch = p.object_chunks * helio::kBatchChunk;
+    const size_t units = (size_t)n * p.object_chunks, groups = p.span_capacity / 32u;
+    p.need[kBufLevels] = level_floats * sizeof(float);
+    p.need[kBufIndirect] = p.out_offset[n] * sizeof(HelioDrawIndexedIndirectArgs);
+    p.need[kBufDraws] = p.out_offset[n] * sizeof(HelioGpuVgDraw);
+    p.need[kBufClear] = (((16u * n + 4u) * 4u + 7u) & ~(size_t)7u) + helio::kBatchPhaseStamps * 8u;
+    p.need[kBufViews] = n * sizeof(helio::BatchViewDev);
+    p.need[kBufCViews] = n * sizeof(helio::CullView);
+    p.need[kBufLod] = (size_t)n * (p.lod_pitch ? p.lod_pitch : helio::kBatchChunk);
+    p.need[kBufChunkCounts] = (units + 1) * 4;
+    p.need[kBufChunkVis] = (units + 1) * 4;
+    p.need[kBufVisList] = std::max<size_t>(1, units) * helio::kBatchChunk * sizeof(uint16_t);
+    p.need[kBufChunkOffs] = (units + 1) * 4;
+    p.need[kBufSegTotals] = (size_t)p.grid * 4;
+    p.need[kBufViewSpanStart] = (size_t)(n + 1) * 4;
+    p.need[kBufSpans] = (size_t)p.span_capacity * sizeof(helio::ActiveSpan);
+    p.need[kBufGroupCounts] = (groups + 1) * 4;
+    p.need[kBufGroupOffs] = (groups + 1) * 4;
+    p.need[kBufGroupBits] = (groups + 1) * helio::kWindowsPerWarp * 4;
+    p.need[kBufSpanVis] = (cfg.flags & HELIO_BATCH_SPAN_VISIBILITY) ? (size_t)p.span_capacity * 8 : 0;
+    for (size_t& x : p.need) x = x ? x : 16;  // DevBuf::ensure allocates at least 16 bytes
     return HELIO_OK;
 }
 
@@ -198,69 +281,22 @@ int32_t helio_batch_prepare(helio_batch* b, const helio_vg_scene* sc, uint32_t n
     b->scene = sc;
     b->view_count = n;
     b->host_views.assign(n, helio::BatchViewDev{});
+    for (uint32_t v = 0; v < n; ++v) HELIO_ARG(views[v].depth, "view depth missing");
 
-    // Pyramids (one buffer for every view) and Hi-Z jobs.
-    std::vector<size_t> level_off(n);
-    size_t level_floats = 0;
-    uint32_t tiles = 0;
-    for (uint32_t v = 0; v < n; ++v) {
-        const helio_batch_view& in = views[v];
-        HELIO_ARG(in.depth && in.width > 0 && in.height > 0 && in.width <= 32768 && in.height <= 32768,
-                  "view depth missing or size out of 1..32768");
-        const uint32_t pitch = in.depth_pitch ? in.depth_pitch : in.width;
-        HELIO_ARG(pitch >= in.width, "depth pitch smaller than width");
-        helio::BatchViewDev& d = b->host_views[v];
-        const size_t need = helio::hiz_layout(in.width, in.height, pitch, (in.flags & HELIO_HIZ_ALIAS_MIP0) == 0u,
-                                              &d.hiz);
-        level_off[v] = level_floats;
-        level_floats += (need + 3u) & ~(size_t)3u;
-        d.hiz.tile_begin = tiles;
-        tiles += d.hiz.tiles_x * d.hiz.tiles_y;
-    }
-    HELIO_CK(b->levels.ensure(level_floats * sizeof(float)));
-    // Per-view outputs.
-    const uint64_t default_cap = sc->max_draw_count < HELIO_VG_DEFAULT_PUBLICATION_LIMIT
-                                     ? sc->max_draw_count
-                                     : (uint64_t)HELIO_VG_DEFAULT_PUBLICATION_LIMIT;
-    b->out_offset.assign(n + 1, 0);
-    for (uint32_t v = 0; v < n; ++v) {
-        const uint32_t cap = views[v].draw_capacity ? views[v].draw_capacity : (uint32_t)default_cap;
-        b->host_views[v].capacity = cap;
-        b->out_offset[v + 1] = b->out_offset[v] + (cap ? cap : 1);
-    }
-    HELIO_CK(b->out_indirect.ensure(b->out_offset[n] * sizeof(HelioDrawIndexedIndirectArgs)));
-    HELIO_CK(b->out_draws.ensure(b->out_offset[n] * sizeof(HelioGpuVgDraw)));
-    b->view_count = n;
-    b->clear_bytes = b->stamps_offset() + helio::kBatchPhaseStamps * sizeof(unsigned long long);
-    HELIO_CK(b->clear.ensure(b->clear_bytes));
+    BatchPlan plan;
+    int32_t st;
+    if ((st = plan_batch(b->cfg, sc, n, views, plan, b->host_views.data()))) return st;
+    b->grid = plan.grid;
+    b->object_chunks = plan.object_chunks;
+    b->hiz_tiles = plan.tiles;
+    b->span_capacity = plan.span_capacity;
+    b->lod_pitch = plan.lod_pitch;
+    b->out_offset = plan.out_offset;
+    for (uint32_t v = 0; v < n; ++v) b->host_views[v].capacity = plan.capacity[v];
+    for (int k = 0; k < kBatchBufs; ++k) HELIO_CK(b->buf(k).ensure(plan.need[k]));
+    b->clear_bytes = plan.need[kBufClear];
     HELIO_CK(cudaMemsetAsync(b->clear.ptr, 0, b->clear_bytes, s));
-    // Scratch.
-    const uint32_t O = sc->object_count;
-    b->object_chunks = (O + helio::kBatchChunk - 1) / helio::kBatchChunk;
-    b->hiz_tiles = tiles;
-    uint64_t span_cap = b->cfg.max_spans ? b->cfg.max_spans : (uint64_t)n * sc->max_spans + 32ull * n;
-    span_cap = (span_cap + 31u) & ~31ull;
-    HELIO_ARG(span_cap <= 0x7FFFFFE0ull, "span capacity exceeds 2^31");
-    b->span_capacity = (uint32_t)span_cap;
-    const size_t units = (size_t)n * b->object_chunks;
-    const uint32_t groups = b->span_capacity / 32u;
-    b->grid = helio::batch_max_grid();
-    HELIO_ARG(b->grid > 0, "the batch kernel does not fit on this device");
-    HELIO_CK(b->views.ensure(n * sizeof(helio::BatchViewDev)));
-    HELIO_CK(b->cviews.ensure(n * sizeof(helio::CullView)));
-    b->lod_pitch = (O + helio::kBatchChunk - 1) / helio::kBatchChunk * helio::kBatchChunk;
-    HELIO_CK(b->lod.ensure((size_t)n * (b->lod_pitch ? b->lod_pitch : helio::kBatchChunk)));
-    HELIO_CK(b->chunk_counts.ensure((units + 1) * 4));
-    HELIO_CK(b->chunk_vis.ensure((units + 1) * 4));
-    HELIO_CK(b->vis_list.ensure(std::max<size_t>(1, units) * helio::kBatchChunk * sizeof(uint16_t)));
-    HELIO_CK(b->chunk_offs.ensure((units + 1) * 4));
-    HELIO_CK(b->seg_totals.ensure((size_t)b->grid * 4));
-    HELIO_CK(b->view_span_start.ensure((size_t)(n + 1) * 4));
-    HELIO_CK(b->spans.ensure((size_t)b->span_capacity * sizeof(helio::ActiveSpan)));
-    HELIO_CK(b->group_counts.ensure((size_t)(groups + 1) * 4));
-    HELIO_CK(b->group_offs.ensure((size_t)(groups + 1) * 4));
-    HELIO_CK(b->group_bits.ensure((size_t)(groups + 1) * helio::kWindowsPerWarp * 4));
-    if (b->cfg.flags & HELIO_BATCH_SPAN_VISIBILITY) HELIO_CK(b->span_vis.ensure((size_t)b->span_capacity * 8));
+    std::vector<size_t>& level_off = plan.level_off;
     // View table.
     for (uint32_t v = 0; v < n; ++v) {
         const helio_batch_view& in = views[v];
@@ -279,6 +315,55 @@ int32_t helio_batch_prepare(helio_batch* b, const helio_vg_scene* sc, uint32_t n
                              cudaMemcpyHostToDevice, s));
     HELIO_CK(cudaStreamSynchronize(s));
     b->prepared = true;
+    return HELIO_OK;
+}
+
+int32_t helio_batch_estimate_bytes(const helio_batch_config* cfg, const helio_vg_scene* sc, uint32_t n,
+                                   const helio_batch_view* views, uint64_t* bytes) {
+    HELIO_ARG(cfg && sc && views && bytes, "null pointer");
+    HELIO_ARG(sc->have, "scene not uploaded");
+    HELIO_ARG(n >= 1 && n <= HELIO_BATCH_MAX_VIEWS, "view count must be 1..128");
+    BatchPlan plan;
+    int32_t st;
+    if ((st = plan_batch(*cfg, sc, n, views, plan, nullptr))) return st;
+    uint64_t total = 0;
+    for (size_t x : plan.need) total += x;
+    *bytes = total;
+    return HELIO_OK;
+}
+
+int32_t helio_batch_growth_bytes(const helio_batch* b, const helio_batch_config* cfg, const helio_vg_scene* sc,
+                                 uint32_t n, const helio_batch_view* views, uint64_t* bytes) {
+    HELIO_ARG(b && cfg && sc && views && bytes, "null pointer");
+    HELIO_ARG(sc->have, "scene not uploaded");
+    HELIO_ARG(n >= 1 && n <= HELIO_BATCH_MAX_VIEWS, "view count must be 1..128");
+    BatchPlan plan;
+    int32_t st;
+    if ((st = plan_batch(*cfg, sc, n, views, plan, nullptr))) return st;
+    uint64_t grow = 0;
+    helio_batch* mb = const_cast<helio_batch*>(b);
+    for (int k = 0; k < kBatchBufs; ++k) {
+        const DevBuf& d = mb->buf(k);
+        if (!d.ptr || plan.need[k] > d.bytes) grow += plan.need[k] - (d.ptr ? d.bytes : 0);
+    }
+    *bytes = grow;
+    return HELIO_OK;
+}
+
+int32_t helio_batch_reconfigure(helio_batch* b, const helio_batch_config* cfg) {
+    HELIO_ARG(b && cfg, "null pointer");
+    HELIO_ARG(cfg->max_views >= 1 && cfg->max_views <= HELIO_BATCH_MAX_VIEWS, "max_views must be 1..128");
+    b->cfg = *cfg;
+    b->prepared = false;
+    return HELIO_OK;
+}
+
+int32_t helio_batch_device_bytes(const helio_batch* b, uint64_t* bytes) {
+    HELIO_ARG(b && bytes, "null pointer");
+    *bytes = b->views.bytes + b->cviews.bytes + b->lod.bytes + b->levels.bytes + b->out_indirect.bytes +
+             b->out_draws.bytes + b->clear.bytes + b->chunk_counts.bytes + b->chunk_vis.bytes + b->vis_list.bytes +
+             b->chunk_offs.bytes + b->seg_totals.bytes + b->view_span_start.bytes + b->spans.bytes +
+             b->group_counts.bytes + b->group_offs.bytes + b->group_bits.bytes + b->span_vis.bytes;
     return HELIO_OK;
 }
 

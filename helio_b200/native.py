@@ -138,7 +138,7 @@ class VgSceneInfo(C.Structure):
 
 
 class BatchConfig(C.Structure):
-    _fields_ = [("max_views", u32), ("flags", u32), ("max_spans", u64)]
+    _fields_ = [("max_views", u32), ("flags", u32), ("max_spans", u64), ("max_ctas", u32), ("reserved", u32)]
 
 
 class BatchView(C.Structure):
@@ -156,12 +156,38 @@ class BatchSpanList(C.Structure):
                 ("view_count", u32)]
 
 
+class ServeConfig(C.Structure):
+    _fields_ = [("hbm_budget_bytes", u64), ("slots", u32), ("max_views", u32), ("ctas_per_slot", u32),
+                ("max_requests_per_batch", u32), ("spans_per_view", u64)]
+
+
+class ServeRequest(C.Structure):
+    _fields_ = [("scene", u32), ("view_count", u32), ("views", C.POINTER(BatchView)), ("arrival_s", C.c_double),
+                ("tag", u64)]
+
+
+class ServeCompletion(C.Structure):
+    _fields_ = [("request", u64), ("tag", u64), ("status", i32), ("batch_requests", u32), ("view_count", u32),
+                ("reserved", u32), ("arrival_s", C.c_double), ("launch_s", C.c_double), ("done_s", C.c_double),
+                ("batch_device_ms", C.c_double)]
+
+
+class ServePending(C.Structure):
+    _fields_ = [("scene", u32), ("view_count", u32)]
+
+
+class ServeStats(C.Structure):
+    _fields_ = [("pending", u32), ("running", u32), ("ctas_per_slot", u32), ("reserved", u32), ("batches", u64),
+                ("bytes_in_use", u64), ("scene_bytes", u64)]
+
+
 HELIO_BATCH_MAX_VIEWS = 128
 HELIO_BATCH_SPAN_VISIBILITY = 1
 
 _SIZES = {GpuCameraUniforms: 368, GpuInstanceData: 144, GpuInstanceAabb: 32, GpuDrawCall: 20,
           DrawIndexedIndirectArgs: 20, GpuMeshletEntry: 64, GpuVgObject: 128, GpuVgDraw: 16, GpuVgWorkItem: 8,
-          InstanceCullData: 16, VgFrameData: 80}
+          InstanceCullData: 16, VgFrameData: 80, BatchConfig: 24, ServeConfig: 32, ServeRequest: 32,
+          ServeCompletion: 64, ServeStats: 40}
 for _t, _n in _SIZES.items():
     assert C.sizeof(_t) == _n, (_t.__name__, C.sizeof(_t), _n)
 
@@ -221,7 +247,21 @@ CULL_EXPORTS = {
     "helio_batch_get_spans": (i32, [vp, C.POINTER(BatchSpanList)]),
     "helio_batch_status": (i32, [vp, vp]),
     "helio_batch_get_phase_times": (i32, [vp, C.POINTER(C.c_double), u32, C.POINTER(u32), vp]),
+    "helio_batch_estimate_bytes": (i32, [C.POINTER(BatchConfig), vp, u32, C.POINTER(BatchView), C.POINTER(u64)]),
+    "helio_batch_device_bytes": (i32, [vp, C.POINTER(u64)]),
+    "helio_batch_growth_bytes": (i32, [vp, C.POINTER(BatchConfig), vp, u32, C.POINTER(BatchView), C.POINTER(u64)]),
+    "helio_batch_reconfigure": (i32, [vp, C.POINTER(BatchConfig)]),
     "helio_batch_destroy": (None, [vp]),
+    "helio_serve_create": (i32, [C.POINTER(ServeConfig), C.POINTER(vp)]),
+    "helio_serve_add_scene": (i32, [vp, vp, C.POINTER(u32)]),
+    "helio_serve_submit": (i32, [vp, C.POINTER(ServeRequest), C.POINTER(u64)]),
+    "helio_serve_pump": (i32, [vp, C.c_double, C.POINTER(u32)]),
+    "helio_serve_completions": (i32, [vp, C.POINTER(ServeCompletion), u32, C.POINTER(u32)]),
+    "helio_serve_outputs": (i32, [vp, u64, u32, C.POINTER(BatchViewOutputs)]),
+    "helio_serve_release": (i32, [vp, u64]),
+    "helio_serve_stats_get": (i32, [vp, C.POINTER(ServeStats)]),
+    "helio_serve_plan_batch": (i32, [C.POINTER(ServePending), u32, u32, u32, C.POINTER(u32), C.POINTER(u32)]),
+    "helio_serve_destroy": (None, [vp]),
 }
 
 _cull = None

@@ -240,6 +240,30 @@ class VgScene:
             self._h = None
 
 
+def batch_views(views: list):
+    """helio_batch_view array of view dicts (camera, device depth H x W float32, optional
+    lod_threshold_px, draw_capacity, alias_mip0)."""
+    arr = (N.BatchView * len(views))()
+    for i, v in enumerate(views):
+        d = v["depth"]
+        assert d.is_cuda and d.dtype == torch.float32 and d.stride(1) == 1
+        arr[i].camera = v["camera"]
+        arr[i].depth = d.data_ptr()
+        arr[i].depth_pitch = d.stride(0)
+        arr[i].height, arr[i].width = d.shape
+        arr[i].lod_error_threshold_px = v.get("lod_threshold_px", 0.0)
+        arr[i].draw_capacity = v.get("draw_capacity", 0)
+        arr[i].flags = N.HELIO_HIZ_ALIAS_MIP0 if v.get("alias_mip0", False) else 0
+    return arr
+
+
+def _batch_outputs(o: N.BatchViewOutputs) -> dict:
+    cap = max(o.capacity, 1)
+    return {"indirect": device_view(o.indirect, (cap, 5)), "draws": device_view(o.draws, (cap, 4)),
+            "counters": device_view(o.counters, (11,)), "lod": device_view(o.lod, (max(o.object_count, 1),), "|u1"),
+            "capacity": o.capacity, "pyramid": o.pyramid}
+
+
 class BatchedCull:
     """Every view of a batch culled against one VgScene in one cooperative launch
     (Hi-Z of each view, object LOD select for every (object, view), meshlet cull and
@@ -257,17 +281,7 @@ class BatchedCull:
     def prepare(self, scene: VgScene, views: list, stream=None) -> None:
         """views: sequence of dicts with camera (GpuCameraUniforms), depth (device
         float32 tensor H x W), optional lod_threshold_px, draw_capacity, alias_mip0."""
-        arr = (N.BatchView * len(views))()
-        for i, v in enumerate(views):
-            d = v["depth"]
-            assert d.is_cuda and d.dtype == torch.float32 and d.stride(1) == 1
-            arr[i].camera = v["camera"]
-            arr[i].depth = d.data_ptr()
-            arr[i].depth_pitch = d.stride(0)
-            arr[i].height, arr[i].width = d.shape
-            arr[i].lod_error_threshold_px = v.get("lod_threshold_px", 0.0)
-            arr[i].draw_capacity = v.get("draw_capacity", 0)
-            arr[i].flags = N.HELIO_HIZ_ALIAS_MIP0 if v.get("alias_mip0", False) else 0
+        arr = batch_views(views)
         self._keep = (scene, [v["depth"] for v in views])
         N.check(self._lib.helio_batch_prepare(self._h, scene._h, len(views), arr, _stream_ptr(stream)))
         self.view_count = len(views)
@@ -296,10 +310,7 @@ class BatchedCull:
     def view_outputs(self, v: int) -> dict:
         o = N.BatchViewOutputs()
         N.check(self._lib.helio_batch_get_view_outputs(self._h, v, C.byref(o)))
-        cap = max(o.capacity, 1)
-        return {"indirect": device_view(o.indirect, (cap, 5)), "draws": device_view(o.draws, (cap, 4)),
-                "counters": device_view(o.counters, (11,)), "lod": device_view(o.lod, (max(o.object_count, 1),), "|u1"),
-                "capacity": o.capacity, "pyramid": o.pyramid}
+        return _batch_outputs(o)
 
     def spans(self) -> dict:
         s = N.BatchSpanList()
@@ -315,6 +326,78 @@ class BatchedCull:
         if h:
             self._lib.helio_batch_destroy(h)
             self._h = None
+
+
+class ServeLoop:
+    """Continuous batching of cull requests over device-resident scenes (helio_serve):
+    submit requests as they arrive, pump with the current time, read completions and
+    their outputs, release them. Times are seconds on the caller's clock."""
+
+    def __init__(self, hbm_budget_bytes: int = 0, slots: int = 4, max_views: int = N.HELIO_BATCH_MAX_VIEWS,
+                 ctas_per_slot: int = 0, max_requests_per_batch: int = 0, spans_per_view: int = 0):
+        self._lib = N.cull_lib()
+        cfg = N.ServeConfig(hbm_budget_bytes, slots, max_views, ctas_per_slot, max_requests_per_batch, spans_per_view)
+        h = C.c_void_p()
+        N.check(self._lib.helio_serve_create(C.byref(cfg), C.byref(h)))
+        self._h = h
+        self._scenes = []
+        self._depths = {}  # request -> depth tensors kept alive until completion
+
+    def add_scene(self, scene: VgScene) -> int:
+        sid = N.u32(0)
+        N.check(self._lib.helio_serve_add_scene(self._h, scene._h, C.byref(sid)))
+        self._scenes.append(scene)
+        return sid.value
+
+    def submit(self, scene_id: int, views: list, arrival_s: float, tag: int = 0) -> int:
+        arr = batch_views(views)
+        rq = N.ServeRequest(scene_id, len(views), arr, arrival_s, tag)
+        rid = N.u64(0)
+        N.check(self._lib.helio_serve_submit(self._h, C.byref(rq), C.byref(rid)))
+        self._depths[rid.value] = [v["depth"] for v in views]
+        return rid.value
+
+    def pump(self, now_s: float) -> int:
+        ready = N.u32(0)
+        N.check(self._lib.helio_serve_pump(self._h, now_s, C.byref(ready)))
+        return ready.value
+
+    def completions(self, capacity: int = 256) -> list:
+        arr = (N.ServeCompletion * capacity)()
+        n = N.u32(0)
+        N.check(self._lib.helio_serve_completions(self._h, arr, capacity, C.byref(n)))
+        return [{f: getattr(arr[i], f) for f, _ in N.ServeCompletion._fields_ if f != "reserved"}
+                for i in range(n.value)]
+
+    def outputs(self, request: int, view: int) -> dict:
+        o = N.BatchViewOutputs()
+        N.check(self._lib.helio_serve_outputs(self._h, request, view, C.byref(o)))
+        return _batch_outputs(o)
+
+    def release(self, request: int) -> None:
+        N.check(self._lib.helio_serve_release(self._h, request))
+        self._depths.pop(request, None)
+
+    def stats(self) -> dict:
+        s = N.ServeStats()
+        N.check(self._lib.helio_serve_stats_get(self._h, C.byref(s)))
+        return {f: getattr(s, f) for f, _ in N.ServeStats._fields_ if f != "reserved"}
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            self._lib.helio_serve_destroy(h)
+            self._h = None
+
+
+def plan_batch(queue: list, max_views: int, max_requests: int = 0) -> list:
+    """The server's batch rule (helio_serve_plan_batch) on a queue of (scene, view_count)."""
+    lib = N.cull_lib()
+    arr = (N.ServePending * max(1, len(queue)))(*[N.ServePending(s, v) for s, v in queue])
+    chosen = (N.u32 * max(1, len(queue)))()
+    n = N.u32(0)
+    N.check(lib.helio_serve_plan_batch(arr, len(queue), max_views, max_requests, chosen, C.byref(n)))
+    return [chosen[i] for i in range(n.value)]
 
 
 class VirtualGeometryPass:

@@ -448,6 +448,9 @@ typedef struct helio_batch_config {
     uint32_t max_views; /* <= HELIO_BATCH_MAX_VIEWS */
     uint32_t flags;
     uint64_t max_spans; /* capacity of the active-span list; 0 = every view at LOD 0 */
+    uint32_t max_ctas;  /* CTAs of the cooperative launch; 0 = as many as fit on the device.
+                         * Fewer CTAs leave SMs free for batches launched on other streams. */
+    uint32_t reserved;
 } helio_batch_config;
 
 /* One view of a batch. */
@@ -509,7 +512,93 @@ int32_t helio_batch_get_phase_times(helio_batch* batch, double* us_out, uint32_t
 /* Synchronises `stream`; HELIO_ERR_TIMEOUT if a bounded grid barrier gave up,
  * HELIO_ERR_CAPACITY if the active spans exceeded max_spans (outputs incomplete). */
 int32_t helio_batch_status(helio_batch* batch, void* stream);
+/* Device bytes helio_batch_prepare would allocate for these views of `scene` (a
+ * batch grows its buffers and never shrinks them). For admission against a memory budget. */
+int32_t helio_batch_estimate_bytes(const helio_batch_config* config, const helio_vg_scene* scene, uint32_t view_count,
+                                   const helio_batch_view* views, uint64_t* bytes);
+/* Device bytes the batch holds now. */
+int32_t helio_batch_device_bytes(const helio_batch* batch, uint64_t* bytes);
+/* Device bytes helio_batch_prepare of these views under `config` would add to what the
+ * batch holds now (buffers that must grow, counted whole). */
+int32_t helio_batch_growth_bytes(const helio_batch* batch, const helio_batch_config* config,
+                                 const helio_vg_scene* scene, uint32_t view_count, const helio_batch_view* views,
+                                 uint64_t* bytes);
+/* Replaces the configuration the next helio_batch_prepare uses (view limit, span
+ * capacity, launch size); the batch must be prepared again before it executes. */
+int32_t helio_batch_reconfigure(helio_batch* batch, const helio_batch_config* config);
 void helio_batch_destroy(helio_batch* batch);
+
+/* ── Serving: continuous batching of cull requests (no counterpart in the reference) ──
+ * Requests name a device-resident scene and carry views; a pump admits them, as batch
+ * slots and the HBM budget allow, into batched launches that run concurrently on the
+ * slots' streams. The caller supplies the clock (seconds, any origin) so that latency
+ * is measured on the caller's timeline: completion time - arrival time. */
+typedef struct helio_serve_config {
+    uint64_t hbm_budget_bytes;       /* scenes + every slot's batch scratch; 0 = no limit */
+    uint32_t slots;                  /* batches in flight at once, each on its own stream: 1..16 */
+    uint32_t max_views;              /* views per batch: 1..HELIO_BATCH_MAX_VIEWS */
+    uint32_t ctas_per_slot;          /* CTAs of each launch; 0 = the device's co-resident grid / slots */
+    uint32_t max_requests_per_batch; /* 0 = no limit */
+    uint64_t spans_per_view;         /* active-span capacity per view; 0 = the scene's bound (never overflows) */
+} helio_serve_config;
+
+typedef struct helio_serve_request {
+    uint32_t scene;                 /* index from helio_serve_add_scene */
+    uint32_t view_count;            /* 1..max_views */
+    const helio_batch_view* views;  /* copied; the depth buffers must stay valid until completion */
+    double arrival_s;               /* arrival time on the caller's clock */
+    uint64_t tag;                   /* caller's value, echoed in the completion */
+} helio_serve_request;
+
+typedef struct helio_serve_completion {
+    uint64_t request;
+    uint64_t tag;
+    int32_t status;           /* HELIO_OK, the batch's status, or HELIO_ERR_CAPACITY if it can never fit */
+    uint32_t batch_requests;  /* requests that shared its launch */
+    uint32_t view_count;
+    uint32_t reserved;
+    double arrival_s, launch_s, done_s; /* caller's clock: arrival, launch, completion seen by a pump */
+    double batch_device_ms;             /* device time of the launch that carried it */
+} helio_serve_completion;
+
+typedef struct helio_serve_pending {
+    uint32_t scene;
+    uint32_t view_count;
+} helio_serve_pending;
+
+typedef struct helio_serve_stats {
+    uint32_t pending;
+    uint32_t running;
+    uint32_t ctas_per_slot;
+    uint32_t reserved;
+    uint64_t batches;
+    uint64_t bytes_in_use;   /* scenes + slot scratch */
+    uint64_t scene_bytes;
+} helio_serve_stats;
+
+typedef struct helio_serve helio_serve;
+int32_t helio_serve_create(const helio_serve_config* config, helio_serve** out);
+/* Registers an uploaded scene (it must outlive the server); its bytes count against the budget. */
+int32_t helio_serve_add_scene(helio_serve* server, const helio_vg_scene* scene, uint32_t* scene_id);
+int32_t helio_serve_submit(helio_serve* server, const helio_serve_request* request, uint64_t* request_id);
+/* One scheduling step at time now_s: retires finished launches (no blocking), then
+ * admits and launches batches while a slot and memory are free. *ready = completions
+ * waiting to be read. */
+int32_t helio_serve_pump(helio_serve* server, double now_s, uint32_t* ready);
+/* Moves up to `capacity` completions out, oldest first. */
+int32_t helio_serve_completions(helio_serve* server, helio_serve_completion* out, uint32_t capacity, uint32_t* count);
+/* Outputs of view `view` of a completed request; valid until helio_serve_release. */
+int32_t helio_serve_outputs(const helio_serve* server, uint64_t request_id, uint32_t view,
+                            helio_batch_view_outputs* out);
+/* Frees a completed request's outputs; a slot is reused once all its requests are released. */
+int32_t helio_serve_release(helio_serve* server, uint64_t request_id);
+int32_t helio_serve_stats_get(const helio_serve* server, helio_serve_stats* out);
+/* The scheduler's batch rule, on the pending queue (oldest first): the oldest request,
+ * then later requests of the same scene, in arrival order, that keep the batch within
+ * max_views (and max_requests, 0 = no limit). Writes their queue positions. */
+int32_t helio_serve_plan_batch(const helio_serve_pending* queue, uint32_t n, uint32_t max_views,
+                               uint32_t max_requests, uint32_t* chosen, uint32_t* count);
+void helio_serve_destroy(helio_serve* server);
 
 #ifdef __cplusplus
 } /* extern "C" */
