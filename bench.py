@@ -15,6 +15,12 @@ Workloads
                       85 plain per-view pipelines are timed beside it (same inputs).
   plain2              100,000 instances x 100 LOD0 meshlets (10M), one 3840x2160 view.
   plain1 / plain0     1M meshlets at 1920x1080 / 262,144 meshlets at 1024x1024.
+  serve4              the serving loop: 8 device-resident scenes (10k..2M instances x 100
+                      LOD0 meshlets), a seeded Poisson stream of requests at 2,000/s, each
+                      naming a scene and 1..85 views of the 85-view mix, admitted against a
+                      40 GB HBM budget and batched continuously (helio_serve); reports
+                      p50/p99 latency beside meshlets/s, and the same stream served one
+                      request at a time through the plain single-view passes.
 
 `value` is measured with inputs resident in HBM, the step replayed as a CUDA graph,
 CUDA events on the launching stream, L2 flushed between timed steps. `e2e` runs the
@@ -52,11 +58,14 @@ def parse_args():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
-    ap.add_argument("--workload", default="batched3", choices=["batched3", "plain2", "plain1", "plain0"])
+    ap.add_argument("--workload", default="batched3", choices=["batched3", "plain2", "plain1", "plain0", "serve4"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="batched3: skip the per-view plain comparison")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="bound of the CPU baseline sample")
+    ap.add_argument("--requests", type=int, default=1000, help="serve4: timed requests (after --warmup x 20)")
+    ap.add_argument("--rate", type=float, default=2000.0, help="serve4: arrival rate (requests/s)")
+    ap.add_argument("--slots", type=int, default=2, help="serve4: batches in flight")
     return ap.parse_args()
 
 
@@ -515,6 +524,151 @@ def run_ours(args, rank, world, local_rank):
     return line
 
 
+# ── serve4: continuous batching of a request stream ───────────────────────────
+
+SERVE_BUDGET = 40 * (1 << 30)
+SERVE_SPANS_PER_VIEW = 1 << 19
+
+
+def run_serve(args, rank, world, local_rank):
+    import torch
+    from helio_b200 import dist as D
+    from helio_b200 import native as N
+    from helio_b200 import scene as S
+    from helio_b200.passes import HiZBuildPass, ServeLoop, VgScene, VirtualGeometryPass, camera_bytes
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    lib = N.cull_lib()
+    scenes = S.serving_scenes()
+    pool = S.multiview_set(S.SEED_BASE + 4)
+    depths = [torch.from_numpy(v.depth).to(dev) for v in pool]
+    vgs = []
+    for sc in scenes:
+        vs = VgScene()
+        vs.upload(S.frame_data(sc))
+        vgs.append(vs)
+    loop = ServeLoop(hbm_budget_bytes=SERVE_BUDGET, slots=args.slots, max_views=N.HELIO_BATCH_MAX_VIEWS,
+                     spans_per_view=SERVE_SPANS_PER_VIEW)
+    ids = [loop.add_scene(vs) for vs in vgs]
+    warm = max(3, args.warmup) * 20
+    total = warm + args.requests
+    # Replicas: rank r serves every world-th request of the same stream (weak scaling).
+    reqs = S.serving_requests(total * world, args.rate * world)[rank::world]
+    specs = [[{"camera": pool[p].camera, "depth": depths[p], "alias_mip0": True,
+               "lod_threshold_px": pool[p].lod_threshold_px} for p in r.views] for r in reqs]
+    units = [scenes[r.scene].lod0_total * len(r.views) for r in reqs]
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    clocks = Clocks(local_rank)
+    done, batches0, i = {}, None, 0
+    launches0 = lib.helio_kernel_launch_count()
+    t0 = time.perf_counter()
+    clocks.start()
+    offset = reqs[0].arrival_s
+    while len(done) < len(reqs):
+        now = time.perf_counter() - t0
+        while i < len(reqs) and reqs[i].arrival_s - offset <= now:
+            loop.submit(ids[reqs[i].scene], specs[i], reqs[i].arrival_s - offset, tag=i)
+            i += 1
+            if i == warm:
+                batches0 = loop.stats()["batches"]
+                launches0 = lib.helio_kernel_launch_count()
+        loop.pump(now)
+        for c in loop.completions():
+            done[c["tag"]] = c
+            loop.release(c["request"])
+        if now > 600:
+            raise RuntimeError("serving run exceeded 600 s")
+    clk = clocks.stop()
+    timed = [done[k] for k in range(warm, len(reqs))]
+    failed = sum(c["status"] != 0 for c in timed)
+    lat = [1e3 * (c["done_s"] - c["arrival_s"]) for c in timed]
+    span_s = max(c["done_s"] for c in timed) - min(c["arrival_s"] for c in timed)
+    span_s = D.max_over_ranks(span_s * 1e3, dev) / 1e3
+    served = sum(units[k] for k in range(warm, len(reqs)) if done[k]["status"] == 0)
+    value = D.sum_over_ranks(float(served), dev) / span_s
+    batches = loop.stats()["batches"] - (batches0 or 0)
+    launches = lib.helio_kernel_launch_count() - launches0
+
+    # The same timed stream served one request at a time through the plain single-view
+    # passes: per-request device time (CUDA events), then the FIFO queue over the same
+    # arrivals (start = max(arrival, previous finish)).
+    hz = [HiZBuildPass(v.width, v.height, alias_mip0=True) for v in pool]
+    for h, d in zip(hz, depths):
+        h.prepare(d)
+    cams = [torch.from_numpy(camera_bytes(v.camera)).to(dev) for v in pool]
+    plain_ms = {}
+    budget_s, t_plain = 60.0, time.perf_counter()
+    for sid in ([] if args.no_plain else range(len(scenes))):
+        vg = VirtualGeometryPass(pool[0].width, pool[0].height)
+        vg.prepare(S.frame_data(scenes[sid]))
+        mine = [k for k in range(warm, len(reqs)) if reqs[k].scene == sid]
+        for k in mine:
+            if time.perf_counter() - t_plain > budget_s:
+                break
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            for p in reqs[k].views:
+                hz[p].execute()
+                vg.on_resize(pool[p].width, pool[p].height)
+                vg.execute(cams[p], hz[p].publish())
+            b.record()
+            b.synchronize()
+            plain_ms[k] = a.elapsed_time(b)
+        del vg
+    measured = sorted(plain_ms)
+    plain = None
+    if measured:
+        # Requests not timed (time bound) take the mean service time per (scene, view).
+        per_view = {}
+        for k in measured:
+            per_view.setdefault(reqs[k].scene, []).append(plain_ms[k] / len(reqs[k].views))
+        fin, plat = 0.0, []
+        for k in range(warm, len(reqs)):
+            svc = plain_ms.get(k)
+            if svc is None:
+                pv = per_view.get(reqs[k].scene) or [statistics.mean(plain_ms.values())]
+                svc = statistics.mean(pv) * len(reqs[k].views)
+            arr = 1e3 * (reqs[k].arrival_s - offset)
+            fin = max(arr, fin) + svc
+            plat.append(fin - arr)
+        first = 1e3 * (reqs[warm].arrival_s - offset)
+        plain = {"value": sum(units[warm:]) / ((fin - first) / 1e3), "unit": "meshlets/s",
+                 "latency_ms": {"p50": pct(plat, 0.5), "p99": pct(plat, 0.99)},
+                 "requests_timed_on_device": len(measured), "requests": len(reqs) - warm,
+                 "method": "per-request device time of the plain passes (CUDA events), FIFO queue over the same "
+                           "arrivals; requests beyond the 60 s timing bound use their scene's mean time per view"}
+
+    cpu = None
+    if rank == 0 and world == 1:
+        small = min(range(len(scenes)), key=lambda k: len(scenes[k].objects))
+        cpu = cpu_baseline(S.Workload(4, scenes[small], pool), min(args.cpu_seconds, 10.0))
+        cpu["sample"] = f"scene {small} ({len(scenes[small].objects)} instances): " + cpu["sample"]
+    st = loop.stats()
+    return {
+        "metric": "meshlets culled/s", "value": value, "unit": "meshlets/s", "n_gpus": world,
+        "steps": len(timed), "warmup": warm, "ms_per_step": statistics.mean(lat), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator)",
+        "config": {"workload": "serve4: 8 scenes of " + "/".join(str(len(s.objects)) for s in scenes) +
+                               " instances x 100 LOD0 meshlets; Poisson requests at "
+                               f"{args.rate:g}/s per GPU, 1..85 views each from the 85-view mix; "
+                               f"{args.slots} slots, {SERVE_BUDGET >> 30} GB HBM budget",
+                   "requests": len(timed), "failed": failed, "batches": batches,
+                   "ctas_per_slot": st["ctas_per_slot"], "peak_bytes_in_use": st["bytes_in_use"],
+                   "timing": "host clock from each request's scheduled arrival to the pump that saw its "
+                             "batch's completion event; value = served (view, LOD0 meshlet) pairs / (last "
+                             "completion - first arrival)",
+                   "l2": "not flushed: the request stream itself exceeds L2 (scenes of up to 2M instances)",
+                   "parallelism": f"replica x{world}" if world > 1 else "single GPU"},
+        "latency_ms": {"p50": pct(lat, 0.5), "p99": pct(lat, 0.99), "mean": statistics.mean(lat)},
+        "plain_per_request": plain, "cpu_baseline": cpu, "e2e": None, "roofline": None,
+        "gpu_launches": int(launches), "clocks": clk,
+        "batch_requests_mean": statistics.mean(c["batch_requests"] for c in timed),
+    }
+
+
 # ── CPU baseline / reference arm (the oracle) ────────────────────────────────
 
 def oracle_views(wl, views, threads: int) -> int:
@@ -556,8 +710,14 @@ def cpu_baseline(wl, seconds: float) -> dict:
 def run_reference(args):
     from helio_b200 import scene as S
 
-    cfg = {"batched3": 3, "plain2": 2, "plain1": 1, "plain0": 0}[args.workload]
-    wl = S.config(cfg)
+    if args.workload == "serve4":
+        # The reference has no serving loop; its per-view cull, restated, on the smallest
+        # serving scene and the 85-view mix.
+        scenes = S.serving_scenes()
+        small = min(scenes, key=lambda sc: len(sc.objects))
+        wl = S.Workload(4, small, S.multiview_set(S.SEED_BASE + 4))
+    else:
+        wl = S.config({"batched3": 3, "plain2": 2, "plain1": 1, "plain0": 0}[args.workload])
     threads = max(1, os.cpu_count() or 1)
     for k in range(args.warmup):
         oracle_views(wl, sample_views(wl, k), threads)
@@ -597,7 +757,8 @@ def main():
         from helio_b200 import dist as D
 
         D.init("nccl", timeout_s=120)
-    line = run_ours(args, rank, world, local_rank)
+    line = run_serve(args, rank, world, local_rank) if args.workload == "serve4" else \
+        run_ours(args, rank, world, local_rank)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

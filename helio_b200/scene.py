@@ -220,6 +220,38 @@ def config(config_id: int, scale: float = 1.0, with_depth: bool = True, threads:
     raise ValueError(f"unknown config {config_id}")
 
 
+@dataclass
+class ServeRequestSpec:
+    arrival_s: float
+    scene: int
+    views: list  # indices into the view pool
+
+
+def serving_scenes(scale: float = 1.0, threads: int | None = None) -> list:
+    """The serving workload's 8 scenes: instance counts log-uniform in [10k, 2M] (times
+    `scale`), 100 LOD0 meshlets each, configs-1 distributions (uniform in a 200 m cube,
+    log-uniform LOD errors); the instances draw their meshes from a library of 256."""
+    seed = SEED_BASE + 4
+    rng = _Split(seed)
+    counts = [max(1, int(round(math.exp(rng.u(math.log(1e4), math.log(2e6))) * scale))) for _ in range(8)]
+    return [make_scene(seed + 1 + k, n, 100, 4, 0, 100.0, lod_error_mode=1, mesh_library=256, threads=threads)
+            for k, n in enumerate(counts)]
+
+
+def serving_requests(n: int, rate_hz: float = 2000.0, n_scenes: int = 8, pool: int = 85, max_views: int = 85,
+                     seed: int = SEED_BASE + 4) -> list:
+    """A seeded Poisson request stream: exponential inter-arrival times at `rate_hz`;
+    each request names a scene uniformly and carries 1..max_views views drawn uniformly
+    (with replacement) from a pool of `pool` views, so the view sizes follow the pool's mix."""
+    g = np.random.default_rng(seed)
+    t = np.cumsum(g.exponential(1.0 / rate_hz, size=n))
+    out = []
+    for i in range(n):
+        k = int(g.integers(1, max_views + 1))
+        out.append(ServeRequestSpec(float(t[i]), int(g.integers(n_scenes)), [int(x) for x in g.integers(pool, size=k)]))
+    return out
+
+
 def work_items_for(objects) -> list:
     """64-meshlet work spans of (object_index, max_meshlet_count) pairs, in order
     (crates/helio/src/scene/virtual_geometry/rebuild.rs:45-58): one span per started
