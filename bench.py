@@ -530,6 +530,33 @@ SERVE_BUDGET = 40 * (1 << 30)
 SERVE_SPANS_PER_VIEW = 1 << 19
 
 
+def serve_stream(loop, lib, reqs, specs, ids, warm):
+    """Replays a request stream in real time: submits each request when the host clock
+    reaches its arrival, pumps the server, and records completions (releasing their
+    outputs). Returns (completions by request index, batches and kernel launches after
+    the first `warm` requests)."""
+    done, i = {}, 0
+    batches0 = loop.stats()["batches"]
+    launches0 = lib.helio_kernel_launch_count()
+    t0 = time.perf_counter()
+    offset = reqs[0].arrival_s
+    while len(done) < len(reqs):
+        now = time.perf_counter() - t0
+        while i < len(reqs) and reqs[i].arrival_s - offset <= now:
+            loop.submit(ids[reqs[i].scene], specs[i], reqs[i].arrival_s - offset, tag=i)
+            i += 1
+            if i == warm:
+                batches0 = loop.stats()["batches"]
+                launches0 = lib.helio_kernel_launch_count()
+        loop.pump(now)
+        for c in loop.completions():
+            done[c["tag"]] = c
+            loop.release(c["request"])
+        if now > 600:
+            raise RuntimeError("serving run exceeded 600 s")
+    return done, loop.stats()["batches"] - batches0, lib.helio_kernel_launch_count() - launches0
+
+
 def run_serve(args, rank, world, local_rank):
     import torch
     from helio_b200 import dist as D
@@ -562,26 +589,10 @@ def run_serve(args, rank, world, local_rank):
     if world > 1:
         torch.distributed.barrier()
     clocks = Clocks(local_rank)
-    done, batches0, i = {}, None, 0
-    launches0 = lib.helio_kernel_launch_count()
-    t0 = time.perf_counter()
     clocks.start()
-    offset = reqs[0].arrival_s
-    while len(done) < len(reqs):
-        now = time.perf_counter() - t0
-        while i < len(reqs) and reqs[i].arrival_s - offset <= now:
-            loop.submit(ids[reqs[i].scene], specs[i], reqs[i].arrival_s - offset, tag=i)
-            i += 1
-            if i == warm:
-                batches0 = loop.stats()["batches"]
-                launches0 = lib.helio_kernel_launch_count()
-        loop.pump(now)
-        for c in loop.completions():
-            done[c["tag"]] = c
-            loop.release(c["request"])
-        if now > 600:
-            raise RuntimeError("serving run exceeded 600 s")
+    done, batches, launches = serve_stream(loop, lib, reqs, specs, ids, warm)
     clk = clocks.stop()
+    offset = reqs[0].arrival_s
     timed = [done[k] for k in range(warm, len(reqs))]
     failed = sum(c["status"] != 0 for c in timed)
     lat = [1e3 * (c["done_s"] - c["arrival_s"]) for c in timed]
@@ -589,8 +600,18 @@ def run_serve(args, rank, world, local_rank):
     span_s = D.max_over_ranks(span_s * 1e3, dev) / 1e3
     served = sum(units[k] for k in range(warm, len(reqs)) if done[k]["status"] == 0)
     value = D.sum_over_ranks(float(served), dev) / span_s
-    batches = loop.stats()["batches"] - (batches0 or 0)
-    launches = lib.helio_kernel_launch_count() - launches0
+    capacity_rps = (len(timed) - failed) / span_s
+
+    # Latency below saturation: the same kind of stream at half the rate just served.
+    low_rate = 0.5 * capacity_rps
+    low_n = max(20, min(200, int(3.0 * low_rate)))
+    lreqs = S.serving_requests(low_n + 20, low_rate, seed=S.SEED_BASE + 44)
+    lspecs = [[{"camera": pool[p].camera, "depth": depths[p], "alias_mip0": True,
+                "lod_threshold_px": pool[p].lod_threshold_px} for p in r.views] for r in lreqs]
+    ldone, _, _ = serve_stream(loop, lib, lreqs, lspecs, ids, 20)
+    llat = [1e3 * (ldone[k]["done_s"] - ldone[k]["arrival_s"]) for k in range(20, len(lreqs))]
+    low_load = {"rate_per_s": low_rate, "requests": len(llat), "latency_ms": {"p50": pct(llat, 0.5),
+                "p99": pct(llat, 0.99)}, "note": "half of the request rate served at saturation"}
 
     # The same timed stream served one request at a time through the plain single-view
     # passes: per-request device time (CUDA events), then the FIFO queue over the same
@@ -663,6 +684,7 @@ def run_serve(args, rank, world, local_rank):
                    "l2": "not flushed: the request stream itself exceeds L2 (scenes of up to 2M instances)",
                    "parallelism": f"replica x{world}" if world > 1 else "single GPU"},
         "latency_ms": {"p50": pct(lat, 0.5), "p99": pct(lat, 0.99), "mean": statistics.mean(lat)},
+        "capacity_requests_per_s": capacity_rps, "low_load": low_load,
         "plain_per_request": plain, "cpu_baseline": cpu, "e2e": None, "roofline": None,
         "gpu_launches": int(launches), "clocks": clk,
         "batch_requests_mean": statistics.mean(c["batch_requests"] for c in timed),
