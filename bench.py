@@ -266,6 +266,8 @@ class BatchedWorkload:
                                           "lod_threshold_px": v.lod_threshold_px}
                                          for v, d in zip(self.views, self.depths)])
         torch.cuda.synchronize()
+        # Launch shape chosen by the autotuner on this device, before anything is timed.
+        self.tuning = self.batch.autotune(repeats=3)
         self.plain = None
         if with_plain:
             # The same 85 views through the plain single-view passes, one after another.
@@ -481,6 +483,7 @@ def run_ours(args, rank, world, local_rank):
         torch.cuda._sleep(SLEEP_CYCLES)
         wl.step()
         extra["phases_us"] = wl.batch.phase_times()
+        extra["autotune"] = wl.tuning
     if getattr(wl, "plain", None) is not None:
         plain_ms, plain_graphed = timer.run(wl.plain, max(3, args.steps // 4), args.warmup)
         pm = D.max_over_ranks(sum(plain_ms), dev) / len(plain_ms)

@@ -880,7 +880,8 @@ __global__ void __launch_bounds__(kBatchThreads, 3) batch_kernel(BatchParams P) 
         // kinds of work and CTAs that draw cheap units draw more of them. Thread 0
         // claims the next unit while the block works on the current one. Unit u is a
         // select unit iff floor((u + 1) S / U) > floor(u S / U).
-        const uint32_t vgroups = (P.view_count + kSelectMaxViews - 1) / kSelectMaxViews;
+        const uint32_t group_cap = min(max(P.select_views, 1u), kSelectMaxViews);
+        const uint32_t vgroups = (P.view_count + group_cap - 1) / group_cap;
         const uint32_t gsize = (P.view_count + vgroups - 1) / vgroups;  // balanced view groups
         const uint32_t sel_units = P.object_chunks * vgroups;
         const uint32_t units = P.hiz_tiles + sel_units;

@@ -49,6 +49,7 @@ struct BatchParams {
     uint8_t* lod;             // [view_count * lod_pitch]: LOD + 1 per (view, object), 0 = culled
     uint32_t lod_pitch;       // bytes per view row: object_count rounded up to kBatchChunk
     uint32_t view_count;
+    uint32_t select_views;    // views per select unit, 1..32
     uint32_t object_chunks;   // ceil(object_count / kBatchChunk)
     uint32_t hiz_tiles;       // Hi-Z tiles of all views
     uint32_t* barrier;        // [2] arrival count (zero before the launch), generation

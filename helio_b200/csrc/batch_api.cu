@@ -318,6 +318,69 @@ int32_t helio_batch_prepare(helio_batch* b, const helio_vg_scene* sc, uint32_t n
     return HELIO_OK;
 }
 
+int32_t helio_batch_autotune(helio_batch* b, uint32_t repeats, helio_batch_tuning* out, void* stream) {
+    HELIO_ARG(b && out, "null pointer");
+    if (!b->prepared) return helio_fail(HELIO_ERR_RESOURCE, "autotune before prepare");
+    cudaStream_t s = as_stream(stream);
+    repeats = repeats ? repeats : 3u;
+    int dev = 0, sms = 0;
+    HELIO_CK(cudaGetDevice(&dev));
+    HELIO_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    cudaEvent_t e0, e1;
+    HELIO_CK(cudaEventCreate(&e0));
+    HELIO_CK(cudaEventCreate(&e1));
+    const helio_batch_config saved = b->cfg;
+    auto time_cfg = [&](uint32_t views, uint32_t ctas, double& ms) -> int32_t {
+        b->cfg.select_views = views;
+        b->cfg.max_ctas = ctas;
+        std::vector<float> t(repeats);
+        int32_t st = helio_batch_execute(b, s);  // warm-up
+        if (st) return st;
+        for (uint32_t r = 0; r < repeats; ++r) {
+            HELIO_CK(cudaEventRecord(e0, s));
+            if ((st = helio_batch_execute(b, s))) return st;
+            HELIO_CK(cudaEventRecord(e1, s));
+            HELIO_CK(cudaEventSynchronize(e1));
+            HELIO_CK(cudaEventElapsedTime(&t[r], e0, e1));
+        }
+        std::sort(t.begin(), t.end());
+        ms = t[repeats / 2];
+        return HELIO_OK;
+    };
+    double base = 0.0, best = 1e30;
+    uint32_t best_v = 32, best_c = b->grid, n = 0;
+    int32_t st = time_cfg(saved.select_views, saved.max_ctas, base);
+    for (uint32_t v = 8; !st && v <= 32; v += 8) {
+        for (uint32_t k = 1; !st && k <= 3; ++k) {
+            const uint32_t ctas = std::min<uint32_t>((uint32_t)sms * k, b->grid);
+            double ms = 0.0;
+            if ((st = time_cfg(v, ctas, ms))) break;
+            ++n;
+            if (ms < best) {
+                best = ms;
+                best_v = v;
+                best_c = ctas;
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    b->cfg = saved;
+    if (st) return st;
+    b->cfg.select_views = best_v;
+    b->cfg.max_ctas = best_c;
+    // Leave the outputs of the chosen configuration in the buffers.
+    if ((st = helio_batch_execute(b, s))) return st;
+    HELIO_CK(cudaStreamSynchronize(s));
+    std::memset(out, 0, sizeof(*out));
+    out->select_views = best_v;
+    out->ctas = best_c;
+    out->candidates = n;
+    out->best_ms = best;
+    out->default_ms = base;
+    return HELIO_OK;
+}
+
 int32_t helio_batch_estimate_bytes(const helio_batch_config* cfg, const helio_vg_scene* sc, uint32_t n,
                                    const helio_batch_view* views, uint64_t* bytes) {
     HELIO_ARG(cfg && sc && views && bytes, "null pointer");
@@ -393,6 +456,7 @@ int32_t helio_batch_execute(helio_batch* b, void* stream) {
     P.lod_pitch = b->lod_pitch;
     P.scene_bounds = b->scene->bounds.as<uint32_t>();
     P.view_count = b->view_count;
+    P.select_views = b->cfg.select_views ? b->cfg.select_views : 32u;
     P.object_chunks = b->object_chunks;
     P.hiz_tiles = b->hiz_tiles;
     P.barrier = b->barrier();
@@ -411,7 +475,8 @@ int32_t helio_batch_execute(helio_batch* b, void* stream) {
     P.group_bits = b->group_bits.as<uint32_t>();
     P.span_vis = (b->cfg.flags & HELIO_BATCH_SPAN_VISIBILITY) ? b->span_vis.as<uint32_t>() : nullptr;
     P.phase_ns = b->stamps();
-    HELIO_CK(helio::launch_batch(P, b->grid, s));
+    const uint32_t grid = (b->cfg.max_ctas && b->cfg.max_ctas < b->grid) ? b->cfg.max_ctas : b->grid;
+    HELIO_CK(helio::launch_batch(P, grid, s));
     return HELIO_OK;
 }
 

@@ -138,7 +138,12 @@ class VgSceneInfo(C.Structure):
 
 
 class BatchConfig(C.Structure):
-    _fields_ = [("max_views", u32), ("flags", u32), ("max_spans", u64), ("max_ctas", u32), ("reserved", u32)]
+    _fields_ = [("max_views", u32), ("flags", u32), ("max_spans", u64), ("max_ctas", u32), ("select_views", u32)]
+
+
+class BatchTuning(C.Structure):
+    _fields_ = [("select_views", u32), ("ctas", u32), ("candidates", u32), ("reserved", u32),
+                ("best_ms", C.c_double), ("default_ms", C.c_double)]
 
 
 class BatchView(C.Structure):
@@ -251,6 +256,7 @@ CULL_EXPORTS = {
     "helio_batch_device_bytes": (i32, [vp, C.POINTER(u64)]),
     "helio_batch_growth_bytes": (i32, [vp, C.POINTER(BatchConfig), vp, u32, C.POINTER(BatchView), C.POINTER(u64)]),
     "helio_batch_reconfigure": (i32, [vp, C.POINTER(BatchConfig)]),
+    "helio_batch_autotune": (i32, [vp, u32, C.POINTER(BatchTuning), vp]),
     "helio_batch_destroy": (None, [vp]),
     "helio_serve_create": (i32, [C.POINTER(ServeConfig), C.POINTER(vp)]),
     "helio_serve_add_scene": (i32, [vp, vp, C.POINTER(u32)]),

@@ -286,6 +286,14 @@ class BatchedCull:
         N.check(self._lib.helio_batch_prepare(self._h, scene._h, len(views), arr, _stream_ptr(stream)))
         self.view_count = len(views)
 
+    def autotune(self, repeats: int = 3, stream=None) -> dict:
+        """Times the prepared batch under every launch-shape candidate (views per
+        select unit x CTAs per SM) and keeps the fastest (helio_batch_autotune)."""
+        t = N.BatchTuning()
+        N.check(self._lib.helio_batch_autotune(self._h, repeats, C.byref(t), _stream_ptr(stream)))
+        return {"select_views": t.select_views, "ctas": t.ctas, "candidates": t.candidates, "best_ms": t.best_ms,
+                "default_ms": t.default_ms}
+
     def set_cameras(self, cameras: list, stream=None) -> None:
         arr = (N.GpuCameraUniforms * len(cameras))(*cameras)
         N.check(self._lib.helio_batch_set_cameras(self._h, len(cameras), arr, _stream_ptr(stream)))

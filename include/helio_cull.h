@@ -448,9 +448,9 @@ typedef struct helio_batch_config {
     uint32_t max_views; /* <= HELIO_BATCH_MAX_VIEWS */
     uint32_t flags;
     uint64_t max_spans; /* capacity of the active-span list; 0 = every view at LOD 0 */
-    uint32_t max_ctas;  /* CTAs of the cooperative launch; 0 = as many as fit on the device.
-                         * Fewer CTAs leave SMs free for batches launched on other streams. */
-    uint32_t reserved;
+    uint32_t max_ctas;     /* CTAs of the cooperative launch; 0 = as many as fit on the device.
+                            * Fewer CTAs leave SMs free for batches launched on other streams. */
+    uint32_t select_views; /* views tested per object load in the select (1..32); 0 = 32 */
 } helio_batch_config;
 
 /* One view of a batch. */
@@ -516,6 +516,19 @@ int32_t helio_batch_status(helio_batch* batch, void* stream);
  * batch grows its buffers and never shrinks them). For admission against a memory budget. */
 int32_t helio_batch_estimate_bytes(const helio_batch_config* config, const helio_vg_scene* scene, uint32_t view_count,
                                    const helio_batch_view* views, uint64_t* bytes);
+/* Launch-shape autotuner: times helio_batch_execute of the prepared views (on
+ * `stream`, `repeats` runs per candidate, median) for every candidate of select_views
+ * {8, 16, 24, 32} x CTAs {1, 2, 3} per SM (at most the prepared grid), keeps the fastest
+ * in the batch's configuration and reports it. Synchronises `stream`. */
+typedef struct helio_batch_tuning {
+    uint32_t select_views;
+    uint32_t ctas;
+    uint32_t candidates;
+    uint32_t reserved;
+    double best_ms;
+    double default_ms; /* the configuration before tuning */
+} helio_batch_tuning;
+int32_t helio_batch_autotune(helio_batch* batch, uint32_t repeats, helio_batch_tuning* out, void* stream);
 /* Device bytes the batch holds now. */
 int32_t helio_batch_device_bytes(const helio_batch* batch, uint64_t* bytes);
 /* Device bytes helio_batch_prepare of these views under `config` would add to what the

@@ -143,3 +143,20 @@ def test_batch_benchmark_scene(cuda):
     got = gather(b, 0, len(sc.objects))
     assert got["counters"][0] == 64 * 1024 and got["counters"][1] == 0
     np.testing.assert_array_equal(got["indirect"][:, 4], np.arange(64 * 1024))
+
+
+def test_autotune_keeps_results(cuda):
+    """The launch-shape autotuner only changes how work is split, never the results."""
+    from helio_b200 import scene as S
+
+    w = S.config(3, scale=0.05)
+    views = w.views[:24]
+    b, vs, _ = run_batch(w.scene, views, span_visibility=False)
+    before = [gather(b, i, len(w.scene.objects)) for i in range(len(views))]
+    t = b.autotune(repeats=2)
+    assert t["candidates"] == 12 and 8 <= t["select_views"] <= 32 and t["ctas"] >= 1
+    assert t["best_ms"] <= t["default_ms"] * 1.5
+    after = [gather(b, i, len(w.scene.objects)) for i in range(len(views))]
+    for x, y in zip(before, after):
+        for k in ("counters", "indirect", "draws", "lod"):
+            np.testing.assert_array_equal(x[k], y[k])
