@@ -24,6 +24,37 @@ __device__ __forceinline__ void load_view(const CullView* src, CullView& dst, in
     for (int k = tid; k < (int)(sizeof(CullView) / 16); k += nthreads) d[k] = __ldg(s + k);
 }
 
+__device__ __forceinline__ float rsqrt_approx(float x) {
+    float r;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+// The cone test's decision dot(cta / |cta|, a / |a|) >= cutoff (vg_cull.wgsl:172-180),
+// bit-for-bit. The reference value E normalises both vectors with a correctly rounded
+// square root and three divisions each, then takes the dot product; it lies within
+// about 10 ulp(1) of the real cosine R (both vectors are unit length after
+// normalisation, so every term is at most 1). D = fma-dot(cta, a) * rsqrt.approx(|cta|^2)
+// * rsqrt.approx(|a|^2) lies within about 16 ulp(1) of R: 3 roundings in the dot
+// (relative to sum |cta_i a_i| <= |cta||a|), at most 2^-22.9 relative error in each
+// rsqrt.approx (PTX ISA) plus the squared norms' own rounding, and two products. So
+// |D - E| < 2^-19, and D outside cutoff +- 2^-16 decides the comparison; everything
+// else (and squared norms outside [1e-30, 1e30], non-finite values) takes the
+// reference's own sequence.
+__device__ __forceinline__ bool cone_rejects(F3 a, F3 cta, float ads, float cutoff) {
+    const float da = dot3(a, a);
+    if (da >= 1.0e-30f && da <= 1.0e30f && ads <= 1.0e30f) {
+        const float t = fmaf(cta.z, a.z, fmaf(cta.y, a.y, cta.x * a.x));
+        const float d = t * rsqrt_approx(ads) * rsqrt_approx(da);
+        if (isfinite(d)) {
+            if (d >= cutoff + 0x1p-16f) return true;
+            if (d < cutoff - 0x1p-16f) return false;
+        }
+    }
+    const F3 axis_ws = divs3(a, fsqrt(da));
+    return dot3(divs3(cta, fsqrt(ads)), axis_ws) >= cutoff;
+}
+
 // World-space bounding sphere of meshlet mi of an instance (vg_cull.wgsl:150-152).
 __device__ __forceinline__ void meshlet_sphere(const VgSceneDev& S, uint32_t mi, const Mat4& model,
                                                const HelioInstanceCullData& cd, F3& c, float& wr) {
@@ -69,11 +100,10 @@ __device__ __forceinline__ bool meshlet_frustum_cone(const CullView& C, const Me
         const float guard = fmul(wr, 1.5f);
         if (cam_dist_sq > fmul(guard, guard) && m.cone.w <= 1.0f) {
             const F3 a = mat3_vec(m.n0, m.n1, m.n2, f3(m.axis.x, m.axis.y, m.axis.z));
-            const F3 axis_ws = divs3(a, fsqrt(dot3(a, a)));
             const F3 apex = mat4_point3(model, f3(m.cone.x, m.cone.y, m.cone.z));
             const F3 cta = sub3(apex, cam);
             const float ads = dot3(cta, cta);
-            if (ads > 1.0e-12f && dot3(divs3(cta, fsqrt(ads)), axis_ws) >= m.cone.w) return false;
+            if (ads > 1.0e-12f && cone_rejects(a, cta, ads, m.cone.w)) return false;
         }
     }
     return true;
