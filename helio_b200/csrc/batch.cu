@@ -62,8 +62,8 @@ constexpr size_t kSmSelSpans = kSmSelQueue + 2 * 8 * kSelQueue;                 
 constexpr size_t kSmSelMask = kSmSelSpans + 4 * kSelectMaxViews;                // u32[kSelectMaxViews][8]
 constexpr size_t kSmSelStats = kSmSelMask + 4 * 8 * kSelectMaxViews;             // u32[kSelectMaxViews][9]
 constexpr size_t kSmHizJob = kSmSelStats + 4 * 9 * kSelectMaxViews;             // HizJob
-constexpr size_t kSmHizM3 = kSmHizJob + ((sizeof(HizJob) + 15) / 16) * 16;    // float[8][9]
-constexpr size_t kSmMisc = kSmHizM3 + 8 * 9 * 4;                              // u32[64]
+constexpr size_t kSmHizM3 = kSmHizJob + ((sizeof(HizJob) + 15) / 16) * 16;    // float[2][8][9]
+constexpr size_t kSmMisc = kSmHizM3 + 2 * 8 * 9 * 4;                          // u32[64]
 constexpr size_t kSmTileBegin = kSmMisc + 64 * 4;                             // u32[kBatchMaxViews]
 constexpr size_t kSmTotal = kSmTileBegin + 4 * kBatchMaxViews;
 // Phases 2..6 reuse the region from offset 0.
@@ -326,7 +326,8 @@ __device__ void phase_setup(const BatchParams& P) {
     }
 }
 
-// ── Phase 1a: one Hi-Z tile (levels 0..6; the tails follow the phase barrier) ─
+// ── Phase 1a: one Hi-Z unit: two consecutive tiles of a view (levels 0..6; the
+// tails follow the phase barrier) ──
 // The view's HizJob stays in shared memory while consecutive tiles of a CTA
 // belong to the same view (s_job holds its index, ~0u before the first tile).
 __device__ void load_hiz_job(const BatchParams& P, uint32_t v, char* sm) {
@@ -355,7 +356,24 @@ __device__ void phase_hiz_tile(const BatchParams& P, uint32_t tile, char* sm) {
         }
     }
     __syncthreads();
-    hiz_tile(J, *s_job, tile - J.tile_begin, nullptr, reinterpret_cast<float(*)[9]>(sm + kSmHizM3));
+    // Both tiles' loads are in flight together; warps 0 and 1 then finish one tile each.
+    const uint32_t lp = tile - s_tb[*s_job], t0 = 2u * lp, t1 = t0 + 1u;
+    const bool has1 = t1 < J.tiles_x * J.tiles_y;  // uniform over the CTA
+    float (*m3a)[9] = reinterpret_cast<float(*)[9]>(sm + kSmHizM3);
+    float (*m3b)[9] = m3a + 8;
+    float v0[4][4], v1[4][4];
+    hiz_tile_load(J, t0, v0);
+    if (has1) hiz_tile_load(J, t1, v1);
+    hiz_tile_copy0(J, t0, v0);
+    if (has1) hiz_tile_copy0(J, t1, v1);
+    if (J.mip_count <= 1) return;
+    hiz_tile_levels123(J, t0, v0, m3a);
+    if (has1) hiz_tile_levels123(J, t1, v1, m3b);
+    if (J.mip_count <= 3) return;
+    __syncthreads();
+    const uint32_t warp = threadIdx.x >> 5;
+    if (warp == 0) hiz_tile_levels456(J, t0, m3a);
+    else if (warp == 1 && has1) hiz_tile_levels456(J, t1, m3b);
 }
 
 // ── Phase 1b: object select against a group of views (vg_cull.wgsl:282-352) ──
@@ -873,7 +891,7 @@ __global__ void __launch_bounds__(kBatchThreads, 3) batch_kernel(BatchParams P) 
             }
             bx.pad[0] = bx.pad[1] = 0u;
             reinterpret_cast<SelBox*>(sm + kSmSelBox)[k] = bx;
-            reinterpret_cast<uint32_t*>(sm + kSmTileBegin)[k] = P.views[k].hiz.tile_begin;
+            reinterpret_cast<uint32_t*>(sm + kSmTileBegin)[k] = P.views[k].hiz_pair_begin;
         }
         // Hi-Z tiles (memory bound) and select units (arithmetic bound) are spread
         // evenly through one work queue, so that the CTAs sharing an SM overlap the two

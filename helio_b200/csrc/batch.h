@@ -26,7 +26,8 @@ struct alignas(16) BatchViewDev {
     HelioGpuVgDraw* draws;                   // [capacity]
     uint32_t* counters;                      // [16]; layout of the VG counters
     float reject_box[6];  // written by phase 0: x/y/z lower bounds, then upper bounds
-    uint32_t pad2[2];
+    uint32_t hiz_pair_begin;  // first Hi-Z unit (pair of tiles) of this view in the batch
+    uint32_t pad2;
 };
 
 static_assert(sizeof(BatchViewDev) % 16 == 0, "view table entries stay 16-byte aligned");
@@ -51,7 +52,7 @@ struct BatchParams {
     uint32_t view_count;
     uint32_t select_views;    // views per select unit, 1..32
     uint32_t object_chunks;   // ceil(object_count / kBatchChunk)
-    uint32_t hiz_tiles;       // Hi-Z tiles of all views
+    uint32_t hiz_tiles;       // Hi-Z units of all views: pairs of horizontally consecutive tiles
     uint32_t* barrier;        // [2] arrival count (zero before the launch), generation
     uint32_t* error;          // [1] kBatchErr* bits, zero before the launch
     uint32_t* work;           // [1] phase-1 work queue head, zero before the launch

@@ -102,7 +102,7 @@ struct BatchPlan {
     size_t need[kBatchBufs] = {};
     std::vector<size_t> level_off, out_offset;
     std::vector<uint32_t> capacity;
-    uint32_t tiles = 0, grid = 0, object_chunks = 0, span_capacity = 0, lod_pitch = 0;
+    uint32_t tiles = 0, pairs = 0, grid = 0, object_chunks = 0, span_capacity = 0, lod_pitch = 0;
 };
 
 int32_t plan_batch(const helio_batch_config& cfg, const helio_vg_scene* sc, uint32_t n, const helio_batch_view* views,
@@ -126,7 +126,9 @@ int32_t plan_batch(const helio_batch_config& cfg, const helio_vg_scene* sc, uint
         p.level_off[v] = level_floats;
         level_floats += (need + 3u) & ~(size_t)3u;
         J.tile_begin = p.tiles;
+        if (dev) dev[v].hiz_pair_begin = p.pairs;
         p.tiles += J.tiles_x * J.tiles_y;
+        p.pairs += (J.tiles_x * J.tiles_y + 1u) / 2u;
         const uint32_t cap = in.draw_capacity ? in.draw_capacity : (uint32_t)default_cap;
         p.capacity[v] = cap;
         p.out_offset[v + 1] = p.out_offset[v] + (cap ? cap : 1);
@@ -288,7 +290,7 @@ int32_t helio_batch_prepare(helio_batch* b, const helio_vg_scene* sc, uint32_t n
     if ((st = plan_batch(b->cfg, sc, n, views, plan, b->host_views.data()))) return st;
     b->grid = plan.grid;
     b->object_chunks = plan.object_chunks;
-    b->hiz_tiles = plan.tiles;
+    b->hiz_tiles = plan.pairs;
     b->span_capacity = plan.span_capacity;
     b->lod_pitch = plan.lod_pitch;
     b->out_offset = plan.out_offset;

@@ -96,22 +96,15 @@ static __device__ __noinline__ void hiz_tail_warp(const HizJob& J) {
     }
 }
 
-// Tile `tile` (flat index within job J, whose ticket is tickets[job]) by all 256
-// threads of the CTA. s_m3 is an 8x9 shared scratch. Warps 1..7 return right
-// after the level-3 barrier; warp 0 finishes levels 4..6 and, if this CTA is the
-// last of the view, the tail. With tickets == nullptr the tile stops at level 6
-// and the caller builds the tail after a grid-wide barrier.
-__device__ __forceinline__ void hiz_tile(const HizJob& J, uint32_t job, uint32_t tile, uint32_t* tickets,
-                                         float (*s_m3)[9]) {
+// Level 0 of tile `tile` of job J into v (4x4 per thread; 256 threads cover 64x64);
+// outside the image the block reads 0 (those texels are never used).
+__device__ __forceinline__ void hiz_tile_load(const HizJob& J, uint32_t tile, float (&v)[4][4]) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t tile_y = tile / J.tiles_x, tile_x = tile - tile_y * J.tiles_x;
     const uint32_t X0 = tile_x * kHizTile, Y0 = tile_y * kHizTile;
     const uint32_t W = J.lw[0], H = J.lh[0];
     const int tx4 = lane & 15, ty4 = warp * 2 + (lane >> 4);
     const uint32_t bx = X0 + 4 * tx4, by = Y0 + 4 * ty4;
-
-    // Level 0: 4x4 block per thread.
-    float v[4][4];
     const bool aligned = ((J.depth_pitch & 3u) == 0u) && ((reinterpret_cast<uintptr_t>(J.depth) & 15u) == 0u);
     if (aligned && bx + 4 <= W && by + 4 <= H) {
 #pragma unroll
@@ -129,25 +122,41 @@ __device__ __forceinline__ void hiz_tile(const HizJob& J, uint32_t job, uint32_t
             for (int c = 0; c < 4; ++c)
                 v[r][c] = (bx + c < W && by + r < H) ? __ldcs(J.depth + (size_t)(by + r) * J.depth_pitch + bx + c) : 0.0f;
     }
-    if (J.copy_mip0) {
-        float* L0 = J.levels[0];
-        const uint32_t p0 = J.lpitch[0];
-        const bool al0 = ((p0 & 3u) == 0u) && ((reinterpret_cast<uintptr_t>(L0) & 15u) == 0u);
+}
+
+// Level 0 of a loaded tile into the pyramid, when the job does not alias it.
+__device__ __forceinline__ void hiz_tile_copy0(const HizJob& J, uint32_t tile, const float (&v)[4][4]) {
+    if (!J.copy_mip0) return;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint32_t tile_y = tile / J.tiles_x, tile_x = tile - tile_y * J.tiles_x;
+    const uint32_t W = J.lw[0], H = J.lh[0];
+    const uint32_t bx = tile_x * kHizTile + 4 * (lane & 15), by = tile_y * kHizTile + 4 * (warp * 2 + (lane >> 4));
+    float* L0 = J.levels[0];
+    const uint32_t p0 = J.lpitch[0];
+    const bool al0 = ((p0 & 3u) == 0u) && ((reinterpret_cast<uintptr_t>(L0) & 15u) == 0u);
 #pragma unroll
-        for (int r = 0; r < 4; ++r) {
-            if (by + r >= H) break;
-            float* row = L0 + (size_t)(by + r) * p0 + bx;
-            if (al0 && bx + 4 <= W) {
-                *reinterpret_cast<float4*>(row) = make_float4(v[r][0], v[r][1], v[r][2], v[r][3]);
-            } else {
+    for (int r = 0; r < 4; ++r) {
+        if (by + r >= H) break;
+        float* row = L0 + (size_t)(by + r) * p0 + bx;
+        if (al0 && bx + 4 <= W) {
+            *reinterpret_cast<float4*>(row) = make_float4(v[r][0], v[r][1], v[r][2], v[r][3]);
+        } else {
 #pragma unroll
-                for (int c = 0; c < 4; ++c)
-                    if (bx + c < W) row[c] = v[r][c];
-            }
+            for (int c = 0; c < 4; ++c)
+                if (bx + c < W) row[c] = v[r][c];
         }
     }
-    if (J.mip_count <= 1) return;
+}
 
+// Levels 1..3 of a loaded tile by all 256 threads (no barrier): level 3 goes to the
+// pyramid and to s_m3 (8x9 shared) for levels 4..6.
+__device__ __forceinline__ void hiz_tile_levels123(const HizJob& J, uint32_t tile, const float (&v)[4][4],
+                                                   float (*s_m3)[9]) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint32_t tile_y = tile / J.tiles_x, tile_x = tile - tile_y * J.tiles_x;
+    const uint32_t X0 = tile_x * kHizTile, Y0 = tile_y * kHizTile;
+    const int tx4 = lane & 15, ty4 = warp * 2 + (lane >> 4);
+    if (J.mip_count <= 1) return;
     // Level 1: 2x2 per thread.
     float m1[2][2];
     {
@@ -174,7 +183,6 @@ __device__ __forceinline__ void hiz_tile(const HizJob& J, uint32_t job, uint32_t
         }
     }
     if (J.mip_count <= 2) return;
-
     // Level 2: one texel per thread.
     const float m2 = hiz_red4(m1[0][0], m1[0][1], m1[1][0], m1[1][1], J.lw[1] == 1u, J.lh[1] == 1u);
     {
@@ -182,56 +190,73 @@ __device__ __forceinline__ void hiz_tile(const HizJob& J, uint32_t job, uint32_t
         if (x2 < J.lw[2] && y2 < J.lh[2]) J.levels[2][(size_t)y2 * J.lpitch[2] + x2] = m2;
     }
     if (J.mip_count <= 3) return;
-
     // Level 3: 2x2 across lanes (x: lane^1, y: lane^16).
-    {
-        float b = __shfl_xor_sync(0xffffffffu, m2, 1);
-        float c = __shfl_xor_sync(0xffffffffu, m2, 16);
-        float d = __shfl_xor_sync(0xffffffffu, m2, 17);
-        float m3 = hiz_red4(m2, b, c, d, J.lw[2] == 1u, J.lh[2] == 1u);
-        if ((lane & 17) == 0) {
-            const int lx = tx4 >> 1, ly = warp;  // ty4 >> 1 == warp
-            s_m3[ly][lx] = m3;
-            const uint32_t x3 = (X0 >> 3) + lx, y3 = (Y0 >> 3) + ly;
-            if (x3 < J.lw[3] && y3 < J.lh[3]) J.levels[3][(size_t)y3 * J.lpitch[3] + x3] = m3;
-        }
+    float b = __shfl_xor_sync(0xffffffffu, m2, 1);
+    float c = __shfl_xor_sync(0xffffffffu, m2, 16);
+    float d = __shfl_xor_sync(0xffffffffu, m2, 17);
+    float m3 = hiz_red4(m2, b, c, d, J.lw[2] == 1u, J.lh[2] == 1u);
+    if ((lane & 17) == 0) {
+        const int lx = tx4 >> 1, ly = warp;  // ty4 >> 1 == warp
+        s_m3[ly][lx] = m3;
+        const uint32_t x3 = (X0 >> 3) + lx, y3 = (Y0 >> 3) + ly;
+        if (x3 < J.lw[3] && y3 < J.lh[3]) J.levels[3][(size_t)y3 * J.lpitch[3] + x3] = m3;
     }
+}
+
+// Levels 4..6 of a tile by one warp (lane = threadIdx.x & 31), from s_m3.
+__device__ __forceinline__ void hiz_tile_levels456(const HizJob& J, uint32_t tile, const float (*s_m3)[9]) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t tile_y = tile / J.tiles_x, tile_x = tile - tile_y * J.tiles_x;
+    const uint32_t X0 = tile_x * kHizTile, Y0 = tile_y * kHizTile;
+    if (J.mip_count <= 4) return;
+    const int x4 = lane & 3, y4 = (lane >> 2) & 3;
+    float m4 = hiz_red4(s_m3[2 * y4][2 * x4], s_m3[2 * y4][2 * x4 + 1], s_m3[2 * y4 + 1][2 * x4],
+                        s_m3[2 * y4 + 1][2 * x4 + 1], J.lw[3] == 1u, J.lh[3] == 1u);
+    if (lane < 16) {
+        const uint32_t gx = (X0 >> 4) + x4, gy = (Y0 >> 4) + y4;
+        if (gx < J.lw[4] && gy < J.lh[4]) J.levels[4][(size_t)gy * J.lpitch[4] + gx] = m4;
+    }
+    if (J.mip_count <= 5) return;
+    float b = __shfl_xor_sync(0xffffffffu, m4, 1);
+    float c = __shfl_xor_sync(0xffffffffu, m4, 4);
+    float d = __shfl_xor_sync(0xffffffffu, m4, 5);
+    float m5 = hiz_red4(m4, b, c, d, J.lw[4] == 1u, J.lh[4] == 1u);
+    if (lane < 16 && (lane & 5) == 0) {
+        const uint32_t gx = (X0 >> 5) + (x4 >> 1), gy = (Y0 >> 5) + (y4 >> 1);
+        if (gx < J.lw[5] && gy < J.lh[5]) J.levels[5][(size_t)gy * J.lpitch[5] + gx] = m5;
+    }
+    if (J.mip_count <= 6) return;
+    float b6 = __shfl_sync(0xffffffffu, m5, 2);
+    float c6 = __shfl_sync(0xffffffffu, m5, 8);
+    float d6 = __shfl_sync(0xffffffffu, m5, 10);
+    float m6 = hiz_red4(m5, b6, c6, d6, J.lw[5] == 1u, J.lh[5] == 1u);
+    if (lane == 0) {
+        const uint32_t gx = X0 >> 6, gy = Y0 >> 6;
+        if (gx < J.lw[6] && gy < J.lh[6]) J.levels[6][(size_t)gy * J.lpitch[6] + gx] = m6;
+    }
+}
+
+// Tile `tile` (flat index within job J, whose ticket is tickets[job]) by all 256
+// threads of the CTA. s_m3 is an 8x9 shared scratch. Warps 1..7 return right
+// after the level-3 barrier; warp 0 finishes levels 4..6 and, if this CTA is the
+// last of the view, the tail. With tickets == nullptr the tile stops at level 6
+// and the caller builds the tail after a grid-wide barrier.
+__device__ __forceinline__ void hiz_tile(const HizJob& J, uint32_t job, uint32_t tile, uint32_t* tickets,
+                                         float (*s_m3)[9]) {
+    float v[4][4];
+    hiz_tile_load(J, tile, v);
+    hiz_tile_copy0(J, tile, v);
+    if (J.mip_count <= 1) return;
+    hiz_tile_levels123(J, tile, v, s_m3);
+    if (J.mip_count <= 3) return;
     __syncthreads();
-    if (warp != 0) return;  // levels 4.. and the tail need only warp 0
-    // Levels 4..6: warp 0.
-    if (J.mip_count > 4) {
-        const int x4 = lane & 3, y4 = (lane >> 2) & 3;
-        float m4 = hiz_red4(s_m3[2 * y4][2 * x4], s_m3[2 * y4][2 * x4 + 1], s_m3[2 * y4 + 1][2 * x4],
-                            s_m3[2 * y4 + 1][2 * x4 + 1], J.lw[3] == 1u, J.lh[3] == 1u);
-        if (lane < 16) {
-            const uint32_t gx = (X0 >> 4) + x4, gy = (Y0 >> 4) + y4;
-            if (gx < J.lw[4] && gy < J.lh[4]) J.levels[4][(size_t)gy * J.lpitch[4] + gx] = m4;
-        }
-        if (J.mip_count > 5) {
-            float b = __shfl_xor_sync(0xffffffffu, m4, 1);
-            float c = __shfl_xor_sync(0xffffffffu, m4, 4);
-            float d = __shfl_xor_sync(0xffffffffu, m4, 5);
-            float m5 = hiz_red4(m4, b, c, d, J.lw[4] == 1u, J.lh[4] == 1u);
-            if (lane < 16 && (lane & 5) == 0) {
-                const uint32_t gx = (X0 >> 5) + (x4 >> 1), gy = (Y0 >> 5) + (y4 >> 1);
-                if (gx < J.lw[5] && gy < J.lh[5]) J.levels[5][(size_t)gy * J.lpitch[5] + gx] = m5;
-            }
-            if (J.mip_count > 6) {
-                float b6 = __shfl_sync(0xffffffffu, m5, 2);
-                float c6 = __shfl_sync(0xffffffffu, m5, 8);
-                float d6 = __shfl_sync(0xffffffffu, m5, 10);
-                float m6 = hiz_red4(m5, b6, c6, d6, J.lw[5] == 1u, J.lh[5] == 1u);
-                if (lane == 0) {
-                    const uint32_t gx = X0 >> 6, gy = Y0 >> 6;
-                    if (gx < J.lw[6] && gy < J.lh[6]) J.levels[6][(size_t)gy * J.lpitch[6] + gx] = m6;
-                }
-            }
-        }
-    }
+    if ((threadIdx.x >> 5) != 0) return;  // levels 4.. and the tail need only warp 0
+    hiz_tile_levels456(J, tile, s_m3);
     if (J.mip_count <= 7 || tickets == nullptr) return;
 
     // Tail: level 6 is written by warp 0 only, so warp 0 alone takes the ticket;
     // the warp of the last CTA of this job builds levels 7.. from level 6.
+    const int lane = threadIdx.x & 31;
     __threadfence();
     __syncwarp();
     uint32_t last = 0u;
