@@ -994,9 +994,45 @@ __global__ void scene_bounds_kernel(VgSceneDev S, uint32_t* bounds) {
 
 }  // namespace
 
+// One CTA per view: the view's first packed draw is the sum of the earlier views'
+// published counts; its draws are copied with the CTA's threads.
+__global__ void pack_draws_kernel(const BatchViewDev* views, uint32_t V, HelioDrawIndexedIndirectArgs* indirect,
+                                  HelioGpuVgDraw* draws, uint32_t* offsets, uint64_t capacity) {
+    __shared__ uint32_t s_part[kBatchThreads / 32];
+    const uint32_t v = blockIdx.x, tid = threadIdx.x;
+    uint32_t before = 0;
+    for (uint32_t u = tid; u < v; u += blockDim.x) before += min(__ldg(views[u].counters), views[u].capacity);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) before += __shfl_xor_sync(0xffffffffu, before, o);
+    if ((tid & 31u) == 0) s_part[tid >> 5] = before;
+    __syncthreads();
+    uint64_t base = 0;
+    for (uint32_t w = 0; w < blockDim.x / 32; ++w) base += s_part[w];
+    const uint32_t n = min(__ldg(views[v].counters), views[v].capacity);
+    if (tid == 0) {
+        offsets[v] = (uint32_t)(base < capacity ? base : capacity);
+        if (v == V - 1) offsets[V] = (uint32_t)(base + n < capacity ? base + n : capacity);
+    }
+    const uint32_t* src_i = reinterpret_cast<const uint32_t*>(views[v].indirect);
+    uint32_t* dst_i = reinterpret_cast<uint32_t*>(indirect);
+    const uint64_t room = base >= capacity ? 0u : capacity - base;
+    const uint64_t m = (uint64_t)n < room ? (uint64_t)n : room;
+    for (uint64_t k = tid; k < m * 5u; k += blockDim.x) dst_i[base * 5u + k] = __ldg(src_i + k);
+    const uint4* src_d = reinterpret_cast<const uint4*>(views[v].draws);
+    uint4* dst_d = reinterpret_cast<uint4*>(draws);
+    for (uint64_t k = tid; k < m; k += blockDim.x) dst_d[base + k] = __ldg(src_d + k);
+}
+
 cudaError_t launch_scene_bounds(const VgSceneDev& scene, uint32_t* bounds, cudaStream_t stream) {
     const uint32_t n = scene.object_count;
     if (n) scene_bounds_kernel<<<(n + 255) / 256, 256, 0, stream>>>(scene, bounds);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pack_draws(const BatchViewDev* views, uint32_t view_count, HelioDrawIndexedIndirectArgs* indirect,
+                              HelioGpuVgDraw* draws, uint32_t* offsets, uint64_t capacity, cudaStream_t stream) {
+    if (view_count) pack_draws_kernel<<<view_count, kBatchThreads, 0, stream>>>(views, view_count, indirect, draws,
+                                                                                offsets, capacity);
     return cudaGetLastError();
 }
 

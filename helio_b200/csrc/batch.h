@@ -83,6 +83,12 @@ constexpr uint32_t kBatchPhaseStamps = 10;
 // the select computes them). `bounds` must be zero before the launch.
 cudaError_t launch_scene_bounds(const VgSceneDev& scene, uint32_t* bounds, cudaStream_t stream);
 
+// Packs the published draws of every view (min(counters[0], capacity) each) into
+// one pair of arrays, view after view; offsets[v] = first draw of view v, offsets[V] =
+// the total (entries past `capacity` are not written).
+cudaError_t launch_pack_draws(const BatchViewDev* views, uint32_t view_count, HelioDrawIndexedIndirectArgs* indirect,
+                              HelioGpuVgDraw* draws, uint32_t* offsets, uint64_t capacity, cudaStream_t stream);
+
 // Dynamic shared memory of the persistent kernel (bytes).
 size_t batch_dynamic_smem();
 // Launches the cooperative kernel with `grid` CTAs (all co-resident) on `stream`.

@@ -1,6 +1,7 @@
 // batch_api.cu — host side of the device-resident scene and of the batched
 // multi-view cull (include/helio_cull.h, "Batched multi-view culling").
 
+#include <cstddef>
 #include <cstring>
 #include <new>
 #include <algorithm>
@@ -436,11 +437,29 @@ int32_t helio_batch_set_cameras(helio_batch* b, uint32_t n, const HelioGpuCamera
     HELIO_ARG(b && cams, "null pointer");
     HELIO_ARG(b->prepared && n == b->view_count, "camera count differs from the prepared views");
     cudaStream_t s = as_stream(stream);
-    for (uint32_t v = 0; v < n; ++v) {
-        b->host_views[v].camera = cams[v];
-        HELIO_CK(cudaMemcpyAsync(b->views.as<helio::BatchViewDev>() + v, &b->host_views[v].camera,
-                                 sizeof(HelioGpuCameraUniforms), cudaMemcpyHostToDevice, s));
-    }
+    for (uint32_t v = 0; v < n; ++v) b->host_views[v].camera = cams[v];
+    // One strided copy: the camera leads every entry of the view table.
+    static_assert(offsetof(helio::BatchViewDev, camera) == 0, "camera leads the view table entry");
+    HELIO_CK(cudaMemcpy2DAsync(b->views.ptr, sizeof(helio::BatchViewDev), b->host_views.data(),
+                               sizeof(helio::BatchViewDev), sizeof(HelioGpuCameraUniforms), n, cudaMemcpyHostToDevice,
+                               s));
+    return HELIO_OK;
+}
+
+int32_t helio_batch_set_cameras_device(helio_batch* b, uint32_t n, const HelioGpuCameraUniforms* cams, void* stream) {
+    HELIO_ARG(b && cams, "null pointer");
+    HELIO_ARG(b->prepared && n == b->view_count, "camera count differs from the prepared views");
+    HELIO_CK(cudaMemcpy2DAsync(b->views.ptr, sizeof(helio::BatchViewDev), cams, sizeof(HelioGpuCameraUniforms),
+                               sizeof(HelioGpuCameraUniforms), n, cudaMemcpyDeviceToDevice, as_stream(stream)));
+    return HELIO_OK;
+}
+
+int32_t helio_batch_pack_draws(const helio_batch* b, HelioDrawIndexedIndirectArgs* indirect, HelioGpuVgDraw* draws,
+                               uint32_t* offsets, uint64_t capacity, void* stream) {
+    HELIO_ARG(b && indirect && draws && offsets, "null pointer");
+    HELIO_ARG(b->prepared, "batch not prepared");
+    HELIO_CK(helio::launch_pack_draws(b->views.as<helio::BatchViewDev>(), b->view_count, indirect, draws, offsets,
+                                      capacity, as_stream(stream)));
     return HELIO_OK;
 }
 

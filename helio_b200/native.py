@@ -247,6 +247,7 @@ CULL_EXPORTS = {
     "helio_batch_create": (i32, [C.POINTER(BatchConfig), C.POINTER(vp)]),
     "helio_batch_prepare": (i32, [vp, vp, u32, C.POINTER(BatchView), vp]),
     "helio_batch_set_cameras": (i32, [vp, u32, C.POINTER(GpuCameraUniforms), vp]),
+    "helio_batch_set_cameras_device": (i32, [vp, u32, vp, vp]),
     "helio_batch_execute": (i32, [vp, vp]),
     "helio_batch_get_view_outputs": (i32, [vp, u32, C.POINTER(BatchViewOutputs)]),
     "helio_batch_get_spans": (i32, [vp, C.POINTER(BatchSpanList)]),
@@ -257,6 +258,7 @@ CULL_EXPORTS = {
     "helio_batch_growth_bytes": (i32, [vp, C.POINTER(BatchConfig), vp, u32, C.POINTER(BatchView), C.POINTER(u64)]),
     "helio_batch_reconfigure": (i32, [vp, C.POINTER(BatchConfig)]),
     "helio_batch_autotune": (i32, [vp, u32, C.POINTER(BatchTuning), vp]),
+    "helio_batch_pack_draws": (i32, [vp, vp, vp, vp, u64, vp]),
     "helio_batch_destroy": (None, [vp]),
     "helio_serve_create": (i32, [C.POINTER(ServeConfig), C.POINTER(vp)]),
     "helio_serve_add_scene": (i32, [vp, vp, C.POINTER(u32)]),

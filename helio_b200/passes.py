@@ -286,6 +286,12 @@ class BatchedCull:
         N.check(self._lib.helio_batch_prepare(self._h, scene._h, len(views), arr, _stream_ptr(stream)))
         self.view_count = len(views)
 
+    def pack_draws(self, indirect, draws, offsets, stream=None) -> None:
+        """Every view's published draws into one pair of device tensors (int32 [cap, 5]
+        and [cap, 4]), view after view; offsets (int32 [views + 1]) receives the view starts."""
+        N.check(self._lib.helio_batch_pack_draws(self._h, indirect.data_ptr(), draws.data_ptr(), offsets.data_ptr(),
+                                                 indirect.shape[0], _stream_ptr(stream)))
+
     def autotune(self, repeats: int = 3, stream=None) -> dict:
         """Times the prepared batch under every launch-shape candidate (views per
         select unit x CTAs per SM) and keeps the fastest (helio_batch_autotune)."""
@@ -293,6 +299,12 @@ class BatchedCull:
         N.check(self._lib.helio_batch_autotune(self._h, repeats, C.byref(t), _stream_ptr(stream)))
         return {"select_views": t.select_views, "ctas": t.ctas, "candidates": t.candidates, "best_ms": t.best_ms,
                 "default_ms": t.default_ms}
+
+    def set_cameras_device(self, cameras: torch.Tensor, stream=None) -> None:
+        """Cameras from a device tensor of view_count x 368 bytes (stream-ordered)."""
+        assert cameras.is_cuda and cameras.numel() * cameras.element_size() >= 368 * self.view_count
+        N.check(self._lib.helio_batch_set_cameras_device(self._h, self.view_count, cameras.data_ptr(),
+                                                         _stream_ptr(stream)))
 
     def set_cameras(self, cameras: list, stream=None) -> None:
         arr = (N.GpuCameraUniforms * len(cameras))(*cameras)

@@ -498,10 +498,20 @@ int32_t helio_batch_prepare(helio_batch* batch, const helio_vg_scene* scene, uin
 /* Replaces the cameras of the prepared views (no allocation). */
 int32_t helio_batch_set_cameras(helio_batch* batch, uint32_t view_count, const HelioGpuCameraUniforms* cameras,
                                 void* stream);
+/* The same from device memory (stream-ordered; for hosts that upload cameras with
+ * their other per-frame inputs in one copy). */
+int32_t helio_batch_set_cameras_device(helio_batch* batch, uint32_t view_count, const HelioGpuCameraUniforms* cameras,
+                                       void* stream);
 /* Clears the counters and runs the persistent cooperative kernel on `stream`. */
 int32_t helio_batch_execute(helio_batch* batch, void* stream);
 int32_t helio_batch_get_view_outputs(const helio_batch* batch, uint32_t view, helio_batch_view_outputs* out);
 int32_t helio_batch_get_spans(const helio_batch* batch, helio_batch_span_list* out);
+/* Packs every view's published draws (min(counters[0], capacity) each) into one pair
+ * of device arrays, view after view, on `stream` (after helio_batch_execute):
+ * offsets[v] = first draw of view v, offsets[view_count] = the total; draws past
+ * `capacity` are not written. Lets a host read all views' draws back in one copy. */
+int32_t helio_batch_pack_draws(const helio_batch* batch, HelioDrawIndexedIndirectArgs* indirect, HelioGpuVgDraw* draws,
+                               uint32_t* offsets, uint64_t capacity, void* stream);
 /* Tracing: device time (us) of the phases of the last execute, read from timer
  * stamps the kernel takes at its grid barriers (synchronises `stream`). Order:
  * view setup, Hi-Z + object select, span-count scan, span expansion, meshlet tests,

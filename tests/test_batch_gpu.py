@@ -160,3 +160,35 @@ def test_autotune_keeps_results(cuda):
     for x, y in zip(before, after):
         for k in ("counters", "indirect", "draws", "lod"):
             np.testing.assert_array_equal(x[k], y[k])
+
+
+def test_pack_draws_matches_per_view_outputs(cuda):
+    """helio_batch_pack_draws lays every view's published draws end to end."""
+    import torch
+    from helio_b200 import scene as S
+
+    w = S.config(3, scale=0.05)
+    views = w.views[:16]
+    b, vs, _ = run_batch(w.scene, views, span_visibility=False)
+    per = [gather(b, i, len(w.scene.objects)) for i in range(len(views))]
+    total = sum(len(p["indirect"]) for p in per)
+    cap = total + 7
+    ind = torch.full((cap, 5), -1, dtype=torch.int32, device="cuda")
+    drw = torch.full((cap, 4), -1, dtype=torch.int32, device="cuda")
+    off = torch.zeros(len(views) + 1, dtype=torch.int32, device="cuda")
+    b.pack_draws(ind, drw, off)
+    torch.cuda.synchronize()
+    o = off.cpu().numpy()
+    assert o[-1] == total
+    for i, p in enumerate(per):
+        np.testing.assert_array_equal(u32(ind[o[i]:o[i + 1]]), p["indirect"], err_msg=f"view {i} indirect")
+        np.testing.assert_array_equal(u32(drw[o[i]:o[i + 1]]), p["draws"], err_msg=f"view {i} draws")
+    assert (ind[total:].cpu().numpy() == -1).all()
+    # A capacity below the total writes only what fits.
+    small = max(1, total // 3)
+    ind2 = torch.zeros((small, 5), dtype=torch.int32, device="cuda")
+    drw2 = torch.zeros((small, 4), dtype=torch.int32, device="cuda")
+    b.pack_draws(ind2, drw2, off)
+    torch.cuda.synchronize()
+    assert off.cpu().numpy()[-1] == small
+    np.testing.assert_array_equal(u32(ind2), np.concatenate([p["indirect"] for p in per])[:small])
