@@ -192,24 +192,30 @@ __device__ void grid_exclusive_scan(const BatchParams& P, const uint32_t* in, ui
 // double precision may have misplaced), or when Q is unbounded: a recession
 // direction of Q is a cross product of two normals (lanes 0..14, both signs) that
 // no plane rejects.
+struct PlaneD {
+    double x, y, z, w;  // normal and offset pushed out by s_i
+    __device__ double norm() const { return sqrt(x * x + y * y + z * z); }
+    __device__ double at(double px, double py, double pz) const { return x * px + y * py + z * pz + w; }
+};
+
+// Plane i of `pl` (shared memory, so a lane-dependent i costs no local memory) with
+// its offset pushed out by rmax + 2^-20 (cl1 + |w| + rmax).
+__device__ __forceinline__ PlaneD pushed_plane(const Planes& pl, int i, double rmax, double cl1) {
+    const float4 p = pl.p[i];
+    return PlaneD{p.x, p.y, p.z, (double)p.w + rmax + 0x1p-20 * (cl1 + fabs((double)p.w) + rmax)};
+}
+
 __device__ void reject_box_warp(const Planes& pl, float rmax_f, float cl1_f, float box[6]) {
     const int lane = threadIdx.x & 31;
-    double n[6][3], w[6];
     bool finite = isfinite(rmax_f) && isfinite(cl1_f);
     const double rmax = rmax_f, cl1 = cl1_f;
 #pragma unroll
     for (int i = 0; i < 6; ++i) {
         const float4 p = pl.p[i];
         finite = finite && isfinite(p.x) && isfinite(p.y) && isfinite(p.z) && isfinite(p.w);
-        n[i][0] = p.x;
-        n[i][1] = p.y;
-        n[i][2] = p.z;
-        w[i] = (double)p.w + rmax + 0x1p-20 * (cl1 + fabs((double)p.w) + rmax);
     }
-    auto nrm = [&](int i) { return sqrt(n[i][0] * n[i][0] + n[i][1] * n[i][1] + n[i][2] * n[i][2]); };
-    auto slack = [&](int j, double x, double y, double z) { return n[j][0] * x + n[j][1] * y + n[j][2] * z + w[j]; };
-    auto scale = [&](int j, double x, double y, double z) {
-        return (fabs(x) + fabs(y) + fabs(z)) * nrm(j) + fabs(w[j]) + 1e-30;
+    auto scale = [&](const PlaneD& q, double x, double y, double z) {
+        return (fabs(x) + fabs(y) + fabs(z)) * q.norm() + fabs(q.w) + 1e-30;
     };
     bool bad = !finite;
     double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
@@ -225,26 +231,27 @@ __device__ void reject_box_warp(const Planes& pl, float rmax_f, float cl1_f, flo
                 c = b + 1;
             }
         }
-        const double bc[3] = {n[b][1] * n[c][2] - n[b][2] * n[c][1], n[b][2] * n[c][0] - n[b][0] * n[c][2],
-                              n[b][0] * n[c][1] - n[b][1] * n[c][0]};
-        const double ca[3] = {n[c][1] * n[a][2] - n[c][2] * n[a][1], n[c][2] * n[a][0] - n[c][0] * n[a][2],
-                              n[c][0] * n[a][1] - n[c][1] * n[a][0]};
-        const double ab[3] = {n[a][1] * n[b][2] - n[a][2] * n[b][1], n[a][2] * n[b][0] - n[a][0] * n[b][2],
-                              n[a][0] * n[b][1] - n[a][1] * n[b][0]};
-        const double det = n[a][0] * bc[0] + n[a][1] * bc[1] + n[a][2] * bc[2];
-        const double rel = fabs(det) / (nrm(a) * nrm(b) * nrm(c) + 1e-300);
+        const PlaneD A = pushed_plane(pl, a, rmax, cl1), B = pushed_plane(pl, b, rmax, cl1),
+                     Cc = pushed_plane(pl, c, rmax, cl1);
+        const double bc[3] = {B.y * Cc.z - B.z * Cc.y, B.z * Cc.x - B.x * Cc.z, B.x * Cc.y - B.y * Cc.x};
+        const double ca[3] = {Cc.y * A.z - Cc.z * A.y, Cc.z * A.x - Cc.x * A.z, Cc.x * A.y - Cc.y * A.x};
+        const double ab[3] = {A.y * B.z - A.z * B.y, A.z * B.x - A.x * B.z, A.x * B.y - A.y * B.x};
+        const double det = A.x * bc[0] + A.y * bc[1] + A.z * bc[2];
+        const double rel = fabs(det) / (A.norm() * B.norm() * Cc.norm() + 1e-300);
         const bool corner = a < 2 && b >= 2 && b < 4 && c >= 4;
         double p[3] = {0.0, 0.0, 0.0};
         bool feasible = false, loose = false;
         if (rel > 1e-12) {
 #pragma unroll
-            for (int k = 0; k < 3; ++k) p[k] = -(w[a] * bc[k] + w[b] * ca[k] + w[c] * ab[k]) / det;
+            for (int k = 0; k < 3; ++k) p[k] = -(A.w * bc[k] + B.w * ca[k] + Cc.w * ab[k]) / det;
             feasible = isfinite(p[0]) && isfinite(p[1]) && isfinite(p[2]);
             loose = feasible;
+#pragma unroll
             for (int j = 0; j < 6; ++j) {
-                const double s = slack(j, p[0], p[1], p[2]), sc = scale(j, p[0], p[1], p[2]);
-                feasible = feasible && s >= -1e-7 * sc;
-                loose = loose && s >= -1e-3 * sc;
+                const PlaneD q = pushed_plane(pl, j, rmax, cl1);
+                const double sl = q.at(p[0], p[1], p[2]), sc = scale(q, p[0], p[1], p[2]);
+                feasible = feasible && sl >= -1e-7 * sc;
+                loose = loose && sl >= -1e-3 * sc;
             }
         }
         if (corner && !(rel > 1e-4 && feasible)) bad = true;
@@ -259,14 +266,17 @@ __device__ void reject_box_warp(const Planes& pl, float rmax_f, float cl1_f, flo
                 ++a;
                 b = a + 1;
             }
-        const double d[3] = {n[a][1] * n[b][2] - n[a][2] * n[b][1], n[a][2] * n[b][0] - n[a][0] * n[b][2],
-                             n[a][0] * n[b][1] - n[a][1] * n[b][0]};
+        const PlaneD A = pushed_plane(pl, a, rmax, cl1), B = pushed_plane(pl, b, rmax, cl1);
+        const double d[3] = {A.y * B.z - A.z * B.y, A.z * B.x - A.x * B.z, A.x * B.y - A.y * B.x};
         const double len = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
-        if (len > 1e-12 * nrm(a) * nrm(b)) {
+        if (len > 1e-12 * A.norm() * B.norm()) {
             for (int sgn = -1; sgn <= 1; sgn += 2) {
                 bool ray = true;
-                for (int j = 0; j < 6; ++j)
-                    ray = ray && sgn * (n[j][0] * d[0] + n[j][1] * d[1] + n[j][2] * d[2]) >= -1e-9 * nrm(j) * len;
+#pragma unroll
+                for (int j = 0; j < 6; ++j) {
+                    const PlaneD q = pushed_plane(pl, j, rmax, cl1);
+                    ray = ray && sgn * (q.x * d[0] + q.y * d[1] + q.z * d[2]) >= -1e-9 * q.norm() * len;
+                }
                 if (ray) bad = true;
             }
         }
