@@ -73,6 +73,10 @@ constexpr int kBits = kWindowsPerWarp + 2;
 constexpr size_t kSmTestQueue = kSmTestBits + 8 * kBits * 4;            // u16[8][64]
 constexpr size_t kSmVStart = 0;                                          // u32[kBatchMaxViews + 1]
 static_assert(kSmTestQueue + 8 * 64 * 2 <= kSmMisc, "test phase fits");
+// The cull kernel (phases 4..6) has its own, small layout: the test phase's region
+// from offset 0, then the scan scratch.
+constexpr size_t kSm2Misc = ((kSmTestQueue + 8 * 64 * 2) + 15) / 16 * 16;  // u32[64]
+constexpr size_t kSm2Total = kSm2Misc + 64 * 4;
 
 __device__ __forceinline__ uint32_t ld_cg(const uint32_t* p) { return __ldcg(p); }
 
@@ -951,9 +955,15 @@ __global__ void __launch_bounds__(kBatchThreads, 3) batch_kernel(BatchParams P) 
     grid_exclusive_scan(P, P.chunk_counts, P.chunk_offs, P.view_count * P.object_chunks, s_tmp);
     stamp(P, 3);
     phase_expand(P, sm);
-    grid_sync(P);
-    stamp(P, 4);
+}
 
+// Phases 4..6 as a second cooperative launch: the meshlet tests need fewer registers
+// than the select, so this kernel runs more warps per SM. The kernel boundary is the
+// barrier after the expansion.
+__global__ void __launch_bounds__(kBatchThreads, 4) batch_cull_kernel(BatchParams P) {
+    extern __shared__ __align__(16) char sm[];
+    uint32_t* s_tmp = reinterpret_cast<uint32_t*>(sm + kSm2Misc);
+    stamp(P, 4);
     const uint32_t total_spans = min(ld_cg(P.view_span_start + P.view_count), P.span_capacity);
     const uint32_t groups = total_spans >> 5;
     phase_test(P, groups, sm);
@@ -1057,21 +1067,42 @@ uint32_t batch_max_grid() {
     return (uint32_t)(sms * per_sm);
 }
 
-cudaError_t launch_batch(const BatchParams& p, uint32_t grid, cudaStream_t stream) {
-    cudaError_t e = cudaFuncSetAttribute(batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmTotal);
-    if (e != cudaSuccess) return e;
+uint32_t batch_cull_max_grid() {
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_cull_kernel, kBatchThreads, kSm2Total);
+    return (uint32_t)(sms * per_sm);
+}
+
+namespace {
+
+cudaError_t launch_coop(const void* fn, uint32_t grid, size_t smem, const BatchParams& p, cudaStream_t stream) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid);
     cfg.blockDim = dim3(kBatchThreads);
-    cfg.dynamicSmemBytes = kSmTotal;
+    cfg.dynamicSmemBytes = smem;
     cfg.stream = stream;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeCooperative;
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
+    void* args[] = {const_cast<BatchParams*>(&p)};
+    return cudaLaunchKernelExC(&cfg, fn, args);
+}
+
+}  // namespace
+
+cudaError_t launch_batch(const BatchParams& p, uint32_t grid, uint32_t cull_grid, cudaStream_t stream) {
+    cudaError_t e = cudaFuncSetAttribute(batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmTotal);
+    if (e != cudaSuccess) return e;
     helio_launch_begin("batch_cull", stream);
-    e = cudaLaunchKernelEx(&cfg, batch_kernel, p);
+    e = launch_coop(reinterpret_cast<const void*>(batch_kernel), grid, kSmTotal, p, stream);
+    if (e == cudaSuccess) {
+        helio_launch_note();
+        e = launch_coop(reinterpret_cast<const void*>(batch_cull_kernel), cull_grid, kSm2Total, p, stream);
+    }
     helio_launch_end(stream);
     return e;
 }

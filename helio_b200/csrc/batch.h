@@ -91,9 +91,11 @@ cudaError_t launch_pack_draws(const BatchViewDev* views, uint32_t view_count, He
 
 // Dynamic shared memory of the persistent kernel (bytes).
 size_t batch_dynamic_smem();
-// Launches the cooperative kernel with `grid` CTAs (all co-resident) on `stream`.
-cudaError_t launch_batch(const BatchParams& p, uint32_t grid, cudaStream_t stream);
-// Largest co-resident grid for this device.
+// Launches the two cooperative kernels of a batch on `stream`: phases 0..3 with
+// `grid` CTAs, then phases 4..6 with `cull_grid` CTAs (each grid all co-resident).
+cudaError_t launch_batch(const BatchParams& p, uint32_t grid, uint32_t cull_grid, cudaStream_t stream);
+// Largest co-resident grids for this device (phases 0..3, phases 4..6).
 uint32_t batch_max_grid();
+uint32_t batch_cull_max_grid();
 
 }  // namespace helio

@@ -156,7 +156,7 @@ int32_t plan_batch(const helio_batch_config& cfg, const helio_vg_scene* sc, uint
     p.need[kBufChunkVis] = (units + 1) * 4;
     p.need[kBufVisList] = std::max<size_t>(1, units) * helio::kBatchChunk * sizeof(uint16_t);
     p.need[kBufChunkOffs] = (units + 1) * 4;
-    p.need[kBufSegTotals] = (size_t)p.grid * 4;
+    p.need[kBufSegTotals] = (size_t)std::max(p.grid, helio::batch_cull_max_grid()) * 4;
     p.need[kBufViewSpanStart] = (size_t)(n + 1) * 4;
     p.need[kBufSpans] = (size_t)p.span_capacity * sizeof(helio::ActiveSpan);
     p.need[kBufGroupCounts] = (groups + 1) * 4;
@@ -497,7 +497,10 @@ int32_t helio_batch_execute(helio_batch* b, void* stream) {
     P.span_vis = (b->cfg.flags & HELIO_BATCH_SPAN_VISIBILITY) ? b->span_vis.as<uint32_t>() : nullptr;
     P.phase_ns = b->stamps();
     const uint32_t grid = (b->cfg.max_ctas && b->cfg.max_ctas < b->grid) ? b->cfg.max_ctas : b->grid;
-    HELIO_CK(helio::launch_batch(P, grid, s));
+    // The cull kernel takes the same share of the device as the select kernel.
+    const uint32_t full = helio::batch_max_grid(), cull_full = helio::batch_cull_max_grid();
+    const uint32_t cull_grid = std::max(1u, (uint32_t)((uint64_t)cull_full * grid / std::max(1u, full)));
+    HELIO_CK(helio::launch_batch(P, grid, cull_grid, s));
     return HELIO_OK;
 }
 

@@ -71,6 +71,8 @@ void helio_launch_begin(const char* kernel, cudaStream_t stream) {
     cudaEventRecord(Profiler::open_start, stream);
 }
 
+void helio_launch_note(void) { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
 void helio_launch_end(cudaStream_t stream) {
     g_launches.fetch_add(1, std::memory_order_relaxed);
     if (!Profiler::open_start) return;

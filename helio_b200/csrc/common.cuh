@@ -224,5 +224,7 @@ constexpr uint32_t kSpinLimit = 1u << 22;  // polls before a bounded wait gives 
 // event profiler (helio_profiler_*): every launch is bracketed by these two calls.
 void helio_launch_begin(const char* kernel, cudaStream_t stream);
 void helio_launch_end(cudaStream_t stream);
+// Counts one more launch inside an open begin/end bracket (a step of several kernels).
+void helio_launch_note(void);
 // Records `message` as the calling thread's helio_last_error() and returns `code`.
 int32_t helio_report_error(int32_t code, const char* message);
