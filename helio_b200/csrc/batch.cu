@@ -610,44 +610,59 @@ __device__ void phase_expand(const BatchParams& P, char* sm) {
     const uint32_t gw = blockIdx.x * (kBatchThreads / 32) + warp, GW = gridDim.x * (kBatchThreads / 32);
     // Units are dealt out strided (lane k of warp w looks at unit w + k * W) so that the
     // heavy consecutive chunks of a large view spread over many warps.
+    // A warp takes 32 units at a time (lane l: unit w + (k0 + l) * W) and flattens
+    // their visible lists into one sequence: round r gives lane i the entry
+    // 32 r + i, so the list and object loads of every unit are in flight together
+    // (two round trips per round instead of two per unit). The spans of an entry go to
+    // its unit's first span + the spans of the unit's earlier entries: a scan of the
+    // span counts within the round, less the scan before the unit's first entry in the
+    // round, plus what the unit wrote in earlier rounds (carried by the unit's lane).
     for (uint32_t k0 = 0; gw + (size_t)k0 * GW < n_units; k0 += 32u) {
         const size_t u = gw + (size_t)(k0 + lane) * GW;
-        // Units with visible objects (the only ones that can have spans).
-        const uint32_t busy = u < n_units ? ld_cg(P.chunk_vis + u) : 0u;
-        uint32_t mask = __ballot_sync(0xffffffffu, busy != 0u);
-        while (mask) {
-            const uint32_t src_lane = __ffs(mask) - 1;
-            const uint32_t uu = gw + (k0 + src_lane) * GW;
-            const uint32_t vis = __shfl_sync(0xffffffffu, busy, src_lane);
-            mask &= mask - 1u;
-            const uint32_t v = uu / C, ch = uu - v * C;
-            uint32_t pos = s_vstart[v] + (ld_cg(P.chunk_offs + uu) - ld_cg(P.chunk_offs + (size_t)v * C));
-            // Round trip 1: the chunk's visible list (slot | LOD << 8, object order);
-            // round trip 2: the visible objects' selected ranges.
-            const uint16_t* list = P.vis_list + (size_t)uu * kBatchChunk;
-            for (uint32_t base = 0; base < vis; base += 32u) {
-                const uint32_t i = base + lane;
-                uint32_t count = 0, first = 0, inst = 0, lod = 0, o = 0;
-                if (i < vis) {
-                    const uint32_t e = __ldcg(list + i);
-                    lod = e >> 8;
-                    o = ch * kBatchChunk + (e & 0xFFu);
-                    const HelioGpuVgObject* obj = S.objects + o;
-                    count = __ldg(&obj->lod_meshlet_counts[lod]);
-                    first = __ldg(&obj->lod_first_meshlets[lod]);
-                    inst = __ldg(&obj->instance_index);
-                }
-                const uint32_t ns = (count + 63u) >> 6;
-                const uint32_t inc = warp_inclusive(ns);
-                uint32_t p = pos + inc - ns;
-                for (uint32_t j = 0; j < ns; ++j, ++p) {
-                    if (p < P.span_capacity) {
-                        const uint32_t n = min(64u, count - 64u * j);
-                        P.spans[p] = make_uint4(first + 64u * j, n | (lod << 8) | (v << 16), inst, o);
-                    }
-                }
-                pos += __shfl_sync(0xffffffffu, inc, 31);
+        const bool live = u < n_units;
+        const uint32_t vis = live ? ld_cg(P.chunk_vis + u) : 0u;
+        if (!__any_sync(0xffffffffu, vis != 0u)) continue;
+        const uint32_t v = live ? (uint32_t)(u / C) : 0u, ch = live ? (uint32_t)(u - (size_t)v * C) : 0u;
+        uint32_t pos = 0;  // the unit's first span in the view-major list
+        if (vis) pos = s_vstart[v] + (ld_cg(P.chunk_offs + u) - ld_cg(P.chunk_offs + (size_t)v * C));
+        const uint32_t inc_vis = warp_inclusive(vis);
+        const uint32_t first_e = inc_vis - vis, total = __shfl_sync(0xffffffffu, inc_vis, 31);
+        uint32_t written = 0;  // spans this lane's unit has written in earlier rounds
+        for (uint32_t base = 0; base < total; base += 32u) {
+            const uint32_t e = base + lane;
+            const int j = owner_lane(first_e, e);  // the unit (lane) owning entry e
+            const uint32_t jfirst = __shfl_sync(0xffffffffu, first_e, j);
+            const uint32_t jv = __shfl_sync(0xffffffffu, v, j), jch = __shfl_sync(0xffffffffu, ch, j);
+            const uint32_t jpos = __shfl_sync(0xffffffffu, pos, j), jdone = __shfl_sync(0xffffffffu, written, j);
+            const size_t ju = gw + (size_t)(k0 + (uint32_t)j) * GW;
+            uint32_t count = 0, first = 0, inst = 0, lod = 0, o = 0;
+            if (e < total) {
+                const uint32_t en = __ldcg(P.vis_list + ju * kBatchChunk + (e - jfirst));
+                lod = en >> 8;
+                o = jch * kBatchChunk + (en & 0xFFu);
+                const HelioGpuVgObject* obj = S.objects + o;
+                count = __ldg(&obj->lod_meshlet_counts[lod]);
+                first = __ldg(&obj->lod_first_meshlets[lod]);
+                inst = __ldg(&obj->instance_index);
             }
+            const uint32_t ns = (count + 63u) >> 6;
+            const uint32_t inc = warp_inclusive(ns);
+            // Lane of the unit's first entry in this round, and the scan before it.
+            const uint32_t lead = jfirst > base ? jfirst - base : 0u;
+            // Every lane takes part in the shuffle (its source differs per lane).
+            const uint32_t inc_before_lead = __shfl_sync(0xffffffffu, inc, lead ? lead - 1u : 0u);
+            const uint32_t before = lead ? inc_before_lead : 0u;
+            uint32_t p = jpos + jdone + (inc - ns - before);
+            for (uint32_t q = 0; q < ns; ++q, ++p) {
+                if (p < P.span_capacity)
+                    P.spans[p] = make_uint4(first + 64u * q, min(64u, count - 64u * q) | (lod << 8) | (jv << 16), inst, o);
+            }
+            // Each unit's lane adds the spans its entries wrote in this round.
+            const uint32_t lo = first_e > base ? first_e - base : 0u;
+            const uint32_t end = inc_vis > base ? min(inc_vis - base, 32u) : 0u;  // one past the unit's last lane here
+            const uint32_t at_end = __shfl_sync(0xffffffffu, inc, end ? end - 1u : 0u);
+            const uint32_t at_lo = __shfl_sync(0xffffffffu, inc, lo ? lo - 1u : 0u);
+            if (vis && end > lo && lo < 32u) written += at_end - (lo ? at_lo : 0u);
         }
     }
     // Padding spans (n = 0) complete every view to a multiple of 32.

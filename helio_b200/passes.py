@@ -269,9 +269,10 @@ class BatchedCull:
     (Hi-Z of each view, object LOD select for every (object, view), meshlet cull and
     per-view deterministic compaction)."""
 
-    def __init__(self, max_views: int = N.HELIO_BATCH_MAX_VIEWS, span_visibility: bool = False, max_spans: int = 0):
+    def __init__(self, max_views: int = N.HELIO_BATCH_MAX_VIEWS, span_visibility: bool = False, max_spans: int = 0,
+                 max_ctas: int = 0):
         self._lib = N.cull_lib()
-        cfg = N.BatchConfig(max_views, N.HELIO_BATCH_SPAN_VISIBILITY if span_visibility else 0, max_spans)
+        cfg = N.BatchConfig(max_views, N.HELIO_BATCH_SPAN_VISIBILITY if span_visibility else 0, max_spans, max_ctas)
         h = C.c_void_p()
         N.check(self._lib.helio_batch_create(C.byref(cfg), C.byref(h)))
         self._h = h

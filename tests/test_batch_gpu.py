@@ -10,7 +10,7 @@ from oracle import oracle as O
 pytestmark = pytest.mark.gpu
 
 
-def run_batch(scene, views, span_visibility=True, alias=False, capacities=None, repeats=1):
+def run_batch(scene, views, span_visibility=True, alias=False, capacities=None, repeats=1, max_ctas=0):
     import torch
     from helio_b200 import scene as S
     from helio_b200.passes import BatchedCull, VgScene
@@ -18,7 +18,7 @@ def run_batch(scene, views, span_visibility=True, alias=False, capacities=None, 
     vs = VgScene()
     vs.upload(S.frame_data(scene))
     depths = [torch.from_numpy(np.ascontiguousarray(v.depth)).cuda() for v in views]
-    b = BatchedCull(len(views), span_visibility=span_visibility)
+    b = BatchedCull(len(views), span_visibility=span_visibility, max_ctas=max_ctas)
     specs = []
     for i, (v, d) in enumerate(zip(views, depths)):
         spec = {"camera": v.camera, "depth": d, "alias_mip0": alias, "lod_threshold_px": v.lod_threshold_px}
@@ -192,3 +192,15 @@ def test_pack_draws_matches_per_view_outputs(cuda):
     torch.cuda.synchronize()
     assert off.cpu().numpy()[-1] == small
     np.testing.assert_array_equal(u32(ind2), np.concatenate([p["indirect"] for p in per])[:small])
+
+
+@pytest.mark.parametrize("ctas", [1, 7])
+def test_batch_small_grid_matches_oracle(cuda, ctas):
+    """A grid of a few CTAs gives every warp many units in every phase (multi-round
+    span expansion over 32 chunks at a time, many Hi-Z and select units per CTA)."""
+    from helio_b200 import scene as S
+
+    w = S.config(3, scale=0.05)
+    views = w.views[:1] + w.views[1:5] + w.views[5:9] + w.views[21:30]
+    _check_batch(w, views, max_ctas=ctas)
+
