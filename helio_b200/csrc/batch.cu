@@ -53,12 +53,10 @@ struct SelBox {
 
 // Dynamic shared memory layout (bytes).
 constexpr uint32_t kSelectMaxViews = 32;  // views per select unit, at most
-constexpr uint32_t kSelQueue = 64;        // candidate (view, lane) slots per warp
 constexpr size_t kSmSelViews = 0;                                               // SelView[kBatchMaxViews]
 constexpr size_t kSmSelBox = kSmSelViews + sizeof(SelView) * kBatchMaxViews;    // SelBox[kBatchMaxViews]
 constexpr size_t kSmSelLod = kSmSelBox + sizeof(SelBox) * kBatchMaxViews;       // u8[kSelectMaxViews][256]
-constexpr size_t kSmSelQueue = kSmSelLod + kSelectMaxViews * kBatchChunk;       // u16[8][kSelQueue]
-constexpr size_t kSmSelSpans = kSmSelQueue + 2 * 8 * kSelQueue;                 // u32[kSelectMaxViews]
+constexpr size_t kSmSelSpans = kSmSelLod + kSelectMaxViews * kBatchChunk;       // u32[kSelectMaxViews]
 constexpr size_t kSmSelMask = kSmSelSpans + 4 * kSelectMaxViews;                // u32[kSelectMaxViews][8]
 constexpr size_t kSmSelStats = kSmSelMask + 4 * 8 * kSelectMaxViews;             // u32[kSelectMaxViews][9]
 constexpr size_t kSmHizJob = kSmSelStats + 4 * 9 * kSelectMaxViews;             // HizJob
@@ -392,28 +390,28 @@ __device__ void phase_hiz_tile(const BatchParams& P, uint32_t tile, char* sm) {
 
 // ── Phase 1b: object select against a group of views (vg_cull.wgsl:282-352) ──
 // Unit = (256-object chunk, group of at most kSelectMaxViews views); lane j of warp
-// w holds object chunk * 256 + 32 w + j. For each view of the group the warp tests
-// the world centres against the view's reject box (broadcast from shared memory)
-// and queues the (view, lane) pairs the box does not reject; every 32 queued pairs
-// are tested exactly, one pair per lane (select_batch). The selected LOD + 1 of the
+// w holds object chunk * 256 + 32 w + j. Each lane tests its object's world centre
+// against the reject boxes of all views of the group (broadcast from shared memory)
+// into a bit mask; the warp's (object, view) pairs that pass are then flattened in
+// lane-major order and tested exactly, 32 pairs at a time, one pair per lane
+// (select_batch). The selected LOD + 1 of the
 // unit's pairs collects in a shared tile (zero = culled) that is written out row by
 // row; spans and visible objects per view are counted with shared atomics.
 
-// Exact sphere test and LOD walk of n <= 32 queued pairs (vg_cull.wgsl:315-336).
-__device__ void select_batch(const BatchParams& P, uint32_t chunk, uint32_t v_begin, const uint16_t* queue,
-                             uint32_t n, F3 c, float wr, float max_scale, char* sm) {
+// Exact sphere test and LOD walk of the pair (view v_begin + k, object of lane j) on
+// each active lane (vg_cull.wgsl:315-336). Every lane of the warp calls it.
+__device__ void select_batch(const BatchParams& P, uint32_t chunk, uint32_t v_begin, bool active, uint32_t k,
+                             uint32_t j, F3 c, float wr, float max_scale, char* sm) {
     const SelView* s_sv = reinterpret_cast<const SelView*>(sm + kSmSelViews);
     uint8_t* s_lod = reinterpret_cast<uint8_t*>(sm + kSmSelLod);
     uint32_t* s_spans = reinterpret_cast<uint32_t*>(sm + kSmSelSpans);
     uint32_t* s_vmask = reinterpret_cast<uint32_t*>(sm + kSmSelMask);
     uint32_t* s_stats = reinterpret_cast<uint32_t*>(sm + kSmSelStats);
-    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-    const uint32_t e = lane < n ? (uint32_t)queue[lane] : lane;
-    const uint32_t j = e & 31u, k = e >> 5;
+    const uint32_t warp = threadIdx.x >> 5;
     const F3 cj = f3(__shfl_sync(0xffffffffu, c.x, j), __shfl_sync(0xffffffffu, c.y, j),
                      __shfl_sync(0xffffffffu, c.z, j));
     const float wrj = __shfl_sync(0xffffffffu, wr, j), msj = __shfl_sync(0xffffffffu, max_scale, j);
-    if (lane >= n) return;
+    if (!active) return;
     const SelView& sv = s_sv[v_begin + k];
     if (!sphere_visible_vg(sv.planes, cj, wrj)) return;
     const uint32_t slot = warp * 32u + j;
@@ -531,33 +529,35 @@ __device__ void phase_select_chunk(const BatchParams& P, uint32_t chunk, uint32_
     uint32_t* s_stats = reinterpret_cast<uint32_t*>(sm + kSmSelStats);
     for (uint32_t i = tid; i < nv * 9u; i += kBatchThreads) s_stats[i] = 0u;
     __syncthreads();
-    uint16_t* q = reinterpret_cast<uint16_t*>(sm + kSmSelQueue) + warp * kSelQueue;
-    const uint32_t lt = (1u << lane) - 1u;
-    uint32_t qn = 0;  // warp-uniform
-    for (uint32_t k = 0; k < nv; ++k) {
-        const SelBox& b = s_box[v_begin + k];
-        // NaN centres are never rejected here; the exact test decides them.
-        const bool out = c.x < b.lo[0] || c.x > b.hi[0] || c.y < b.lo[1] || c.y > b.hi[1] || c.z < b.lo[2] ||
-                         c.z > b.hi[2];
-        const bool pass = valid && !out;
-        const uint32_t bal = __ballot_sync(0xffffffffu, pass);
-        if (pass) q[qn + __popc(bal & lt)] = (uint16_t)((k << 5) | lane);
-        qn += __popc(bal);
-        if (qn >= 32u) {
-            __syncwarp();
-            select_batch(P, chunk, v_begin, q, 32u, c, wr, max_scale, sm);
-            __syncwarp();
-            const uint32_t rest = qn - 32u;
-            const uint16_t x = lane < rest ? q[32u + lane] : (uint16_t)0;
-            __syncwarp();
-            if (lane < rest) q[lane] = x;
-            __syncwarp();
-            qn = rest;
+    // Bit k of hits: the box of view v_begin + k does not reject this object. The
+    // views' tests are independent of one another, so they pipeline. NaN centres are
+    // never rejected here; the exact test decides them.
+    uint32_t hits = 0;
+    if (valid) {
+        const float4* bx = reinterpret_cast<const float4*>(s_box + v_begin);  // lo.xyz hi.x | hi.yz pad
+#pragma unroll 4
+        for (uint32_t k = 0; k < nv; ++k) {
+            const float4 a = bx[2 * k], b = bx[2 * k + 1];
+            const bool out = (c.x < a.x) | (c.x > a.w) | (c.y < a.y) | (c.y > b.x) | (c.z < a.z) | (c.z > b.y);
+            hits |= (out ? 0u : 1u) << k;
         }
     }
-    if (qn) {
-        __syncwarp();
-        select_batch(P, chunk, v_begin, q, qn, c, wr, max_scale, sm);
+    const uint32_t hit_count = __popc(hits);
+    const uint32_t hit_inc = warp_inclusive(hit_count);
+    const uint32_t total = __shfl_sync(0xffffffffu, hit_inc, 31);
+    for (uint32_t base = 0; base < total; base += 32u) {
+        const uint32_t i = base + lane;
+        // Owner lane j of pair i: the number of lanes whose inclusive count is <= i
+        // (binary search over the non-decreasing counts; at most 31 when i < total).
+        uint32_t j = 0;
+#pragma unroll
+        for (uint32_t step = 16; step; step >>= 1)
+            if (__shfl_sync(0xffffffffu, hit_inc, j + step - 1u) <= i) j += step;
+        const uint32_t hj = __shfl_sync(0xffffffffu, hits, j);
+        const uint32_t before = __shfl_sync(0xffffffffu, hit_inc - hit_count, j);
+        const bool active = i < total;
+        const uint32_t k = active ? select_bit(hj, i - before) : 0u;
+        select_batch(P, chunk, v_begin, active, k, j, c, wr, max_scale, sm);
     }
     __syncthreads();
     for (uint32_t i = tid; i < nv * kRow4; i += kBatchThreads) {
