@@ -53,6 +53,7 @@ struct SelBox {
 
 // Dynamic shared memory layout (bytes).
 constexpr uint32_t kSelectMaxViews = 32;  // views per select unit, at most
+static_assert(kSelectMaxViews * 8 <= kBatchThreads, "one thread per (view, mask word) in the write-out");
 constexpr size_t kSmSelViews = 0;                                               // SelView[kBatchMaxViews]
 constexpr size_t kSmSelBox = kSmSelViews + sizeof(SelView) * kBatchMaxViews;    // SelBox[kBatchMaxViews]
 constexpr size_t kSmSelLod = kSmSelBox + sizeof(SelBox) * kBatchMaxViews;       // u8[kSelectMaxViews][256]
@@ -457,41 +458,42 @@ __device__ __forceinline__ uint32_t select_bit(uint32_t x, uint32_t r) {
     return p;
 }
 
-// The visible objects of view v in a chunk, in object order, by one warp: entry i
-// = slot | LOD << 8 of the i-th set bit of the chunk's 256-bit mask (lane i of
-// round i / 32 finds it from the words' bit counts, scanned over lanes 0..7).
-__device__ void select_write_list(const BatchParams& P, uint32_t chunk, uint32_t v, const uint8_t* row,
-                                  const uint32_t* mask, const uint32_t* stats, uint32_t spans) {
-    const uint32_t lane = threadIdx.x & 31u;
-    // The unit's share of counters 2..9 (LOD histogram) and 10 (largest lod_count - 1).
-    if (lane < 9u && stats[lane]) {
-        uint32_t* counters = P.views[v].counters;
-        if (lane < 8u) atomicAdd(counters + 2 + lane, stats[lane]);
-        else atomicMax(counters + 10, stats[8] - 1u);
-    }
-    const uint32_t word = lane < 8u ? mask[lane] : 0u;
-    const uint32_t wc = __popc(word);
-    const uint32_t winc = warp_inclusive(wc);
-    const uint32_t visible = __shfl_sync(0xffffffffu, winc, 7);
-    const size_t u = (size_t)v * P.object_chunks + chunk;
-    uint16_t* list = P.vis_list + u * kBatchChunk;
-    for (uint32_t base = 0; base < visible; base += 32u) {
-        const uint32_t i = base + lane;
-        uint32_t w = 0;  // the word of the i-th set bit: words whose inclusive count is <= i
+// The visible objects of the unit's views, in object order: thread t takes mask word
+// w = t % 8 of view k = t / 8 (nv <= 32 views, so nv * 8 <= 256 threads) and writes
+// entry slot | LOD << 8 for each set bit of the word, after the entries of the view's
+// words 0..w-1 (a scan over the view's 8 lanes). The last word's thread writes the
+// (view, chunk) counts; the view's lanes add the unit's share of counters 2..9 (LOD
+// histogram) and 10 (largest lod_count - 1).
+__device__ void select_write_lists(const BatchParams& P, uint32_t chunk, uint32_t v_begin, uint32_t nv,
+                                   const uint8_t* s_lod, const uint32_t* s_vmask, const uint32_t* s_stats,
+                                   const uint32_t* s_spans) {
+    const uint32_t tid = threadIdx.x, k = tid >> 3, w = tid & 7u;
+    const bool has = k < nv;
+    const uint32_t m = has ? s_vmask[k * 8u + w] : 0u;
+    const uint32_t c = __popc(m);
+    uint32_t inc = c;
 #pragma unroll
-        for (uint32_t q = 0; q < 8u; ++q) w += __shfl_sync(0xffffffffu, winc, q) <= i ? 1u : 0u;
-        w = min(w, 7u);
-        const uint32_t before = __shfl_sync(0xffffffffu, winc - wc, w);
-        const uint32_t wd = __shfl_sync(0xffffffffu, word, w);
-        if (i < visible) {
-            const uint32_t slot = w * 32u + select_bit(wd, i - before);
-            list[i] = (uint16_t)(slot | ((uint32_t)(row[slot] - 1u) << 8));
-        }
+    for (uint32_t d = 1; d < 8u; d <<= 1) {
+        const uint32_t x = __shfl_up_sync(0xffffffffu, inc, d, 8);
+        if (w >= d) inc += x;
     }
-    if (lane == 0) {
-        P.chunk_counts[u] = spans;
-        P.chunk_vis[u] = visible;
+    if (!has) return;
+    const uint32_t v = v_begin + k;
+    const size_t u = (size_t)v * P.object_chunks + chunk;
+    uint16_t* list = P.vis_list + u * kBatchChunk + (inc - c);
+    const uint8_t* row = s_lod + k * kBatchChunk;
+    for (uint32_t left = m, i = 0; left; left &= left - 1u, ++i) {
+        const uint32_t slot = w * 32u + (uint32_t)(__ffs(left) - 1);
+        list[i] = (uint16_t)(slot | ((uint32_t)(row[slot] - 1u) << 8));
     }
+    if (w == 7u) {
+        P.chunk_counts[u] = s_spans[k];
+        P.chunk_vis[u] = inc;
+    }
+    const uint32_t* st = s_stats + k * 9u;
+    uint32_t* counters = P.views[v].counters;
+    if (st[w]) atomicAdd(counters + 2 + w, st[w]);
+    if (w == 0u && st[8]) atomicMax(counters + 10, st[8] - 1u);
 }
 
 __device__ void phase_select_chunk(const BatchParams& P, uint32_t chunk, uint32_t v_begin, uint32_t v_end, char* sm) {
@@ -499,7 +501,7 @@ __device__ void phase_select_chunk(const BatchParams& P, uint32_t chunk, uint32_
     uint4* s_lod4 = reinterpret_cast<uint4*>(sm + kSmSelLod);
     uint32_t* s_spans = reinterpret_cast<uint32_t*>(sm + kSmSelSpans);
     uint32_t* s_vmask = reinterpret_cast<uint32_t*>(sm + kSmSelMask);
-    const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5, nv = v_end - v_begin;
+    const uint32_t tid = threadIdx.x, lane = tid & 31u, nv = v_end - v_begin;
     const VgSceneDev& S = P.scene;
     const uint32_t o = chunk * kBatchChunk + tid;
     bool valid = false;
@@ -565,10 +567,8 @@ __device__ void phase_select_chunk(const BatchParams& P, uint32_t chunk, uint32_
         *reinterpret_cast<uint4*>(P.lod + (size_t)(v_begin + k) * P.lod_pitch + chunk * kBatchChunk + w4 * 16u) =
             s_lod4[i];
     }
-    const uint8_t* s_lod = reinterpret_cast<const uint8_t*>(sm + kSmSelLod);
-    for (uint32_t k = warp; k < nv; k += kBatchThreads / 32)
-        select_write_list(P, chunk, v_begin + k, s_lod + k * kBatchChunk, s_vmask + k * 8u, s_stats + k * 9u,
-                          s_spans[k]);
+    select_write_lists(P, chunk, v_begin, nv, reinterpret_cast<const uint8_t*>(sm + kSmSelLod), s_vmask,
+                       reinterpret_cast<const uint32_t*>(sm + kSmSelStats), s_spans);
 }
 
 // ── Phase 3: expansion into the view-major list of active spans ──────────────
