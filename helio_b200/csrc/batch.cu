@@ -71,10 +71,10 @@ constexpr size_t kSmTestBits = kSmTestViews + sizeof(CullView) * 8;      // u32[
 constexpr int kBits = kWindowsPerWarp + 2;
 constexpr size_t kSmTestQueue = kSmTestBits + 8 * kBits * 4;            // u16[8][64]
 constexpr size_t kSmVStart = 0;                                          // u32[kBatchMaxViews + 1]
-static_assert(kSmTestQueue + 8 * 64 * 2 <= kSmMisc, "test phase fits");
+constexpr size_t kSmTestSpheres = ((kSmTestQueue + 8 * 64 * 2) + 15) / 16 * 16;  // float4[8][64]
 // The cull kernel (phases 4..6) has its own, small layout: the test phase's region
 // from offset 0, then the scan scratch.
-constexpr size_t kSm2Misc = ((kSmTestQueue + 8 * 64 * 2) + 15) / 16 * 16;  // u32[64]
+constexpr size_t kSm2Misc = kSmTestSpheres + 8 * 64 * 16;  // u32[64]
 constexpr size_t kSm2Total = kSm2Misc + 64 * 4;
 
 __device__ __forceinline__ uint32_t ld_cg(const uint32_t* p) { return __ldcg(p); }
@@ -694,24 +694,16 @@ __device__ __forceinline__ GroupSpans load_group(const BatchParams& P, uint32_t 
 }
 
 // ── Phase 4: meshlet tests of every group of 32 spans ────────────────────────
-// Hi-Z tests of n <= 32 queued candidates of a group (lane i takes entry i, a
-// meshlet position s of the group); visible ones set bit s of the group's bits.
-__device__ void test_hiz_batch(const VgSceneDev& S, const CullView& cv, const GroupSpans& gs, const uint16_t* q,
-                               uint32_t n, uint32_t* bits) {
+// Hi-Z tests of n <= 32 queued candidates of a group: lane i takes entry i, a
+// meshlet position s of the group with the world sphere the frustum test computed;
+// visible ones set bit s of the group's bits.
+__device__ void test_hiz_batch(const CullView& cv, const uint16_t* q, const float4* spheres, uint32_t n,
+                               uint32_t* bits) {
     const uint32_t lane = threadIdx.x & 31u;
-    const uint32_t s = lane < n ? (uint32_t)q[lane] : 0u;
-    const int j = owner_lane(gs.off, s);
-    const uint32_t j_off = __shfl_sync(0xffffffffu, gs.off, j);
-    const uint32_t j_first = __shfl_sync(0xffffffffu, gs.first, j);
-    const uint32_t j_inst = __shfl_sync(0xffffffffu, gs.inst, j);
     if (lane >= n) return;
-    const uint32_t mi = j_first + (s - j_off);
-    const HelioInstanceCullData cd = load_cull(S.cull + j_inst);
-    const Mat4 model = ldg_mat4(S.instances[j_inst].model);
-    F3 c;
-    float wr;
-    meshlet_sphere(S, mi, model, cd, c, wr);
-    if (meshlet_hiz_visible<true>(cv, c, wr)) atomicOr(bits + (s >> 5), 1u << (s & 31u));
+    const uint32_t s = q[lane];
+    const float4 sp = spheres[lane];
+    if (meshlet_hiz_visible<true>(cv, f3(sp.x, sp.y, sp.z), sp.w)) atomicOr(bits + (s >> 5), 1u << (s & 31u));
 }
 
 // Per group of 32 spans, the warp runs the frustum and cone tests window by window
@@ -723,6 +715,7 @@ __device__ void phase_test(const BatchParams& P, uint32_t groups, char* sm) {
     CullView& cv = *reinterpret_cast<CullView*>(sm + kSmTestViews + sizeof(CullView) * warp);
     uint32_t* bits = reinterpret_cast<uint32_t*>(sm + kSmTestBits) + warp * kBits;
     uint16_t* q = reinterpret_cast<uint16_t*>(sm + kSmTestQueue) + warp * 64;
+    float4* qs = reinterpret_cast<float4*>(sm + kSmTestSpheres) + warp * 64;
     const uint32_t lt = (1u << lane) - 1u;
     const VgSceneDev& S = P.scene;
     uint32_t cached_view = 0xFFFFFFFFu;
@@ -747,35 +740,44 @@ __device__ void phase_test(const BatchParams& P, uint32_t groups, char* sm) {
             const uint32_t j_first = __shfl_sync(0xffffffffu, gs.first, j);
             const uint32_t j_inst = __shfl_sync(0xffffffffu, gs.inst, j);
             bool cand = false;
+            F3 c = f3(0.f, 0.f, 0.f);
+            float wr = 0.0f;
             if (s < gs.total) {
                 const uint32_t mi = j_first + (s - j_off);
                 if (mi < S.meshlet_count) {
                     const HelioGpuInstanceData* in = S.instances + j_inst;
                     const HelioInstanceCullData cd = load_cull(S.cull + j_inst);
                     const Mat4 model = ldg_mat4(in->model);
-                    F3 c;
-                    float wr;
                     cand = meshlet_frustum_cone(cv, load_meshlet(S, mi, in), model, cd, c, wr);
                 }
             }
             const uint32_t b = __ballot_sync(0xffffffffu, cand);
-            if (cand) q[qn + __popc(b & lt)] = (uint16_t)s;
+            if (cand) {
+                const uint32_t at = qn + __popc(b & lt);
+                q[at] = (uint16_t)s;
+                qs[at] = make_float4(c.x, c.y, c.z, wr);
+            }
             qn += __popc(b);
             if (qn >= 32u) {
                 __syncwarp();
-                test_hiz_batch(S, cv, gs, q, 32u, bits);
+                test_hiz_batch(cv, q, qs, 32u, bits);
                 __syncwarp();
                 const uint32_t rest = qn - 32u;
-                const uint16_t x = (uint32_t)lane < rest ? q[32 + lane] : (uint16_t)0;
+                const bool mv = (uint32_t)lane < rest;
+                const uint16_t x = mv ? q[32 + lane] : (uint16_t)0;
+                const float4 xs = mv ? qs[32 + lane] : make_float4(0.f, 0.f, 0.f, 0.f);
                 __syncwarp();
-                if ((uint32_t)lane < rest) q[lane] = x;
+                if (mv) {
+                    q[lane] = x;
+                    qs[lane] = xs;
+                }
                 __syncwarp();
                 qn = rest;
             }
         }
         if (qn) {
             __syncwarp();
-            test_hiz_batch(S, cv, gs, q, qn, bits);
+            test_hiz_batch(cv, q, qs, qn, bits);
         }
         __syncwarp();
         uint32_t count = __popc(bits[lane]) + __popc(bits[lane + 32]);
