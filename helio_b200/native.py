@@ -115,6 +115,21 @@ class SceneBuffers(C.Structure):
                 ("draw_count", u32), ("aabbs", vp), ("indirect", vp)]
 
 
+class VgMeshRecord(C.Structure):
+    """HelioVgMeshRecord: a library mesh whose descriptors are pool[first_meshlet, +meshlet_count)."""
+    _fields_ = [("first_meshlet", u32), ("meshlet_count", u32), ("lod_count", u32), ("max_meshlet_count", u32),
+                ("local_bounds", f32 * 4), ("lod_errors", f32 * 8), ("lod_first_meshlets", u32 * 8),
+                ("lod_meshlet_counts", u32 * 8)]
+
+
+class VgBuildInputs(C.Structure):
+    _fields_ = [("pool", vp), ("meshes", vp), ("slot_mesh", vp), ("slot_instances", vp), ("pool_count", u32),
+                ("mesh_count", u32), ("slot_count", u32), ("reserved0", u32)]
+
+
+VG_NO_MESH = 0xFFFFFFFF
+
+
 class VgFrameData(C.Structure):
     _fields_ = [("meshlets", vp), ("objects", vp), ("instances", vp), ("work_items", vp),
                 ("meshlet_count", u32), ("object_count", u32), ("work_item_count", u32), ("max_draw_count", u32),
@@ -270,6 +285,10 @@ CULL_EXPORTS = {
     "helio_serve_stats_get": (i32, [vp, C.POINTER(ServeStats)]),
     "helio_serve_plan_batch": (i32, [C.POINTER(ServePending), u32, u32, u32, C.POINTER(u32), C.POINTER(u32)]),
     "helio_serve_destroy": (None, [vp]),
+    "helio_vg_builder_create": (i32, [C.POINTER(vp)]),
+    "helio_vg_builder_run": (i32, [vp, C.POINTER(VgBuildInputs), vp]),
+    "helio_vg_builder_frame_data": (i32, [vp, C.POINTER(VgFrameData)]),
+    "helio_vg_builder_destroy": (None, [vp]),
 }
 
 _cull = None

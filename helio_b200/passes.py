@@ -240,6 +240,56 @@ class VgScene:
             self._h = None
 
 
+class VgBuilder:
+    """The VG input producer (helio_vg_builder): rebuild_vg_buffers on the device, from a
+    descriptor pool, mesh records and dense object slots held in device memory
+    (crates/helio/src/scene/virtual_geometry/rebuild.rs:98-172)."""
+
+    def __init__(self):
+        self._lib = N.cull_lib()
+        h = C.c_void_p()
+        N.check(self._lib.helio_vg_builder_create(C.byref(h)))
+        self._h = h
+
+    def run(self, pool: torch.Tensor, meshes: torch.Tensor, slot_mesh: torch.Tensor, slot_instances: torch.Tensor,
+            stream=None) -> N.VgFrameData:
+        """Byte tensors on the device (64 B per descriptor, 128 B per mesh record, u32 per
+        slot, 144 B per slot instance). Returns the outputs as device frame data."""
+        for t in (pool, meshes, slot_mesh, slot_instances):
+            assert t.is_cuda and t.is_contiguous()
+        inp = N.VgBuildInputs(_ptr(pool), _ptr(meshes), _ptr(slot_mesh), _ptr(slot_instances),
+                              pool.numel() * pool.element_size() // C.sizeof(N.GpuMeshletEntry),
+                              meshes.numel() * meshes.element_size() // C.sizeof(N.VgMeshRecord),
+                              slot_mesh.numel() * slot_mesh.element_size() // 4, 0)
+        assert slot_instances.numel() * slot_instances.element_size() == inp.slot_count * C.sizeof(N.GpuInstanceData)
+        N.check(self._lib.helio_vg_builder_run(self._h, C.byref(inp), _stream_ptr(stream)))
+        return self.frame_data()
+
+    def frame_data(self) -> N.VgFrameData:
+        out = N.VgFrameData()
+        N.check(self._lib.helio_vg_builder_frame_data(self._h, C.byref(out)))
+        return out
+
+    def outputs(self) -> dict:
+        """The last run's arrays as device byte tensors (aliasing the builder's buffers)."""
+        f = self.frame_data()
+
+        def view(ptr, n, size):
+            return device_view(ptr, (max(n, 1) * size,), "|u1")[: n * size] if n else torch.empty(0, dtype=torch.uint8)
+
+        return {"meshlets": view(f.meshlets, f.meshlet_count, C.sizeof(N.GpuMeshletEntry)),
+                "objects": view(f.objects, f.object_count, C.sizeof(N.GpuVgObject)),
+                "instances": view(f.instances, f.object_count, C.sizeof(N.GpuInstanceData)),
+                "work_items": view(f.work_items, f.work_item_count, C.sizeof(N.GpuVgWorkItem)),
+                "max_draw_count": f.max_draw_count}
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            self._lib.helio_vg_builder_destroy(h)
+            self._h = None
+
+
 def batch_views(views: list):
     """helio_batch_view array of view dicts (camera, device depth H x W float32, optional
     lod_threshold_px, draw_capacity, alias_mip0)."""

@@ -262,6 +262,54 @@ def work_items_for(objects) -> list:
     return out
 
 
+DT_MESH = np.dtype(N.np_dtype(N.VgMeshRecord))
+
+
+@dataclass
+class Library:
+    """Input of the VG input producer: a descriptor pool, mesh records and dense object
+    slots (mesh index, VG_NO_MESH for a free slot, and instance data)."""
+    pool: np.ndarray
+    meshes: np.ndarray
+    slot_mesh: np.ndarray
+    slot_instances: np.ndarray
+
+
+def library_from_scene(scene: Scene, free_slots: float = 0.0, seed: int = 1) -> Library:
+    """Mesh library whose rebuild gives back the scene's objects: one record per distinct
+    (descriptor range, LOD table) of the scene's objects, the scene's meshlets as the
+    pool, and one slot per object in order, with free slots mixed in at rate free_slots."""
+    obj = scene.objects
+    lc = np.minimum(obj["lod_count"], 8).astype(np.int64)
+    used = np.arange(8)[None, :] < lc[:, None]
+    firsts = obj["lod_first_meshlets"].astype(np.int64)
+    counts = obj["lod_meshlet_counts"].astype(np.int64)
+    big = np.int64(1) << 40
+    first = np.where(used, firsts, big).min(axis=1)
+    end = np.where(used, firsts + counts, 0).max(axis=1)
+    first = np.where(lc > 0, first, 0)
+    rec = np.zeros(len(obj), DT_MESH)
+    rec["first_meshlet"] = first
+    rec["meshlet_count"] = np.where(lc > 0, end - first, 0)
+    rec["lod_count"] = obj["lod_count"]
+    rec["max_meshlet_count"] = obj["max_meshlet_count"]
+    rec["local_bounds"] = obj["local_bounds"]
+    rec["lod_errors"] = obj["lod_errors"]
+    rec["lod_first_meshlets"] = np.where(used, firsts - first[:, None], 0)
+    rec["lod_meshlet_counts"] = obj["lod_meshlet_counts"]
+    meshes, mesh_of = np.unique(rec.view(np.dtype((np.void, DT_MESH.itemsize))), return_inverse=True)
+    meshes = meshes.view(DT_MESH)
+    mesh_of = mesh_of.astype(np.uint32).reshape(-1)
+    rng = np.random.default_rng(seed)
+    n_free = int(round(free_slots * len(obj)))
+    slot_mesh = np.full(len(obj) + n_free, N.VG_NO_MESH, np.uint32)
+    slot_inst = np.zeros(len(obj) + n_free, DT_INSTANCE)
+    taken = np.sort(rng.choice(len(slot_mesh), size=len(obj), replace=False)) if n_free else np.arange(len(obj))
+    slot_mesh[taken] = mesh_of
+    slot_inst[taken] = scene.instances
+    return Library(scene.meshlets, meshes, slot_mesh, slot_inst)
+
+
 def frame_data(scene: Scene, buffer_version: int = 1, instance_version: int = 1, dirty=(0, 0),
                device: dict | None = None) -> N.VgFrameData:
     """VgFrameData over host arrays (or device tensors when `device` holds them)."""

@@ -623,6 +623,58 @@ int32_t helio_serve_plan_batch(const helio_serve_pending* queue, uint32_t n, uin
                                uint32_t max_requests, uint32_t* chosen, uint32_t* count);
 void helio_serve_destroy(helio_serve* server);
 
+/* ════════════════════════════════════════════════════════════════════════════
+ * VG input producer: rebuild_vg_buffers on the device
+ *   (crates/helio/src/scene/virtual_geometry/rebuild.rs:18-58, 98-172)
+ *
+ * Input, in device memory: a descriptor pool holding the meshlets of every mesh of
+ * a library, the library's mesh records, and the scene's dense object slots (each
+ * slot's mesh and instance data). Output, in device memory: the VgFrameData arrays
+ * of the reference's rebuild (each referenced mesh's descriptors once, in
+ * first-reference order; one object and one instance per slot whose mesh exists
+ * and has descriptors and LODs; 64-meshlet work items) and max_draw_count, ready
+ * for helio_vg_scene_upload / helio_vg_prepare with memory = HELIO_MEM_DEVICE.
+ * ════════════════════════════════════════════════════════════════════════════ */
+
+#define HELIO_VG_NO_MESH 0xFFFFFFFFu /* slot_mesh of a free slot (any value >= mesh_count acts alike) */
+
+/* VirtualMeshRecord (crates/helio/src/scene/types.rs:211-236); its descriptors are
+ * pool[first_meshlet .. first_meshlet + meshlet_count). 128 bytes. */
+typedef struct HelioVgMeshRecord {
+    uint32_t first_meshlet;
+    uint32_t meshlet_count;
+    uint32_t lod_count;
+    uint32_t max_meshlet_count;
+    float local_bounds[4];
+    float lod_errors[HELIO_VG_LOD_LEVELS];
+    uint32_t lod_first_meshlets[HELIO_VG_LOD_LEVELS]; /* relative to the mesh's first descriptor */
+    uint32_t lod_meshlet_counts[HELIO_VG_LOD_LEVELS];
+} HelioVgMeshRecord;
+
+typedef struct helio_vg_build_inputs {
+    const HelioGpuMeshletEntry* pool;           /* device */
+    const HelioVgMeshRecord* meshes;            /* device */
+    const uint32_t* slot_mesh;                  /* device, [slot_count] */
+    const HelioGpuInstanceData* slot_instances; /* device, [slot_count] */
+    uint32_t pool_count;
+    uint32_t mesh_count;
+    uint32_t slot_count;
+    uint32_t reserved0;
+} helio_vg_build_inputs;
+
+typedef struct helio_vg_builder helio_vg_builder;
+int32_t helio_vg_builder_create(helio_vg_builder** out);
+/* Rebuilds the frame data from `in` on `stream` and waits for it (the totals are
+ * read back once to size the outputs). HELIO_ERR_INVALID_ARG when a used mesh's
+ * descriptor range leaves the pool, or when a count, max_draw_count or an LOD
+ * descriptor offset exceeds u32 (where the reference panics); the previous outputs
+ * are then gone. The outputs stay valid until the next run or destroy. */
+int32_t helio_vg_builder_run(helio_vg_builder* builder, const helio_vg_build_inputs* in, void* stream);
+/* The last run's outputs as frame data: device pointers, memory = HELIO_MEM_DEVICE,
+ * buffer_version and instance_version = the number of successful runs, no dirty range. */
+int32_t helio_vg_builder_frame_data(const helio_vg_builder* builder, helio_vg_frame_data* out);
+void helio_vg_builder_destroy(helio_vg_builder* builder);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

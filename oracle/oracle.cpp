@@ -703,4 +703,67 @@ void oracle_vg_cull(const HelioGpuCameraUniforms* cam, const oracle_vg_uniforms*
     if (st) st->meshlets_visible += slot;
 }
 
+
+// rebuild_vg_buffers, crates/helio/src/scene/virtual_geometry/rebuild.rs:98-172, with
+// append_unique_meshlets (:18-43) and append_work_items (:45-58). A slot whose mesh
+// index is not below mesh_count stands for a free dense slot or a missing mesh record
+// (both skipped by the reference, :110-129).
+int oracle_vg_rebuild(const HelioGpuMeshletEntry* pool, uint32_t pool_count, const HelioVgMeshRecord* meshes,
+                      uint32_t mesh_count, const uint32_t* slot_mesh, const HelioGpuInstanceData* slot_instances,
+                      uint32_t slot_count, HelioGpuMeshletEntry* out_meshlets, HelioGpuVgObject* out_objects,
+                      HelioGpuInstanceData* out_instances, HelioGpuVgWorkItem* out_items, uint64_t counts[4]) {
+    const uint64_t kU32 = 0xFFFFFFFFull;
+    std::vector<int64_t> base(mesh_count, -1);
+    uint64_t descriptors = 0;
+    // append_unique_meshlets over the referenced meshes in dense order (:25-40).
+    for (uint32_t o = 0; o < slot_count; ++o) {
+        const uint32_t m = slot_mesh[o];
+        if (m >= mesh_count || base[m] >= 0) continue;
+        const HelioVgMeshRecord& r = meshes[m];
+        if (r.meshlet_count == 0 || r.lod_count == 0) continue;
+        if ((uint64_t)r.first_meshlet + r.meshlet_count > pool_count) return 1;
+        if (descriptors > kU32) return 1;  // u32::try_from(output.len()) (:36-37)
+        base[m] = (int64_t)descriptors;
+        if (out_meshlets)
+            std::memcpy(out_meshlets + descriptors, pool + r.first_meshlet, sizeof(HelioGpuMeshletEntry) * r.meshlet_count);
+        descriptors += r.meshlet_count;
+    }
+    if (descriptors > kU32) return 1;  // meshlet_count = u32::try_from(len) (vg_frame_data, :72-73)
+    uint64_t objects = 0, items = 0, draws = 0;
+    for (uint32_t o = 0; o < slot_count; ++o) {
+        const uint32_t m = slot_mesh[o];
+        if (m >= mesh_count || base[m] < 0) continue;  // :124-129
+        const HelioVgMeshRecord& r = meshes[m];
+        HelioGpuVgObject ob;
+        ob.instance_index = (uint32_t)objects;  // instance and object indices advance together (:131-134)
+        ob.lod_count = r.lod_count;
+        ob.max_meshlet_count = r.max_meshlet_count;
+        ob.reserved = 0;
+        for (int k = 0; k < 4; ++k) ob.local_bounds[k] = r.local_bounds[k];
+        for (int l = 0; l < HELIO_VG_LOD_LEVELS; ++l) {
+            const uint64_t first = (uint64_t)base[m] + r.lod_first_meshlets[l];  // checked_add (:137-139)
+            if (first > kU32) return 1;
+            ob.lod_errors[l] = r.lod_errors[l];
+            ob.lod_first_meshlets[l] = (uint32_t)first;
+            ob.lod_meshlet_counts[l] = r.lod_meshlet_counts[l];
+        }
+        if (out_objects) out_objects[objects] = ob;
+        if (out_instances) out_instances[objects] = slot_instances[o];
+        // append_work_items: (object, 0), (object, 64), ... below max_meshlet_count (:45-58).
+        for (uint64_t b = 0; b < r.max_meshlet_count; b += HELIO_VG_MESHLETS_PER_WORK_ITEM) {
+            if (out_items) out_items[items] = HelioGpuVgWorkItem{(uint32_t)objects, (uint32_t)b};
+            ++items;
+        }
+        draws += r.max_meshlet_count;  // checked_add (:158-161)
+        if (draws > kU32) return 1;
+        ++objects;
+    }
+    if (items > kU32) return 1;  // work_item_count = u32::try_from(len) (:76-77)
+    counts[0] = descriptors;
+    counts[1] = objects;
+    counts[2] = items;
+    counts[3] = draws;
+    return 0;
+}
+
 }  // extern "C"

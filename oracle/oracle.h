@@ -92,6 +92,17 @@ void oracle_vg_cull(const HelioGpuCameraUniforms* cam, const oracle_vg_uniforms*
                     HelioGpuVgDraw* draws, uint32_t* counters, uint32_t* visibility,
                     oracle_stats* st, int threads);
 
+/* rebuild_vg_buffers (crates/helio/src/scene/virtual_geometry/rebuild.rs:18-58,
+ * 98-172) over a mesh library and dense object slots, sequentially in the reference's
+ * order. counts receives {descriptors, objects, work items, max_draw_count}; null
+ * output arrays skip the writes (a counting pass). Returns 0, or 1 where the
+ * reference panics (a count, max_draw_count or an LOD offset beyond u32) or a used
+ * mesh's descriptors leave the pool. */
+int oracle_vg_rebuild(const HelioGpuMeshletEntry* pool, uint32_t pool_count, const HelioVgMeshRecord* meshes,
+                      uint32_t mesh_count, const uint32_t* slot_mesh, const HelioGpuInstanceData* slot_instances,
+                      uint32_t slot_count, HelioGpuMeshletEntry* out_meshlets, HelioGpuVgObject* out_objects,
+                      HelioGpuInstanceData* out_instances, HelioGpuVgWorkItem* out_items, uint64_t counts[4]);
+
 /* Single decisions, for the reference's known-answer tests. */
 /* sphere_visible (vg_cull.wgsl:126-133) against six given planes. */
 int oracle_sphere_visible(const float planes[24], const float center[3], float radius);

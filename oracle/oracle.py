@@ -86,6 +86,8 @@ def lib() -> C.CDLL:
         L.oracle_cone_reject.restype = C.c_int
         L.oracle_hiz_occludes.argtypes = [f32, f32]
         L.oracle_hiz_occludes.restype = C.c_int
+        L.oracle_vg_rebuild.argtypes = [vp, u32, vp, u32, vp, vp, u32, vp, vp, vp, vp, C.POINTER(C.c_uint64)]
+        L.oracle_vg_rebuild.restype = C.c_int
         _lib = L
     return _lib
 
@@ -206,3 +208,29 @@ def run_view(scene, cam, width: int, height: int, levels: list, lod_threshold: f
     n = int(min(counters[0], cap))
     return {"selected": selected, "counters": counters, "indirect": indirect[:n], "draws": draws[:n],
             "visibility": vis[:W], "stats": st, "cull": cull}
+
+
+def vg_rebuild(pool: np.ndarray, meshes: np.ndarray, slot_mesh: np.ndarray, slot_instances: np.ndarray):
+    """rebuild_vg_buffers over a mesh library (numpy arrays of GpuMeshletEntry, VgMeshRecord,
+    u32 and GpuInstanceData). Returns a dict of the output arrays and max_draw_count, or None
+    where the reference panics."""
+    from helio_b200 import native as N
+
+    L = lib()
+    pool, meshes = np.ascontiguousarray(pool), np.ascontiguousarray(meshes)
+    slot_mesh = np.ascontiguousarray(slot_mesh, dtype=np.uint32)
+    slot_instances = np.ascontiguousarray(slot_instances)
+    counts = (C.c_uint64 * 4)()
+    args = (pool.ctypes.data, len(pool), meshes.ctypes.data, len(meshes), slot_mesh.ctypes.data,
+            slot_instances.ctypes.data, len(slot_mesh))
+    if L.oracle_vg_rebuild(*args, None, None, None, None, counts):
+        return None
+    out = {"meshlets": np.zeros(counts[0], N.np_dtype(N.GpuMeshletEntry)),
+           "objects": np.zeros(counts[1], N.np_dtype(N.GpuVgObject)),
+           "instances": np.zeros(counts[1], N.np_dtype(N.GpuInstanceData)),
+           "work_items": np.zeros(counts[2], N.np_dtype(N.GpuVgWorkItem))}
+    rc = L.oracle_vg_rebuild(*args, out["meshlets"].ctypes.data, out["objects"].ctypes.data,
+                             out["instances"].ctypes.data, out["work_items"].ctypes.data, counts)
+    assert rc == 0
+    out["max_draw_count"] = int(counts[3])
+    return out

@@ -100,6 +100,21 @@ def main(ref: Path) -> None:
     kats["work_spans"] = {"objects": [[3, 0], [5, 1], [7, 64], [11, 65], [13, 130]],
                           "expected": [[5, 0], [7, 0], [11, 0], [11, 64], [13, 0], [13, 64], [13, 128]],
                           "at": f"{reb}:234-259"}
+    # append_unique_meshlets: records 3 -> descriptors with first_index 11, 12 and 7 -> 20,
+    # referenced as [3, 3, 7, 3, 7] (the test's helper gives every record one LOD).
+    text = (ref / reb).read_text()
+    t0 = text.index("fn repeated_instances_share_one_descriptor_copy")
+    body = text[t0: text.index("#[test]", t0)]
+    ids = dict(re.findall(r"let (\w+) = VirtualMeshId\((\d+)\);", body))
+    recs = {ids[n]: [int(x) for x in re.findall(r"meshlet\((\d+)\)", lst)]
+            for n, lst in re.findall(r"\((\w+), record\(vec!\[([^\]]*)\]\)\)", body)}
+    refs = [int(ids[n]) for n in re.search(r"\[((?:\w+,\s*)+\w+)\],\s*&records", body).group(1).replace(" ", "").split(",")]
+    first_idx = [int(x) for x in re.search(r"\.collect::<Vec<_>>\(\),\s*\[([\d,\s]+)\]", body).group(1).split(",")]
+    bases = {ids[n]: int(v) for n, v in re.findall(r"assert_eq!\(bases\[&(\w+)\],\s*(\d+)\)", body)}
+    line = text[:t0].count("\n") + 1
+    kats["unique_meshlets"] = {"meshes": {k: v for k, v in recs.items()}, "references": refs,
+                               "expected_first_index": first_idx, "bases": bases,
+                               "at": f"{reb}:{line}-{line + body.count(chr(10))}"}
     kats["layout_sizes"] = {"GpuMeshletEntry": 64, "GpuVgObject": 128, "GpuVgDraw": 16, "GpuVgWorkItem": 8,
                             "InstanceCullData": 16, "CullUniforms": 48, "IndirectCullUniforms": 112,
                             "DrawIndexedIndirect": 20, "GpuInstanceData": 144, "GpuCameraUniforms": 368,

@@ -114,3 +114,68 @@ def benchmark_scene(objects, per_object):
     sc = S.Scene(m, obj, inst, items, np.zeros(objects, S.DT_AABB), np.zeros(objects, S.DT_DRAWCALL),
                  objects * per_object, per_object)
     return sc, S.View(cam, 1920, 1080, np.ones((1, 1), np.float32))
+
+
+def random_library(seed: int, pool: int = 500, meshes: int = 40, slots: int = 600, max_count: int = 300):
+    """A mesh library with the cases the rebuild skips or shares: free slots, indices past
+    the table, meshes without descriptors or without LODs, repeated references."""
+    from helio_b200 import native as N
+    from helio_b200 import scene as S
+
+    rng = np.random.default_rng(seed)
+    p = np.frombuffer(rng.integers(0, 2**32, size=pool * 16, dtype=np.uint32).tobytes(), S.DT_MESHLET).copy()
+    m = np.zeros(meshes, S.DT_MESH)
+    m["meshlet_count"] = rng.integers(0, 40, meshes)
+    m["meshlet_count"][rng.random(meshes) < 0.15] = 0
+    m["first_meshlet"] = rng.integers(0, pool - m["meshlet_count"] + 1)
+    m["lod_count"] = rng.integers(0, 9, meshes)
+    m["lod_count"][rng.random(meshes) < 0.15] = 0
+    m["max_meshlet_count"] = rng.integers(0, max_count, meshes)
+    m["local_bounds"] = rng.normal(size=(meshes, 4)).astype(np.float32)
+    m["lod_errors"] = rng.random((meshes, 8)).astype(np.float32)
+    m["lod_first_meshlets"] = rng.integers(0, 1000, (meshes, 8))
+    m["lod_meshlet_counts"] = rng.integers(0, 100, (meshes, 8))
+    sm = rng.integers(0, meshes, slots).astype(np.uint32)
+    r = rng.random(slots)
+    sm[r < 0.1] = N.VG_NO_MESH
+    sm[(r >= 0.1) & (r < 0.15)] = meshes + rng.integers(0, 5, int(((r >= 0.1) & (r < 0.15)).sum()))
+    inst = np.frombuffer(rng.integers(0, 2**32, size=slots * 36, dtype=np.uint32).tobytes(), S.DT_INSTANCE).copy()
+    return S.Library(p, m, sm, inst)
+
+
+def kat_unique_meshlets_library(k: dict):
+    """rebuild.rs repeated_instances_share_one_descriptor_copy as a library: mesh ids in
+    ascending order become indices; the test's helper record has one LOD of one meshlet."""
+    from helio_b200 import scene as S
+
+    ids = sorted(k["meshes"], key=int)
+    pool = np.zeros(sum(len(v) for v in k["meshes"].values()), S.DT_MESHLET)
+    m = np.zeros(len(ids), S.DT_MESH)
+    at = 0
+    for i, mid in enumerate(ids):
+        fi = k["meshes"][mid]
+        pool["first_index"][at:at + len(fi)] = fi
+        pool["index_count"][at:at + len(fi)] = 3
+        m[i]["first_meshlet"], m[i]["meshlet_count"] = at, len(fi)
+        at += len(fi)
+    m["lod_count"] = 1
+    m["max_meshlet_count"] = 1
+    m["local_bounds"] = (0.0, 0.0, 0.0, 1.0)
+    m["lod_meshlet_counts"] = 1
+    slots = np.array([ids.index(str(r)) for r in k["references"]], np.uint32)
+    inst = np.zeros(len(slots), S.DT_INSTANCE)
+    return S.Library(pool, m, slots, inst), ids
+
+
+def kat_work_spans_library(k: dict):
+    """rebuild.rs work_items_cover_exact_fixed_meshlet_spans as a library: one used mesh
+    per listed object with its max_meshlet_count, one slot each, in order."""
+    from helio_b200 import scene as S
+
+    n = len(k["objects"])
+    pool = np.zeros(1, S.DT_MESHLET)
+    m = np.zeros(n, S.DT_MESH)
+    m["meshlet_count"] = 1
+    m["lod_count"] = 1
+    m["max_meshlet_count"] = [mx for _, mx in k["objects"]]
+    return S.Library(pool, m, np.arange(n, dtype=np.uint32), np.zeros(n, S.DT_INSTANCE))

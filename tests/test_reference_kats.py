@@ -125,6 +125,29 @@ def test_work_spans():
     assert [list(x) for x in work_items_for(k["objects"])] == k["expected"]
 
 
+def test_unique_meshlets_on_the_oracle():
+    from helpers import kat_unique_meshlets_library
+
+    k = KATS["unique_meshlets"]
+    lib, ids = kat_unique_meshlets_library(k)
+    out = O.vg_rebuild(lib.pool, lib.meshes, lib.slot_mesh, lib.slot_instances)
+    assert out["meshlets"]["first_index"].tolist() == k["expected_first_index"]
+    bases = [k["bases"][str(r)] for r in k["references"]]
+    assert out["objects"]["lod_first_meshlets"][:, 0].tolist() == bases
+
+
+def test_work_spans_on_the_oracle():
+    from helpers import kat_work_spans_library
+
+    k = KATS["work_spans"]
+    lib = kat_work_spans_library(k)
+    out = O.vg_rebuild(lib.pool, lib.meshes, lib.slot_mesh, lib.slot_instances)
+    ids = [obj for obj, _ in k["objects"]]
+    got = [[ids[i["object_index"]], int(i["local_meshlet_base"])] for i in out["work_items"]]
+    assert got == k["expected"]
+    assert out["max_draw_count"] == sum(mx for _, mx in k["objects"])
+
+
 def test_layout_sizes():
     from helio_b200 import native as N
 
