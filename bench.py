@@ -21,6 +21,9 @@ Workloads
                       40 GB HBM budget and batched continuously (helio_serve); reports
                       p50/p99 latency beside meshlets/s, and the same stream served one
                       request at a time through the plain single-view passes.
+  vgbuild             the VG input producer: rebuild_vg_buffers on the device for the
+                      largest serving scene (1.77M instance slots + 5% free slots over a
+                      library of 256 meshes); slots rebuilt per second.
 
 `value` is measured with inputs resident in HBM, the step replayed as a CUDA graph,
 CUDA events on the launching stream, L2 flushed between timed steps. `e2e` runs the
@@ -58,7 +61,7 @@ def parse_args():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
-    ap.add_argument("--workload", default="batched3", choices=["batched3", "plain2", "plain1", "plain0", "serve4"])
+    ap.add_argument("--workload", default="batched3", choices=["batched3", "plain2", "plain1", "plain0", "serve4", "vgbuild"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="batched3: skip the per-view plain comparison")
@@ -851,9 +854,167 @@ def cpu_baseline(wl, seconds: float) -> dict:
                       f"multi-threaded select / cull), {dt:.1f} s", "seconds": dt}
 
 
+# ── vgbuild: the VG input producer ────────────────────────────────────────────
+
+VGBUILD_FREE_SLOTS = 0.05
+
+
+def vgbuild_library():
+    from helio_b200 import scene as S
+
+    counts = S.serving_counts()
+    k = max(range(len(counts)), key=lambda i: counts[i])
+    return S.library_from_scene(S.serving_scene(k), free_slots=VGBUILD_FREE_SLOTS, seed=7), counts[k]
+
+
+def vgbuild_bytes(lib, out) -> int:
+    """Algorithmic bytes of one rebuild: each slot's mesh index and instance read; each
+    mesh record read once; descriptors read and written; objects, instances and work
+    items written."""
+    return int(lib.slot_mesh.nbytes + lib.slot_instances.nbytes + 128 * len(lib.meshes) +
+               2 * out["meshlets"].nbytes + out["objects"].nbytes + out["instances"].nbytes +
+               out["work_items"].nbytes)
+
+
+def vgbuild_cpu(lib, seconds: float, steps: int | None = None) -> tuple[float, int, float]:
+    """Oracle rebuilds of the library (single thread, as the reference's rebuild):
+    returns (slots/s, runs, total seconds)."""
+    from oracle import oracle as O
+
+    O.vg_rebuild(lib.pool, lib.meshes, lib.slot_mesh, lib.slot_instances)
+    t, runs = 0.0, 0
+    while (steps is None and (t < seconds or runs < 1)) or (steps is not None and runs < steps):
+        t0 = time.perf_counter()
+        O.vg_rebuild(lib.pool, lib.meshes, lib.slot_mesh, lib.slot_instances)
+        t += time.perf_counter() - t0
+        runs += 1
+    return len(lib.slot_mesh) * runs / t, runs, t
+
+
+def run_build(args, rank, world, local_rank):
+    import torch
+    from helio_b200 import dist as D
+    from helio_b200 import native as N
+    from helio_b200.passes import VgBuilder
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    lib_n = N.cull_lib()
+    lib, instances = vgbuild_library()
+
+    def up(a):
+        return torch.from_numpy(np.ascontiguousarray(a).view(np.uint8).reshape(-1).copy()).to(dev)
+
+    d = [up(lib.pool), up(lib.meshes), up(lib.slot_mesh), up(lib.slot_instances)]
+    b = VgBuilder()
+
+    def step():
+        b.run(*d)
+
+    step()
+    torch.cuda.synchronize()
+    out = {k: (v.cpu().numpy() if hasattr(v, "cpu") else v) for k, v in b.outputs().items()}
+    launches0 = lib_n.helio_kernel_launch_count()
+    step()
+    launches_per_step = lib_n.helio_kernel_launch_count() - launches0
+    timer = Timer(dev)
+    clocks = Clocks(local_rank)
+    if world > 1:
+        torch.distributed.barrier()
+    clocks.start()
+    # The rebuild reads its totals back once (to size its outputs): eager, not a graph.
+    step_ms, _ = timer.run(step, args.steps, args.warmup, graph=False)
+    clk = clocks.stop()
+    total_ms = D.max_over_ranks(sum(step_ms), dev)
+    slots = len(lib.slot_mesh)
+    value = slots * args.steps * world / (total_ms / 1e3)
+
+    lib_n.helio_profiler_reset()
+    lib_n.helio_profiler_enable(1)
+    for _ in range(args.steps):
+        timer.flush()
+        step()
+    torch.cuda.synchronize()
+    lib_n.helio_profiler_enable(0)
+    prof = N.profiler_collect()
+    lib_n.helio_profiler_reset()
+    n, ms = prof["vg_build"]
+    alg = vgbuild_bytes(lib, out)
+    achieved = alg / (ms / n / 1e3) / 1e9
+    peak, peak_kind = peaks()
+    tfile = ROOT / "profiles" / "dram_traffic.json"
+    traffic = json.loads(tfile.read_text()).get("vgbuild", {}).get("vg_build") if tfile.exists() else None
+    roofline = {"bound": "hbm", "kernel": "vg_build", "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
+                "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                "note": "the six launches of one rebuild and its two read-backs (totals, error word), between one "
+                        "pair of CUDA events"}
+
+    e2e = None
+    if not args.no_e2e:
+        # The per-frame part (slot arrays) copied in from pinned host memory each step;
+        # the pool and mesh records stay resident; then the rebuild.
+        hs = [torch.from_numpy(np.ascontiguousarray(a).view(np.uint8).reshape(-1).copy()).pin_memory()
+              for a in (lib.slot_mesh, lib.slot_instances)]
+
+        def run_e2e():
+            d[2].copy_(hs[0], non_blocking=True)
+            d[3].copy_(hs[1], non_blocking=True)
+            b.run(*d)
+
+        for _ in range(max(args.warmup, 3)):
+            run_e2e()
+        ee = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        for k in range(args.steps):
+            timer.flush()
+            ee[k][0].record()
+            run_e2e()
+            ee[k][1].record()
+        torch.cuda.synchronize()
+        e2e_ms = D.max_over_ranks(float(sum(a.elapsed_time(z) for a, z in ee)), dev)
+        e2e = {"value": slots * args.steps * world / (e2e_ms / 1e3), "unit": "slots/s",
+               "h2d_bytes_per_step": int(sum(h.numel() for h in hs)), "d2h_bytes_per_step": 48 + 4,
+               "ms_per_step": e2e_ms / args.steps,
+               "form": "slot arrays copied in from pinned host memory, then the rebuild (its totals and error "
+                       "word read back)"}
+    cpu = None
+    if rank == 0 and world == 1:
+        v, runs, t = vgbuild_cpu(lib, args.cpu_seconds)
+        cpu = {"value": v, "unit": "slots/s", "cores": 1, "kind": "port",
+               "sample": f"{runs} oracle rebuild(s) of the full library ({slots} slots), {t:.1f} s"}
+    return {
+        "metric": "VG slots rebuilt/s", "value": value, "unit": "slots/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded generator)",
+        "config": {"workload": f"vgbuild: the largest serving scene ({instances} instances x 100 LOD0 meshlets) as "
+                               f"{slots} dense slots ({VGBUILD_FREE_SLOTS:.0%} free) over {len(lib.meshes)} meshes "
+                               f"and {len(lib.pool)} pool descriptors",
+                   "outputs": {"descriptors": len(out["meshlets"]) // 64, "objects": len(out["objects"]) // 128,
+                               "work_items": len(out["work_items"]) // 8, "max_draw_count": out["max_draw_count"]},
+                   "l2": "flushed between timed steps (256 MB write, then 256 MB read)",
+                   "timing": "eager launches (the rebuild synchronises once to size its outputs), CUDA events on "
+                             "the launching stream",
+                   "parallelism": f"replica x{world}" if world > 1 else "single GPU"},
+        "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches_per_step * args.steps),
+        "clocks": clk,
+    }
+
+
 def run_reference(args):
     from helio_b200 import scene as S
 
+    if args.workload == "vgbuild":
+        lib, _ = vgbuild_library()
+        for _ in range(args.warmup):
+            vgbuild_cpu(lib, 0.0, steps=1)
+        v, runs, t = vgbuild_cpu(lib, 0.0, steps=args.steps)
+        return {"metric": "VG slots rebuilt/s", "value": v, "unit": "slots/s", "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / runs, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded generator)",
+                "impl": "reference", "config": {"workload": "vgbuild", "slots": len(lib.slot_mesh)},
+                "cpu_baseline": {"value": v, "unit": "slots/s", "cores": 1, "kind": "port",
+                                 "sample": "each step: one rebuild of the full library by the oracle's restatement "
+                                           "of rebuild_vg_buffers (single thread, as the reference)"},
+                "e2e": {"value": v, "unit": "slots/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     if args.workload == "serve4":
         # The reference has no serving loop; its per-view cull, restated, on the smallest
         # serving scene and the 85-view mix.
@@ -901,8 +1062,12 @@ def main():
         from helio_b200 import dist as D
 
         D.init("nccl", timeout_s=120)
-    line = run_serve(args, rank, world, local_rank) if args.workload == "serve4" else \
-        run_ours(args, rank, world, local_rank)
+    if args.workload == "serve4":
+        line = run_serve(args, rank, world, local_rank)
+    elif args.workload == "vgbuild":
+        line = run_build(args, rank, world, local_rank)
+    else:
+        line = run_ours(args, rank, world, local_rank)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

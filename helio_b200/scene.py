@@ -227,15 +227,23 @@ class ServeRequestSpec:
     views: list  # indices into the view pool
 
 
+def serving_counts(scale: float = 1.0) -> list:
+    """Instance counts of the serving workload's 8 scenes: log-uniform in [10k, 2M] (times `scale`)."""
+    rng = _Split(SEED_BASE + 4)
+    return [max(1, int(round(math.exp(rng.u(math.log(1e4), math.log(2e6))) * scale))) for _ in range(8)]
+
+
+def serving_scene(k: int, scale: float = 1.0, threads: int | None = None) -> Scene:
+    """Scene k of the serving workload: 100 LOD0 meshlets per instance, configs-1
+    distributions (uniform in a 200 m cube, log-uniform LOD errors); the instances draw
+    their meshes from a library of 256."""
+    n = serving_counts(scale)[k]
+    return make_scene(SEED_BASE + 5 + k, n, 100, 4, 0, 100.0, lod_error_mode=1, mesh_library=256, threads=threads)
+
+
 def serving_scenes(scale: float = 1.0, threads: int | None = None) -> list:
-    """The serving workload's 8 scenes: instance counts log-uniform in [10k, 2M] (times
-    `scale`), 100 LOD0 meshlets each, configs-1 distributions (uniform in a 200 m cube,
-    log-uniform LOD errors); the instances draw their meshes from a library of 256."""
-    seed = SEED_BASE + 4
-    rng = _Split(seed)
-    counts = [max(1, int(round(math.exp(rng.u(math.log(1e4), math.log(2e6))) * scale))) for _ in range(8)]
-    return [make_scene(seed + 1 + k, n, 100, 4, 0, 100.0, lod_error_mode=1, mesh_library=256, threads=threads)
-            for k, n in enumerate(counts)]
+    """The serving workload's 8 scenes (serving_scene 0..7)."""
+    return [serving_scene(k, scale, threads) for k in range(8)]
 
 
 def serving_requests(n: int, rate_hz: float = 2000.0, n_scenes: int = 8, pool: int = 85, max_views: int = 85,

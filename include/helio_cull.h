@@ -665,7 +665,8 @@ typedef struct helio_vg_build_inputs {
 typedef struct helio_vg_builder helio_vg_builder;
 int32_t helio_vg_builder_create(helio_vg_builder** out);
 /* Rebuilds the frame data from `in` on `stream` and waits for it (the totals are
- * read back once to size the outputs). HELIO_ERR_INVALID_ARG when a used mesh's
+ * read back once to size the outputs). pool, meshes and slot_instances must be
+ * 16-byte aligned. HELIO_ERR_INVALID_ARG when a used mesh's
  * descriptor range leaves the pool, or when a count, max_draw_count or an LOD
  * descriptor offset exceeds u32 (where the reference panics); the previous outputs
  * are then gone. The outputs stay valid until the next run or destroy. */

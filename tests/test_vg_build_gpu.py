@@ -56,6 +56,15 @@ def test_many_slots_shared_meshes(cuda):
     assert_same(host, ref)
 
 
+def test_large_library_takes_the_global_table(cuda):
+    # More meshes than the per-block shared table holds: the first references go straight
+    # to the one global table.
+    lib = random_library(12, pool=20000, meshes=9000, slots=40000, max_count=200)
+    ref = O.vg_rebuild(lib.pool, lib.meshes, lib.slot_mesh, lib.slot_instances)
+    _, host, _ = gpu_build(lib)
+    assert_same(host, ref)
+
+
 def test_reference_rebuild_tests(cuda):
     k = KATS["unique_meshlets"]
     lib, _ = kat_unique_meshlets_library(k)
