@@ -528,6 +528,7 @@ int32_t helio_vg_create(const helio_vg_config* config, helio_vg_pass** out) {
     HELIO_ARG(config->width > 0 && config->height > 0, "render size must be non-zero");
     HELIO_ARG(config->counter_count == 0 || config->counter_count == 2 || config->counter_count == 11,
               "counter_count must be 2 or 11");
+    HELIO_ARG((config->flags & ~HELIO_VG_CLEAR_INDIRECT) == 0, "unknown VG pass flags");
     helio_vg_pass* p = new (std::nothrow) helio_vg_pass();
     if (!p) return fail(HELIO_ERR_RESOURCE, "out of host memory");
     p->cfg = *config;
@@ -636,6 +637,8 @@ int32_t helio_vg_execute(helio_vg_pass* p, const HelioGpuCameraUniforms* camera_
     cudaStream_t s = as_stream(stream);
     uint32_t* scratch = p->scratch.as<uint32_t>();
     HELIO_CK(cudaMemsetAsync(p->scratch.ptr, 0, p->scratch_clear_bytes, s));
+    if (p->cfg.flags & HELIO_VG_CLEAR_INDIRECT)  // rendering.rs:1128-1130
+        HELIO_CK(cudaMemsetAsync(p->indirect.ptr, 0, (size_t)p->capacity * sizeof(HelioDrawIndexedIndirectArgs), s));
 
     helio::VgSceneDev scene{};
     scene.m_bounds = p->m_bounds.as<float4>();

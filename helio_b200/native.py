@@ -27,6 +27,7 @@ HELIO_ERR_BUDGET = 6
 HELIO_ERR_NOT_READY = 7
 HELIO_MEM_HOST = 0
 HELIO_MEM_DEVICE = 1
+HELIO_VG_CLEAR_INDIRECT = 1
 HELIO_HIZ_MAX_MIPS = 12
 HELIO_HIZ_ALIAS_MIP0 = 1
 HELIO_VG_COUNTER_COUNT = 11

@@ -475,9 +475,10 @@ class VirtualGeometryPass:
     """Virtual-geometry cull: object LOD select + meshlet cull + deterministic compaction."""
 
     def __init__(self, width: int, height: int, lod_quality: int = N.HELIO_LOD_MEDIUM, publication_limit: int = 0,
-                 counter_count: int = 11):
+                 counter_count: int = 11, clear_indirect: bool = False):
         self._lib = N.cull_lib()
-        cfg = N.VgConfig(width, height, lod_quality, publication_limit, counter_count, 0)
+        cfg = N.VgConfig(width, height, lod_quality, publication_limit, counter_count,
+                         N.HELIO_VG_CLEAR_INDIRECT if clear_indirect else 0)
         h = C.c_void_p()
         N.check(self._lib.helio_vg_create(C.byref(cfg), C.byref(h)))
         self._h = h

@@ -379,8 +379,16 @@ typedef struct helio_vg_config {
     uint32_t lod_quality;       /* HELIO_LOD_* */
     uint32_t publication_limit; /* 0 = HELIO_VG_DEFAULT_PUBLICATION_LIMIT */
     uint32_t counter_count;     /* 2 (benchmark layout) or 11 (production layout); 0 = 11 */
-    uint32_t flags;
+    uint32_t flags;             /* HELIO_VG_CLEAR_INDIRECT */
 } helio_vg_config;
+
+/* For a draw side without multi_draw_indexed_indirect_count: execute zeroes the whole
+ * indirect buffer before the cull, so that drawing all `capacity` records draws exactly
+ * the visible ones (the zeroed records are empty draws). The reference clears it when
+ * the device lacks the count feature (rendering.rs:1127-1130, 1203-1208). Without the
+ * flag only the first min(counters[0], capacity) records are defined: the count form
+ * reads the draw count from byte 0 of `counters` (rendering.rs:648-660, 1194-1201). */
+#define HELIO_VG_CLEAR_INDIRECT 1u
 
 /* Published outputs (device pointers owned by the pass). */
 typedef struct helio_vg_outputs {
