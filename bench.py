@@ -21,6 +21,9 @@ Workloads
                       40 GB HBM budget and batched continuously (helio_serve); reports
                       p50/p99 latency beside meshlets/s, and the same stream served one
                       request at a time through the plain single-view passes.
+  shadow              the per-face shadow cull: 100,000 movable draws against 44 dirty
+                      shadow faces (4 cascades, 16 spot lights, 4 point lights x 6 faces);
+                      draw-face tests per second.
   vgbuild             the VG input producer: rebuild_vg_buffers on the device for the
                       largest serving scene (1.77M instance slots + 5% free slots over a
                       library of 256 meshes); slots rebuilt per second.
@@ -61,7 +64,7 @@ def parse_args():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
-    ap.add_argument("--workload", default="batched3", choices=["batched3", "plain2", "plain1", "plain0", "serve4", "vgbuild"])
+    ap.add_argument("--workload", default="batched3", choices=["batched3", "plain2", "plain1", "plain0", "serve4", "vgbuild", "shadow"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="batched3: skip the per-view plain comparison")
@@ -999,8 +1002,134 @@ def run_build(args, rank, world, local_rank):
     }
 
 
+# ── shadow: the per-face shadow cull ──────────────────────────────────────────
+
+SHADOW_DRAWS = 100_000
+
+
+def shadow_workload():
+    """Faces and draws of the shadow workload (seeded synthetic inputs)."""
+    from helio_b200 import scene as S
+
+    mats, nf = S.shadow_faces(11)
+    inst, src = S.shadow_draws(11, SHADOW_DRAWS, SHADOW_DRAWS)
+    dirty = np.zeros(256, np.uint32)
+    dirty[:nf] = 1
+    return mats, nf, inst, src, dirty
+
+
+def shadow_cpu(mats, nf, inst, src, dirty, seconds: float, steps: int | None = None):
+    from oracle import oracle as O
+
+    t, runs = 0.0, 0
+    while (steps is None and (t < seconds or runs < 1)) or (steps is not None and runs < steps):
+        t0 = time.perf_counter()
+        O.shadow_cull(mats, inst, src, dirty, nf)
+        t += time.perf_counter() - t0
+        runs += 1
+    return len(src) * nf * runs / t, runs, t
+
+
+def run_shadow(args, rank, world, local_rank):
+    import torch
+    from helio_b200 import dist as D
+    from helio_b200 import native as N
+    from helio_b200.passes import ShadowCullPass
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    lib_n = N.cull_lib()
+    mats, nf, inst, src, dirty = shadow_workload()
+
+    def up(a):
+        return torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+
+    d = [up(mats), up(inst.view(np.uint8)), up(src.view(np.int32)), up(dirty.view(np.int32))]
+    p = ShadowCullPass()
+    p.prepare(*d, nf)
+    p.execute()
+    torch.cuda.synchronize()
+    visible = int(p.outputs()["face_counts"].cpu().numpy().view(np.uint32)[:nf].sum())
+    launches0 = lib_n.helio_kernel_launch_count()
+    p.execute()
+    launches_per_step = lib_n.helio_kernel_launch_count() - launches0
+    timer = Timer(dev)
+    clocks = Clocks(local_rank)
+    clocks.start()
+    step_ms, graphed = timer.run(p.execute, args.steps, args.warmup)
+    clk = clocks.stop()
+    total_ms = D.max_over_ranks(sum(step_ms), dev)
+    tests = len(src) * nf
+    value = tests * args.steps * world / (total_ms / 1e3)
+    # Algorithmic bytes: each draw's 20-byte record and its instance's 16-byte sphere
+    # read once, each visible (draw, face) record written (up to 4096 a face).
+    stored = int(np.minimum(p.outputs()["face_counts"].cpu().numpy().view(np.uint32)[:nf], 4096).sum())
+    alg = len(src) * 36 + stored * 20 + 256 * 4
+    achieved = alg / (total_ms / args.steps / 1e3) / 1e9
+    peak, peak_kind = peaks()
+    roofline = {"bound": "hbm", "kernel": "shadow_cull", "achieved": achieved, "peak": peak,
+                "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                "note": "three launches per step (graph replay); latency-bound at this size"}
+    e2e = None
+    if not args.no_e2e:
+        hs = torch.from_numpy(np.ascontiguousarray(src.view(np.int32))).pin_memory()
+        out_counts = torch.empty(256, dtype=torch.int32).pin_memory()
+
+        def run_e2e():
+            d[2].copy_(hs, non_blocking=True)
+            p.execute()
+            out_counts.copy_(p.outputs()["face_counts"], non_blocking=True)
+
+        for _ in range(max(args.warmup, 3)):
+            run_e2e()
+        ee = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        for k in range(args.steps):
+            timer.flush()
+            ee[k][0].record()
+            run_e2e()
+            ee[k][1].record()
+        torch.cuda.synchronize()
+        e2e_ms = D.max_over_ranks(float(sum(a.elapsed_time(z) for a, z in ee)), dev)
+        e2e = {"value": tests * args.steps * world / (e2e_ms / 1e3), "unit": "draw-face tests/s",
+               "h2d_bytes_per_step": int(hs.numel() * 4), "d2h_bytes_per_step": 256 * 4,
+               "ms_per_step": e2e_ms / args.steps,
+               "form": "the draw records copied in from pinned host memory, the cull, the 256 counts copied out"}
+    cpu = None
+    if rank == 0 and world == 1:
+        v, runs, t = shadow_cpu(mats, nf, inst, src, dirty, args.cpu_seconds)
+        cpu = {"value": v, "unit": "draw-face tests/s", "cores": 1, "kind": "port",
+               "sample": f"{runs} oracle run(s) of the full workload, {t:.1f} s"}
+    return {
+        "metric": "shadow draw-face tests/s", "value": value, "unit": "draw-face tests/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator)",
+        "config": {"workload": f"shadow: {len(src)} movable draws over {len(inst)} instances x {nf} dirty faces "
+                               "(4 orthographic cascades, 16 spot, 4 point lights x 6)",
+                   "visible_draw_faces": visible,
+                   "l2": "flushed between timed steps (256 MB write, then 256 MB read)",
+                   "timing": ("CUDA-graph replay" if graphed else "eager launches") + ", CUDA events",
+                   "parallelism": f"replica x{world}" if world > 1 else "single GPU"},
+        "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches_per_step * args.steps),
+        "clocks": clk,
+    }
+
+
 def run_reference(args):
     from helio_b200 import scene as S
+
+    if args.workload == "shadow":
+        mats, nf, inst, src, dirty = shadow_workload()
+        for _ in range(args.warmup):
+            shadow_cpu(mats, nf, inst, src, dirty, 0.0, steps=1)
+        v, runs, t = shadow_cpu(mats, nf, inst, src, dirty, 0.0, steps=args.steps)
+        return {"metric": "shadow draw-face tests/s", "value": v, "unit": "draw-face tests/s", "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / runs,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded generator)", "impl": "reference", "config": {"workload": "shadow"},
+                "cpu_baseline": {"value": v, "unit": "draw-face tests/s", "cores": 1, "kind": "port",
+                                 "sample": "each step: the full workload through the oracle's restatement of "
+                                           "shadow_cull.wgsl (single thread)"},
+                "e2e": {"value": v, "unit": "draw-face tests/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
     if args.workload == "vgbuild":
         lib, _ = vgbuild_library()
@@ -1066,6 +1195,8 @@ def main():
         line = run_serve(args, rank, world, local_rank)
     elif args.workload == "vgbuild":
         line = run_build(args, rank, world, local_rank)
+    elif args.workload == "shadow":
+        line = run_shadow(args, rank, world, local_rank)
     else:
         line = run_ours(args, rank, world, local_rank)
     if rank == 0:

@@ -131,6 +131,19 @@ class VgBuildInputs(C.Structure):
 VG_NO_MESH = 0xFFFFFFFF
 
 
+class ShadowCullInputs(C.Structure):
+    _fields_ = [("shadow_matrices", vp), ("instances", vp), ("src_indirect", vp), ("face_dirty", vp),
+                ("instance_count", u32), ("draw_count", u32), ("face_count", u32), ("reserved0", u32)]
+
+
+class ShadowCullOutputs(C.Structure):
+    _fields_ = [("face_indirect", vp), ("face_counts", vp), ("max_faces", u32), ("max_draws_per_face", u32)]
+
+
+SHADOW_MAX_FACES = 256
+SHADOW_MAX_DRAWS_PER_FACE = 4096
+
+
 class VgFrameData(C.Structure):
     _fields_ = [("meshlets", vp), ("objects", vp), ("instances", vp), ("work_items", vp),
                 ("meshlet_count", u32), ("object_count", u32), ("work_item_count", u32), ("max_draw_count", u32),
@@ -290,6 +303,11 @@ CULL_EXPORTS = {
     "helio_vg_builder_run": (i32, [vp, C.POINTER(VgBuildInputs), vp]),
     "helio_vg_builder_frame_data": (i32, [vp, C.POINTER(VgFrameData)]),
     "helio_vg_builder_destroy": (None, [vp]),
+    "helio_shadow_cull_create": (i32, [C.POINTER(vp)]),
+    "helio_shadow_cull_prepare": (i32, [vp, C.POINTER(ShadowCullInputs)]),
+    "helio_shadow_cull_execute": (i32, [vp, vp]),
+    "helio_shadow_cull_publish": (i32, [vp, C.POINTER(ShadowCullOutputs)]),
+    "helio_shadow_cull_destroy": (None, [vp]),
 }
 
 _cull = None

@@ -240,6 +240,48 @@ class VgScene:
             self._h = None
 
 
+class ShadowCullPass:
+    """Per-face shadow frustum cull (helio_shadow_cull_*; ShadowCullPass,
+    crates/helio-pass-shadow-cull/src/lib.rs:57-328)."""
+
+    def __init__(self):
+        self._lib = N.cull_lib()
+        h = C.c_void_p()
+        N.check(self._lib.helio_shadow_cull_create(C.byref(h)))
+        self._h = h
+
+    def name(self) -> str:
+        return "ShadowCull"
+
+    def prepare(self, matrices: torch.Tensor, instances: torch.Tensor, src_indirect: torch.Tensor,
+                face_dirty: torch.Tensor, face_count: int) -> None:
+        """Device tensors: matrices float32 [256, 16], instances bytes (144 per instance),
+        src_indirect int32 [n, 5], face_dirty int32 [256]."""
+        for t in (matrices, instances, src_indirect, face_dirty):
+            assert t.is_cuda and t.is_contiguous()
+        assert matrices.numel() == 256 * 16 and face_dirty.numel() == 256
+        self._keep = (matrices, instances, src_indirect, face_dirty)
+        inp = N.ShadowCullInputs(_ptr(matrices), _ptr(instances), _ptr(src_indirect), _ptr(face_dirty),
+                                 instances.numel() * instances.element_size() // C.sizeof(N.GpuInstanceData),
+                                 src_indirect.numel() * src_indirect.element_size() // 20, face_count, 0)
+        N.check(self._lib.helio_shadow_cull_prepare(self._h, C.byref(inp)))
+
+    def execute(self, stream=None) -> None:
+        N.check(self._lib.helio_shadow_cull_execute(self._h, _stream_ptr(stream)))
+
+    def outputs(self) -> dict:
+        o = N.ShadowCullOutputs()
+        N.check(self._lib.helio_shadow_cull_publish(self._h, C.byref(o)))
+        return {"face_indirect": device_view(o.face_indirect, (o.max_faces * o.max_draws_per_face, 5)),
+                "face_counts": device_view(o.face_counts, (o.max_faces,))}
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            self._lib.helio_shadow_cull_destroy(h)
+            self._h = None
+
+
 class VgBuilder:
     """The VG input producer (helio_vg_builder): rebuild_vg_buffers on the device, from a
     descriptor pool, mesh records and dense object slots held in device memory

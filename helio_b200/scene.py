@@ -260,6 +260,55 @@ def serving_requests(n: int, rate_hz: float = 2000.0, n_scenes: int = 8, pool: i
     return out
 
 
+def shadow_faces(seed: int, n_spot: int = 16, n_point: int = 4) -> tuple:
+    """Shadow faces of the per-face shadow cull: ([256, 16] column-major view-projection
+    matrices, faces in use): 4 orthographic cascades of growing size, spot lights, point
+    lights (6 cube faces each); the rest zero."""
+    rng = np.random.default_rng(seed)
+    mats = []
+    d = np.array([0.3, -1.0, 0.2])
+    for half in (8.0, 32.0, 128.0, 512.0):
+        mats.append(orthographic(tuple(-d * 600.0), (0.0, 0.0, 0.0), (0.0, 0.0, 1.0), half, 1.0, 1500.0))
+    for _ in range(n_spot):
+        eye = rng.uniform(-150, 150, 3)
+        target = eye + rng.normal(size=3) * 50.0
+        mats.append(perspective(tuple(eye), tuple(target), (0.0, 1.0, 0.0) if abs(target[1] - eye[1]) < 40 else
+                                  (1.0, 0.0, 0.0), float(rng.uniform(30, 90)), 1.0, 0.5, 300.0))
+    axes = [(1, 0, 0), (-1, 0, 0), (0, 1, 0), (0, -1, 0), (0, 0, 1), (0, 0, -1)]
+    for _ in range(n_point):
+        eye = rng.uniform(-100, 100, 3)
+        for a in axes:
+            up = (0.0, 1.0, 0.0) if a[1] == 0 else (0.0, 0.0, 1.0)
+            mats.append(perspective(tuple(eye), tuple(eye + np.array(a, float)), up, 90.0, 1.0, 0.1, 60.0))
+    out = np.zeros((256, 16), np.float32)
+    for i, c in enumerate(mats):
+        out[i] = np.ctypeslib.as_array(c.view_proj)
+    return out, len(mats)
+
+
+def shadow_draws(seed: int, instances: int, draws: int, spread: float = 200.0) -> tuple:
+    """(instances, DrawIndexedIndirect [draws, 5] uint32) of the per-face shadow cull:
+    spheres uniform in a cube, with radius 0, -1 and NaN mixed in, and 1% of the draws
+    naming an instance past the array."""
+    rng = np.random.default_rng(seed)
+    inst = np.zeros(instances, DT_INSTANCE)
+    inst["bounds"][:, :3] = rng.uniform(-spread, spread, (instances, 3))
+    inst["bounds"][:, 3] = rng.uniform(0.2, 6.0, instances)
+    k = max(1, instances // 50)
+    inst["bounds"][rng.choice(instances, k, replace=False), 3] = 0.0
+    inst["bounds"][rng.choice(instances, k, replace=False), 3] = -1.0
+    inst["bounds"][rng.choice(instances, 2, replace=False), 3] = np.nan
+    src = np.zeros((draws, 5), np.uint32)
+    src[:, 0] = rng.integers(3, 3000, draws)
+    src[:, 1] = 1
+    src[:, 2] = rng.integers(0, 1 << 20, draws)
+    src[:, 3] = rng.integers(0, 1 << 16, draws)
+    src[:, 4] = rng.integers(0, instances, draws)
+    src[rng.choice(draws, max(1, draws // 100), replace=False), 4] = instances + 7  # past the array
+    return inst, src
+
+
+
 def work_items_for(objects) -> list:
     """64-meshlet work spans of (object_index, max_meshlet_count) pairs, in order
     (crates/helio/src/scene/virtual_geometry/rebuild.rs:45-58): one span per started

@@ -632,6 +632,52 @@ int32_t helio_serve_plan_batch(const helio_serve_pending* queue, uint32_t n, uin
 void helio_serve_destroy(helio_serve* server);
 
 /* ════════════════════════════════════════════════════════════════════════════
+ * Per-face shadow cull — ShadowCullPass
+ *   (crates/helio-pass-shadow-cull/src/lib.rs:37-328, shaders/shadow_cull.wgsl:1-96)
+ *
+ * Every movable draw against every dirty shadow face (CSM cascade, spot, point-light
+ * cube face): the instance's world sphere (GpuInstanceData.bounds of the draw's
+ * first_instance) against the six planes built from the columns of the face's matrix.
+ * The visible draws of face f go to face_indirect[f * 4096 + i], in draw order (the
+ * reference appends them with an atomic counter, in no defined order), and
+ * face_counts[f] counts them all, also past 4096. Faces whose dirty word is zero keep
+ * their records; their counts are cleared. Nothing runs, and the counts keep their
+ * values, when face_count or draw_count is zero (lib.rs:261-263).
+ * ════════════════════════════════════════════════════════════════════════════ */
+
+#define HELIO_SHADOW_MAX_FACES 256u           /* MAX_FACES, lib.rs:37 */
+#define HELIO_SHADOW_MAX_DRAWS_PER_FACE 4096u /* MAX_DRAWS_PER_FACE, lib.rs:40 */
+
+typedef struct helio_shadow_cull_inputs {
+    const float* shadow_matrices;                    /* device [256][16] column-major (GpuShadowMatrix) */
+    const HelioGpuInstanceData* instances;           /* device [instance_count] */
+    const HelioDrawIndexedIndirectArgs* src_indirect; /* device [draw_count]: the movable draws */
+    const uint32_t* face_dirty;                      /* device [256]: non-zero = cull this face */
+    uint32_t instance_count;                         /* draws naming an instance past it are skipped */
+    uint32_t draw_count;                             /* shadow_movable_draw_count */
+    uint32_t face_count;                             /* shadow_count: 0 skips the pass */
+    uint32_t reserved0;
+} helio_shadow_cull_inputs;
+
+typedef struct helio_shadow_cull_outputs {
+    HelioDrawIndexedIndirectArgs* face_indirect; /* [256 * 4096] */
+    uint32_t* face_counts;                       /* [256] */
+    uint32_t max_faces;
+    uint32_t max_draws_per_face;
+} helio_shadow_cull_outputs;
+
+typedef struct helio_shadow_cull_pass helio_shadow_cull_pass;
+/* Allocates the 256 x 4096 indirect records (lib.rs:104-117). */
+int32_t helio_shadow_cull_create(helio_shadow_cull_pass** out);
+/* Binds the inputs (kept until the next prepare) and grows the scratch for draw_count.
+ * shadow_matrices and instances must be 16-byte aligned. */
+int32_t helio_shadow_cull_prepare(helio_shadow_cull_pass* pass, const helio_shadow_cull_inputs* in);
+/* Three launches on `stream`; no allocation, no read-back. */
+int32_t helio_shadow_cull_execute(helio_shadow_cull_pass* pass, void* stream);
+int32_t helio_shadow_cull_publish(const helio_shadow_cull_pass* pass, helio_shadow_cull_outputs* out);
+void helio_shadow_cull_destroy(helio_shadow_cull_pass* pass);
+
+/* ════════════════════════════════════════════════════════════════════════════
  * VG input producer: rebuild_vg_buffers on the device
  *   (crates/helio/src/scene/virtual_geometry/rebuild.rs:18-58, 98-172)
  *

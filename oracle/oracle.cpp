@@ -24,6 +24,7 @@
 #include "oracle.h"
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstring>
 #include <thread>
@@ -764,6 +765,73 @@ int oracle_vg_rebuild(const HelioGpuMeshletEntry* pool, uint32_t pool_count, con
     counts[2] = items;
     counts[3] = draws;
     return 0;
+}
+
+
+// normalize_plane (shadow_cull.wgsl:49-55): p / length(p.xyz) when that length exceeds 1e-10.
+static void shadow_normalize(float p[4]) {
+    const float len = sqrtf((p[0] * p[0] + p[1] * p[1]) + p[2] * p[2]);
+    if (len > 1e-10f) {
+        p[0] = p[0] / len;
+        p[1] = p[1] / len;
+        p[2] = p[2] / len;
+        p[3] = p[3] / len;
+    }
+}
+
+// sphere_in_frustum (shadow_cull.wgsl:57-71): planes from the columns of vp (vp[i] is
+// column i): c3 + c0, c3 - c0, c3 + c1, c3 - c1, c2, c3 - c2.
+static void shadow_planes(const float* vp, float pl[6][4]) {
+    const float* c0 = vp;
+    const float* c1 = vp + 4;
+    const float* c2 = vp + 8;
+    const float* c3 = vp + 12;
+    for (int k = 0; k < 4; ++k) {
+        pl[0][k] = c3[k] + c0[k];
+        pl[1][k] = c3[k] - c0[k];
+        pl[2][k] = c3[k] + c1[k];
+        pl[3][k] = c3[k] - c1[k];
+        pl[4][k] = c2[k];
+        pl[5][k] = c3[k] - c2[k];
+    }
+    for (int i = 0; i < 6; ++i) shadow_normalize(pl[i]);
+}
+
+int oracle_shadow_cull(const float* matrices, const HelioGpuInstanceData* instances, uint32_t instance_count,
+                       const HelioDrawIndexedIndirectArgs* src, uint32_t draw_count, const uint32_t* face_dirty,
+                       uint32_t face_count, uint32_t max_per_face, HelioDrawIndexedIndirectArgs* dst,
+                       uint32_t* face_counts) {
+    constexpr uint32_t kFaces = 256;
+    if (face_count == 0 || draw_count == 0) return 0;  // lib.rs:261-263
+    for (uint32_t f = 0; f < kFaces; ++f) face_counts[f] = 0;  // lib.rs:266-270
+    std::vector<std::array<std::array<float, 4>, 6>> planes(kFaces);
+    for (uint32_t f = 0; f < kFaces; ++f) {
+        if (face_dirty[f] == 0) continue;
+        float pl[6][4];
+        shadow_planes(matrices + 16 * f, pl);
+        for (int i = 0; i < 6; ++i)
+            for (int k = 0; k < 4; ++k) planes[f][i][k] = pl[i][k];
+    }
+    for (uint32_t d = 0; d < draw_count; ++d) {
+        const HelioDrawIndexedIndirectArgs draw = src[d];
+        if (draw.first_instance >= instance_count) continue;
+        const float* b = instances[draw.first_instance].bounds;
+        const V3 c = v3(b[0], b[1], b[2]);
+        const float radius = b[3];
+        if (radius <= 0.0f) continue;  // shadow_cull.wgsl:82 (a NaN radius goes on)
+        for (uint32_t f = 0; f < kFaces; ++f) {
+            if (face_dirty[f] == 0) continue;
+            bool inside = true;
+            for (int i = 0; i < 6 && inside; ++i) {
+                const auto& p = planes[f][i];
+                if ((dot3(v3(p[0], p[1], p[2]), c) + p[3]) + radius < 0.0f) inside = false;
+            }
+            if (!inside) continue;
+            const uint32_t slot = face_counts[f]++;
+            if (slot < max_per_face) dst[(size_t)f * max_per_face + slot] = draw;
+        }
+    }
+    return 1;
 }
 
 }  // extern "C"

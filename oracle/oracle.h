@@ -103,6 +103,19 @@ int oracle_vg_rebuild(const HelioGpuMeshletEntry* pool, uint32_t pool_count, con
                       uint32_t slot_count, HelioGpuMeshletEntry* out_meshlets, HelioGpuVgObject* out_objects,
                       HelioGpuInstanceData* out_instances, HelioGpuVgWorkItem* out_items, uint64_t counts[4]);
 
+/* ShadowCullPass::execute + shadow_cull.wgsl (crates/helio-pass-shadow-cull/src/lib.rs:
+ * 257-328, shaders/shadow_cull.wgsl:49-96) over 256 faces: for every face whose dirty
+ * word is non-zero, the draws whose instance sphere passes the face's six column-built
+ * planes, in draw order (the reference appends with atomics, so its order is not
+ * defined), copied to dst[face * max_per_face + i] for i < max_per_face;
+ * face_counts[face] counts them all. A draw whose first_instance is not below
+ * instance_count is skipped. Returns 0 without touching anything when face_count or
+ * draw_count is zero (the reference returns before clearing the counts), else 1. */
+int oracle_shadow_cull(const float* matrices, const HelioGpuInstanceData* instances, uint32_t instance_count,
+                       const HelioDrawIndexedIndirectArgs* src, uint32_t draw_count, const uint32_t* face_dirty,
+                       uint32_t face_count, uint32_t max_per_face, HelioDrawIndexedIndirectArgs* dst,
+                       uint32_t* face_counts);
+
 /* Single decisions, for the reference's known-answer tests. */
 /* sphere_visible (vg_cull.wgsl:126-133) against six given planes. */
 int oracle_sphere_visible(const float planes[24], const float center[3], float radius);

@@ -88,6 +88,8 @@ def lib() -> C.CDLL:
         L.oracle_hiz_occludes.restype = C.c_int
         L.oracle_vg_rebuild.argtypes = [vp, u32, vp, u32, vp, vp, u32, vp, vp, vp, vp, C.POINTER(C.c_uint64)]
         L.oracle_vg_rebuild.restype = C.c_int
+        L.oracle_shadow_cull.argtypes = [vp, vp, u32, vp, u32, vp, u32, u32, vp, vp]
+        L.oracle_shadow_cull.restype = C.c_int
         _lib = L
     return _lib
 
@@ -234,3 +236,22 @@ def vg_rebuild(pool: np.ndarray, meshes: np.ndarray, slot_mesh: np.ndarray, slot
     assert rc == 0
     out["max_draw_count"] = int(counts[3])
     return out
+
+
+def shadow_cull(matrices: np.ndarray, instances: np.ndarray, src: np.ndarray, face_dirty: np.ndarray,
+                face_count: int, max_per_face: int = 4096, dst=None, counts=None):
+    """ShadowCullPass over 256 faces (matrices float32 [256, 16] column-major, src
+    uint32 [n, 5] DrawIndexedIndirect, face_dirty uint32 [256]). dst / counts carry the
+    previous frame (the pass keeps them when it returns early). Returns (dst [256 *
+    max_per_face, 5], counts [256], ran)."""
+    L = lib()
+    matrices = np.ascontiguousarray(matrices, dtype=np.float32)
+    src = np.ascontiguousarray(src, dtype=np.uint32).reshape(-1, 5)
+    face_dirty = np.ascontiguousarray(face_dirty, dtype=np.uint32)
+    instances = np.ascontiguousarray(instances)
+    dst = np.zeros((256 * max_per_face, 5), np.uint32) if dst is None else dst.copy()
+    counts = np.zeros(256, np.uint32) if counts is None else counts.copy()
+    ran = L.oracle_shadow_cull(matrices.ctypes.data, instances.ctypes.data, len(instances), src.ctypes.data,
+                               len(src), face_dirty.ctypes.data, face_count, max_per_face, dst.ctypes.data,
+                               counts.ctypes.data)
+    return dst, counts, bool(ran)

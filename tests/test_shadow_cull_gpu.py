@@ -1,0 +1,97 @@
+"""Per-face shadow cull (helio_shadow_cull_*: ShadowCullPass, shadow_cull.wgsl) against
+the oracle's restatement: every dirty face's visible draws in draw order, the counts of
+all 256 faces, records of clean faces kept from earlier frames, more than 4096 visible
+draws on a face, the pass's early return, and skipped draws (r <= 0, instance index
+past the array; a NaN radius passes every plane, as in the reference)."""
+import numpy as np
+import pytest
+
+from helpers import u32
+from oracle import oracle as O
+
+
+def shadow_faces(seed):
+    from helio_b200 import scene as S
+
+    return S.shadow_faces(seed)
+
+
+def shadow_scene(seed, instances, draws, spread=200.0):
+    from helio_b200 import scene as S
+
+    return S.shadow_draws(seed, instances, draws, spread)
+
+pytestmark = pytest.mark.gpu
+
+
+class Gpu:
+    def __init__(self):
+        from helio_b200.passes import ShadowCullPass
+
+        self.p = ShadowCullPass()
+
+    def run(self, mats, inst, src, dirty, face_count):
+        import torch
+
+        def dev(a, dt=None):
+            return torch.from_numpy(np.ascontiguousarray(a if dt is None else a.astype(dt))).cuda()
+
+        self.p.prepare(dev(mats), dev(inst.view(np.uint8)), dev(src.view(np.int32)), dev(dirty.view(np.int32)),
+                       face_count)
+        self.p.execute()
+        torch.cuda.synchronize()
+        o = self.p.outputs()
+        return u32(o["face_indirect"]), u32(o["face_counts"])
+
+
+def check_frame(dst, counts, ref_dst, ref_counts, faces):
+    np.testing.assert_array_equal(counts, ref_counts, err_msg="face counts")
+    for f in faces:
+        n = min(int(ref_counts[f]), 4096)
+        np.testing.assert_array_equal(dst[f * 4096:f * 4096 + n], ref_dst[f * 4096:f * 4096 + n],
+                                      err_msg=f"face {f}")
+
+
+@pytest.mark.parametrize("seed,draws", [(1, 3000), (2, 20000)])
+def test_shadow_cull_matches_oracle(cuda, seed, draws):
+    mats, nf = shadow_faces(seed)
+    inst, src = shadow_scene(seed, 5000, draws)
+    rng = np.random.default_rng(seed + 100)
+    dirty = np.zeros(256, np.uint32)
+    dirty[:nf] = rng.random(nf) < 0.8
+    dirty[0] = 1
+    g = Gpu()
+    dst, counts = g.run(mats, inst, src, dirty, nf)
+    ref_dst, ref_counts, ran = O.shadow_cull(mats, inst, src, dirty, nf)
+    assert ran and ref_counts[np.nonzero(dirty)[0]].sum() > 0
+    check_frame(dst, counts, ref_dst, ref_counts, np.nonzero(dirty)[0])
+
+
+def test_clean_faces_keep_their_records_and_full_faces_count_on(cuda):
+    mats, nf = shadow_faces(3)
+    # The widest cascade sees everything: more than 4096 visible draws on face 3.
+    inst, src = shadow_scene(3, 8000, 30000, spread=150.0)
+    g = Gpu()
+    a = np.zeros(256, np.uint32)
+    a[:nf] = 1
+    dst, counts = g.run(mats, inst, src, a, nf)
+    ref_dst, ref_counts, _ = O.shadow_cull(mats, inst, src, a, nf)
+    assert ref_counts[3] > 4096
+    check_frame(dst, counts, ref_dst, ref_counts, range(nf))
+    # Frame 2: other draws, only the even faces dirty; the odd faces keep frame 1's records.
+    inst2, src2 = shadow_scene(4, 8000, 9000, spread=150.0)
+    b = np.zeros(256, np.uint32)
+    b[:nf:2] = 7
+    dst2, counts2 = g.run(mats, inst2, src2, b, nf)
+    ref_dst2, ref_counts2, _ = O.shadow_cull(mats, inst2, src2, b, nf, dst=ref_dst, counts=ref_counts)
+    check_frame(dst2, counts2, ref_dst2, ref_counts2, range(nf))
+    assert (counts2[1:nf:2] == 0).all()  # clean faces' counts are cleared, their records kept
+    for f in range(1, nf, 2):
+        n = min(int(ref_counts[f]), 4096)
+        np.testing.assert_array_equal(dst2[f * 4096:f * 4096 + n], dst[f * 4096:f * 4096 + n])
+    # Frame 3: no faces in use: nothing runs and the counts stay as they were.
+    dst3, counts3 = g.run(mats, inst2, src2, b, 0)
+    np.testing.assert_array_equal(counts3, counts2)
+    _, ref_counts3, ran = O.shadow_cull(mats, inst2, src2, b, 0, dst=ref_dst2, counts=ref_counts2)
+    assert not ran
+    np.testing.assert_array_equal(counts3, ref_counts3)
