@@ -168,6 +168,7 @@ struct helio_occlusion_cull_pass {
     uint32_t width = 0, height = 0;
     uint32_t* stats = nullptr;
     uint32_t draw_count = 0;
+    helio_static_hiz static_hiz{};  // texels null = no static Hi-Z
 };
 
 struct helio_vg_pass {
@@ -457,6 +458,27 @@ static void fill_occlusion(helio::InstanceCullParams& prm, const helio_occlusion
     prm.screen_w = p->width;
     prm.screen_h = p->height;
     prm.hiz_mip_count = mip_levels(p->width, p->height);
+    prm.static_texels = p->static_hiz.texels;
+    for (int k = 0; k < 3; ++k) {
+        prm.static_dims[k] = p->static_hiz.grid_resolution[k];
+        prm.static_min[k] = p->static_hiz.world_bounds_min[k];
+        prm.static_max[k] = p->static_hiz.world_bounds_max[k];
+    }
+}
+
+int32_t helio_occlusion_cull_set_static_hiz(helio_occlusion_cull_pass* p, const helio_static_hiz* hiz) {
+    HELIO_ARG(p, "null pointer");
+    if (!hiz) {
+        p->static_hiz = helio_static_hiz{};
+        return HELIO_OK;
+    }
+    HELIO_ARG(hiz->texels, "static Hi-Z texels missing");
+    for (int k = 0; k < 3; ++k) HELIO_ARG(hiz->grid_resolution[k] > 0, "static Hi-Z grid must be non-empty");
+    HELIO_ARG((uint64_t)hiz->grid_resolution[2] * 6u <= 0x7FFFFFFFull &&
+                  (uint64_t)hiz->grid_resolution[0] <= 0x7FFFFFFFull && (uint64_t)hiz->grid_resolution[1] <= 0x7FFFFFFFull,
+              "static Hi-Z grid too large");
+    p->static_hiz = *hiz;
+    return HELIO_OK;
 }
 
 int32_t helio_occlusion_cull_execute(helio_occlusion_cull_pass* p, const helio_scene_buffers* scene,

@@ -3,8 +3,8 @@
 //
 // References:
 //   crates/helio-pass-indirect-dispatch/shaders/indirect_dispatch.wgsl:79-176
-//   crates/helio-pass-occlusion-cull/shaders/occlusion_cull.wgsl:101-220
-//     (the static Hi-Z branch, :222-259, is off in every supported configuration)
+//   crates/helio-pass-occlusion-cull/shaders/occlusion_cull.wgsl:101-259 (the static
+//     Hi-Z branch, :222-259, when the pass has a baked grid: static_hiz_occludes)
 // One thread per draw call. Statistics are aggregated per warp (ballot + popc)
 // before one atomic per warp and slot; the totals equal the reference's
 // per-thread atomics.
@@ -16,6 +16,58 @@
 namespace helio {
 
 namespace {
+
+// Linear-filtered fetch of level 0 of the static Hi-Z at normalised (x, y, z), clamp to
+// edge: per axis t = x * n - 0.5, taps floor(t) and floor(t) + 1 clamped to [0, n - 1],
+// weight frac(t) rounded to 8 fractional bits; x, then y, then z, each (1 - w) a + w b.
+struct StaticTap {
+    uint32_t i0, i1;
+    float w;
+};
+
+__device__ __forceinline__ StaticTap static_tap(float x, uint32_t n) {
+    const float t = fsub(fmul(x, (float)n), 0.5f);
+    const float fl = floorf(t);
+    const float w = fdiv(rintf(fmul(fsub(t, fl), 256.0f)), 256.0f);
+    const int i = (int)fl;
+    const int hi = (int)n - 1;
+    return StaticTap{(uint32_t)min(max(i, 0), hi), (uint32_t)min(max(i + 1, 0), hi), w};
+}
+
+__device__ __forceinline__ float static_lerp(float a, float b, float w) {
+    return fadd(fmul(fsub(1.0f, w), a), fmul(w, b));
+}
+
+__device__ float static_hiz_sample(const InstanceCullParams& P, float x, float y, float z) {
+    const uint32_t W = P.static_dims[0], H = P.static_dims[1], D = P.static_dims[2] * 6u;
+    const StaticTap tx = static_tap(x, W), ty = static_tap(y, H), tz = static_tap(z, D);
+    const float* T = P.static_texels;
+    auto at = [&](uint32_t i, uint32_t j, uint32_t k) { return __ldg(T + ((size_t)k * H + j) * W + i); };
+    const float c00 = static_lerp(at(tx.i0, ty.i0, tz.i0), at(tx.i1, ty.i0, tz.i0), tx.w);
+    const float c10 = static_lerp(at(tx.i0, ty.i1, tz.i0), at(tx.i1, ty.i1, tz.i0), tx.w);
+    const float c01 = static_lerp(at(tx.i0, ty.i0, tz.i1), at(tx.i1, ty.i0, tz.i1), tx.w);
+    const float c11 = static_lerp(at(tx.i0, ty.i1, tz.i1), at(tx.i1, ty.i1, tz.i1), tx.w);
+    return static_lerp(static_lerp(c00, c10, ty.w), static_lerp(c01, c11, ty.w), tz.w);
+}
+
+// The static Hi-Z test (occlusion_cull.wgsl:222-259): true = occluded.
+__device__ bool static_hiz_occludes(const InstanceCullParams& P, F3 center, F3 cam_pos) {
+    const F3 d = sub3(center, cam_pos);
+    const float dist = fsqrt(dot3(d, d));
+    if (!(dist > 0.001f)) return false;
+    const F3 v = f3(fdiv(d.x, dist), fdiv(d.y, dist), fdiv(d.z, dist));
+    const float ax = fabsf(v.x), ay = fabsf(v.y), az = fabsf(v.z);
+    uint32_t layer;
+    if (ax >= ay && ax >= az) layer = v.x < 0.0f ? 1u : 0u;
+    else if (ay >= az) layer = v.y < 0.0f ? 3u : 2u;
+    else layer = v.z < 0.0f ? 5u : 4u;
+    const float u = clampf(fdiv(fsub(center.x, P.static_min[0]), fsub(P.static_max[0], P.static_min[0])), 0.0f, 1.0f);
+    const float vv = clampf(fdiv(fsub(center.y, P.static_min[1]), fsub(P.static_max[1], P.static_min[1])), 0.0f, 1.0f);
+    const float w0 = clampf(fdiv(fsub(center.z, P.static_min[2]), fsub(P.static_max[2], P.static_min[2])), 0.0f, 1.0f);
+    const float w = fdiv(fadd(w0, (float)layer), 6.0f);
+    const float occ = static_hiz_sample(P, u, vv, w);
+    return dist > fadd(occ, 0.1f);
+}
 
 template <bool kFrustum, bool kOcclusion>
 __global__ void __launch_bounds__(256) instance_cull_kernel(InstanceCullParams P) {
@@ -146,6 +198,8 @@ __global__ void __launch_bounds__(256) instance_cull_kernel(InstanceCullParams P
                         const float h11 = hiz_sample(s_hiz, u1, v1, mip);
                         const float hz = fmaxf(fmaxf(h00, h01), fmaxf(h10, h11));
                         occluded = near_z > fadd(hz, 1.0f / 65536.0f);
+                        if (!occluded && P.static_texels)
+                            occluded = static_hiz_occludes(P, center, f3(pn.x, pn.y, pn.z));
                     }
                 }
             }

@@ -18,6 +18,10 @@ struct InstanceCullParams {
     uint32_t instance_count;  // draws whose first_instance >= instance_count are frustum-culled
     uint32_t screen_w, screen_h;
     uint32_t hiz_mip_count;  // mip_levels(screen_w, screen_h), unclamped (occlusion-cull lib.rs:303)
+    // Static Hi-Z (occlusion_cull.wgsl:222-259); off when static_texels is null.
+    const float* static_texels;  // level 0: dims[0] x dims[1] x (dims[2] * 6), x fastest
+    uint32_t static_dims[3];
+    float static_min[3], static_max[3];
 };
 
 void launch_instance_cull(const InstanceCullParams& p, bool frustum, bool occlusion, cudaStream_t stream);

@@ -131,6 +131,12 @@ class VgBuildInputs(C.Structure):
 VG_NO_MESH = 0xFFFFFFFF
 
 
+class StaticHiz(C.Structure):
+    """helio_static_hiz: level 0 of a baked static Hi-Z grid (six direction layers along z)."""
+    _fields_ = [("texels", vp), ("grid_resolution", u32 * 3), ("world_bounds_min", f32 * 3),
+                ("world_bounds_max", f32 * 3)]
+
+
 class ShadowCullInputs(C.Structure):
     _fields_ = [("shadow_matrices", vp), ("instances", vp), ("src_indirect", vp), ("face_dirty", vp),
                 ("instance_count", u32), ("draw_count", u32), ("face_count", u32), ("reserved0", u32)]
@@ -299,6 +305,7 @@ CULL_EXPORTS = {
     "helio_serve_stats_get": (i32, [vp, C.POINTER(ServeStats)]),
     "helio_serve_plan_batch": (i32, [C.POINTER(ServePending), u32, u32, u32, C.POINTER(u32), C.POINTER(u32)]),
     "helio_serve_destroy": (None, [vp]),
+    "helio_occlusion_cull_set_static_hiz": (i32, [vp, C.POINTER(StaticHiz)]),
     "helio_vg_builder_create": (i32, [C.POINTER(vp)]),
     "helio_vg_builder_run": (i32, [vp, C.POINTER(VgBuildInputs), vp]),
     "helio_vg_builder_frame_data": (i32, [vp, C.POINTER(VgFrameData)]),

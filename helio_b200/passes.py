@@ -202,6 +202,20 @@ class OcclusionCullPass:
     def on_resize(self, width: int, height: int) -> None:
         N.check(self._lib.helio_occlusion_cull_resize(self._h, width, height))
 
+    def set_static_hiz(self, texels, grid=(0, 0, 0), bounds_min=(0.0, 0.0, 0.0), bounds_max=(0.0, 0.0, 0.0)) -> None:
+        """Static Hi-Z for the following executes (texels: device float32 tensor of level
+        0, grid[0] x grid[1] x grid[2] * 6, x fastest), or None to switch it off."""
+        if texels is None:
+            N.check(self._lib.helio_occlusion_cull_set_static_hiz(self._h, None))
+            self._static = None
+            return
+        assert texels.is_cuda and texels.dtype == torch.float32 and texels.is_contiguous()
+        assert texels.numel() == grid[0] * grid[1] * grid[2] * 6
+        s = N.StaticHiz(texels.data_ptr(), (C.c_uint32 * 3)(*grid), (C.c_float * 3)(*bounds_min),
+                        (C.c_float * 3)(*bounds_max))
+        N.check(self._lib.helio_occlusion_cull_set_static_hiz(self._h, C.byref(s)))
+        self._static = texels
+
     def __del__(self):
         h = getattr(self, "_h", None)
         if h:

@@ -315,7 +315,8 @@ typedef struct helio_occlusion_cull_pass helio_occlusion_cull_pass;
 
 int32_t helio_occlusion_cull_create(uint32_t screen_width, uint32_t screen_height,
                                     uint32_t* stats_dev, helio_occlusion_cull_pass** out);
-/* Reference: crates/helio-pass-occlusion-cull/src/lib.rs:297-317 (static Hi-Z off). */
+/* Reference: crates/helio-pass-occlusion-cull/src/lib.rs:297-317 (the static Hi-Z:
+ * helio_occlusion_cull_set_static_hiz). */
 int32_t helio_occlusion_cull_prepare(helio_occlusion_cull_pass* pass, uint32_t draw_count);
 /* One thread per draw: occlusion_cull.wgsl:146-220. Frame 0 is skipped
  * (no temporal pyramid yet, reference lib.rs:321). */
@@ -324,6 +325,29 @@ int32_t helio_occlusion_cull_execute(helio_occlusion_cull_pass* pass,
                                      const helio_hiz_pyramid* hiz, uint64_t frame_num,
                                      void* stream);
 int32_t helio_occlusion_cull_resize(helio_occlusion_cull_pass* pass, uint32_t w, uint32_t h);
+
+/* A baked static Hi-Z (HiZBuildPass::load_static_hiz, crates/helio-pass-hiz/src/lib.rs:272-373):
+ * level 0 of its R32Float 3-D texture, grid_resolution[0] x [1] x ([2] * 6) texels with x
+ * fastest, the six direction layers (+X, -X, +Y, -Y, +Z, -Z) stacked along z, over the
+ * world box [world_bounds_min, world_bounds_max]. */
+typedef struct helio_static_hiz {
+    const float* texels; /* device */
+    uint32_t grid_resolution[3];
+    float world_bounds_min[3];
+    float world_bounds_max[3];
+} helio_static_hiz;
+
+/* The static Hi-Z branch of the occlusion test (occlusion_cull.wgsl:222-259), for this
+ * pass's executes, separate or fused, until the next call: `hiz` non-NULL switches it
+ * on (OcclusionCullPass::set_static_hiz_metadata plus a static Hi-Z in the frame
+ * resources, occlusion-cull/src/lib.rs:267-276, 297-299), NULL off (the default). A draw
+ * that the dynamic test keeps is culled when its camera distance exceeds the texture's
+ * distance at its centre plus 0.1. The texture is read with the reference's linear
+ * filter and clamp-to-edge addressing; WebGPU leaves the filter's weight precision to
+ * the implementation, and this library rounds the weights to 8 fractional bits (the
+ * precision CUDA documents for its texture unit) and interpolates x, then y, then z as
+ * (1 - t) a + t b. The texels stay borrowed until the next call. */
+int32_t helio_occlusion_cull_set_static_hiz(helio_occlusion_cull_pass* pass, const helio_static_hiz* hiz);
 void helio_occlusion_cull_destroy(helio_occlusion_cull_pass* pass);
 
 /* Both instance passes in one kernel launch (frustum + sub-pixel, then the Hi-Z

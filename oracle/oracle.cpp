@@ -357,11 +357,64 @@ void oracle_indirect_dispatch(const HelioGpuCameraUniforms* cam, const float pla
 }
 
 // occlusion_cull.wgsl:101-220 (static Hi-Z branch off).
+// Static Hi-Z fetch: level 0, clamp to edge, linear filter with weights rounded to 8
+// fractional bits, x then y then z, each (1 - w) a + w b (the library's stated rule).
+static float static_hiz_sample(const helio_static_hiz* s, float x, float y, float z) {
+    const uint32_t n[3] = {s->grid_resolution[0], s->grid_resolution[1], s->grid_resolution[2] * 6u};
+    const float c[3] = {x, y, z};
+    uint32_t i0[3], i1[3];
+    float w[3];
+    for (int a = 0; a < 3; ++a) {
+        const float t = c[a] * (float)n[a] - 0.5f;
+        const float fl = floorf(t);
+        w[a] = rintf((t - fl) * 256.0f) / 256.0f;
+        const int i = (int)fl, hi = (int)n[a] - 1;
+        i0[a] = (uint32_t)std::min(std::max(i, 0), hi);
+        i1[a] = (uint32_t)std::min(std::max(i + 1, 0), hi);
+    }
+    auto at = [&](uint32_t i, uint32_t j, uint32_t k) {
+        return s->texels[((size_t)k * n[1] + j) * n[0] + i];
+    };
+    auto lerp = [](float a, float b, float t) { return (1.0f - t) * a + t * b; };
+    const float c00 = lerp(at(i0[0], i0[1], i0[2]), at(i1[0], i0[1], i0[2]), w[0]);
+    const float c10 = lerp(at(i0[0], i1[1], i0[2]), at(i1[0], i1[1], i0[2]), w[0]);
+    const float c01 = lerp(at(i0[0], i0[1], i1[2]), at(i1[0], i0[1], i1[2]), w[0]);
+    const float c11 = lerp(at(i0[0], i1[1], i1[2]), at(i1[0], i1[1], i1[2]), w[0]);
+    return lerp(lerp(c00, c10, w[1]), lerp(c01, c11, w[1]), w[2]);
+}
+
+// occlusion_cull.wgsl:224-258: true = occluded.
+static bool static_hiz_occludes(const helio_static_hiz* s, V3 c, V3 cam_pos) {
+    const V3 d = sub(c, cam_pos);
+    const float dist = sqrtf(dot3(d, d));
+    if (!(dist > 0.001f)) return false;
+    const V3 v = divs(d, dist);
+    const float ax = fabsf(v.x), ay = fabsf(v.y), az = fabsf(v.z);
+    uint32_t layer;
+    if (ax >= ay && ax >= az) layer = v.x < 0.0f ? 1u : 0u;
+    else if (ay >= az) layer = v.y < 0.0f ? 3u : 2u;
+    else layer = v.z < 0.0f ? 5u : 4u;
+    const float u = clampf((c.x - s->world_bounds_min[0]) / (s->world_bounds_max[0] - s->world_bounds_min[0]), 0.0f, 1.0f);
+    const float vv = clampf((c.y - s->world_bounds_min[1]) / (s->world_bounds_max[1] - s->world_bounds_min[1]), 0.0f, 1.0f);
+    const float w0 = clampf((c.z - s->world_bounds_min[2]) / (s->world_bounds_max[2] - s->world_bounds_min[2]), 0.0f, 1.0f);
+    const float w = (w0 + (float)layer) / 6.0f;
+    return dist > static_hiz_sample(s, u, vv, w) + 0.1f;
+}
+
 void oracle_occlusion_cull(const HelioGpuCameraUniforms* cam, uint32_t screen_w,
                            uint32_t screen_h, const helio_hiz_pyramid* hiz,
                            const HelioGpuInstanceData* inst, const HelioGpuDrawCall* dc,
                            uint32_t draw_count, uint32_t instance_count, uint32_t* indirect,
                            uint32_t* stats, oracle_stats* st) {
+    oracle_occlusion_cull_static(cam, screen_w, screen_h, hiz, inst, dc, draw_count, instance_count, indirect,
+                                 stats, st, nullptr);
+}
+
+void oracle_occlusion_cull_static(const HelioGpuCameraUniforms* cam, uint32_t screen_w,
+                                  uint32_t screen_h, const helio_hiz_pyramid* hiz,
+                                  const HelioGpuInstanceData* inst, const HelioGpuDrawCall* dc,
+                                  uint32_t draw_count, uint32_t instance_count, uint32_t* indirect,
+                                  uint32_t* stats, oracle_stats* st, const helio_static_hiz* static_hiz) {
     (void)screen_w;
     uint32_t mip_count = oracle_mip_levels(screen_w, screen_h);
     const float P00 = cam->proj[0], P11 = cam->proj[5];
@@ -413,7 +466,9 @@ void oracle_occlusion_cull(const HelioGpuCameraUniforms* cam, uint32_t screen_w,
         float hz = fmaxf(fmaxf(h00, h01), fmaxf(h10, h11));
         float biased = hz + 1.0f / 65536.0f;
         mg.cmp(near_z, biased);
-        if (near_z > biased) {
+        bool occluded = near_z > biased;
+        if (!occluded && static_hiz) occluded = static_hiz_occludes(static_hiz, c, cam_pos);
+        if (occluded) {
             uint32_t* o = indirect + (size_t)idx * 5;
             bool was_visible = o[1] != 0u;
             o[1] = 0u;

@@ -61,6 +61,15 @@ void oracle_occlusion_cull(const HelioGpuCameraUniforms* cam, uint32_t screen_w,
                            uint32_t draw_count, uint32_t instance_count, uint32_t* indirect,
                            uint32_t* stats, oracle_stats* st);
 
+/* oracle_occlusion_cull with the static Hi-Z branch (occlusion_cull.wgsl:222-259) when
+ * static_hiz is non-null (its texels are host memory here); the library's filter rule
+ * (helio_occlusion_cull_set_static_hiz) is restated exactly. */
+void oracle_occlusion_cull_static(const HelioGpuCameraUniforms* cam, uint32_t screen_w,
+                                  uint32_t screen_h, const helio_hiz_pyramid* hiz,
+                                  const HelioGpuInstanceData* inst, const HelioGpuDrawCall* dc,
+                                  uint32_t draw_count, uint32_t instance_count, uint32_t* indirect,
+                                  uint32_t* stats, oracle_stats* st, const helio_static_hiz* static_hiz);
+
 /* Uniforms of the VG cull (CullUniforms, rendering.rs:828-859). */
 typedef struct oracle_vg_uniforms {
     uint32_t object_count;

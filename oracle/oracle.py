@@ -71,6 +71,9 @@ def lib() -> C.CDLL:
         L.oracle_occlusion_cull.argtypes = [vp, u32, u32, C.POINTER(Pyramid), vp, vp, u32, u32, vp, vp,
                                             C.POINTER(OracleStats)]
         L.oracle_occlusion_cull.restype = None
+        L.oracle_occlusion_cull_static.argtypes = [vp, u32, u32, C.POINTER(Pyramid), vp, vp, u32, u32, vp, vp,
+                                                   C.POINTER(OracleStats), vp]
+        L.oracle_occlusion_cull_static.restype = None
         L.oracle_vg_select.argtypes = [vp, C.POINTER(OracleVgUniforms), vp, vp, vp, vp, vp, C.POINTER(OracleStats),
                                        C.c_int]
         L.oracle_vg_select.restype = None
@@ -173,13 +176,22 @@ def indirect_dispatch(cam, instances, draw_calls, aabbs):
     return indirect, stats
 
 
-def occlusion_cull(cam, screen_w, screen_h, levels, instances, draw_calls, indirect, stats):
-    """In place on `indirect` / `stats` (as the reference pass)."""
+def occlusion_cull(cam, screen_w, screen_h, levels, instances, draw_calls, indirect, stats, static_hiz=None):
+    """In place on `indirect` / `stats` (as the reference pass). static_hiz: None, or a
+    dict of level-0 texels (float32, x fastest), grid (3 ints), min and max (3 floats)."""
+    from helio_b200 import native as N
+
     cam_b = camera_array(cam)
     pyr = pyramid(levels)
     st = OracleStats()
-    lib().oracle_occlusion_cull(_p(cam_b), screen_w, screen_h, C.byref(pyr), _p(instances), _p(draw_calls),
-                                len(draw_calls), len(instances), _p(indirect), _p(stats), C.byref(st))
+    sh = None
+    if static_hiz is not None:
+        tex = np.ascontiguousarray(static_hiz["texels"], dtype=np.float32)
+        sh = N.StaticHiz(tex.ctypes.data, (C.c_uint32 * 3)(*static_hiz["grid"]), (C.c_float * 3)(*static_hiz["min"]),
+                         (C.c_float * 3)(*static_hiz["max"]))
+    lib().oracle_occlusion_cull_static(_p(cam_b), screen_w, screen_h, C.byref(pyr), _p(instances), _p(draw_calls),
+                                       len(draw_calls), len(instances), _p(indirect), _p(stats), C.byref(st),
+                                       C.byref(sh) if sh is not None else None)
     return st
 
 

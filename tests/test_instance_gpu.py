@@ -31,7 +31,7 @@ def _scene(cfg=0, scale=1.0, edge_cases=True):
     return w, inst, aabbs, draws
 
 
-def _gpu_instance(w, inst, aabbs, draws, levels_gpu=None, hz=None, mode="separate", frame=1):
+def _gpu_instance(w, inst, aabbs, draws, levels_gpu=None, hz=None, mode="separate", frame=1, static_hiz=None):
     import torch
     from helio_b200 import passes as P
 
@@ -48,6 +48,9 @@ def _gpu_instance(w, inst, aabbs, draws, levels_gpu=None, hz=None, mode="separat
     oc = P.OcclusionCullPass(view.width, view.height, stats)
     fr.prepare(view.camera, len(draws))
     oc.prepare(len(draws))
+    if static_hiz is not None:
+        oc.set_static_hiz(torch.from_numpy(static_hiz["texels"]).cuda(), static_hiz["grid"], static_hiz["min"],
+                          static_hiz["max"])
     if mode == "separate":
         fr.execute(sb)
         oc.execute(sb, hz.publish(), frame)
@@ -94,3 +97,55 @@ def test_instance_cull_larger_scene(cuda):
     O.occlusion_cull(view.camera, view.width, view.height, O.hiz_build(view.depth), inst, draws, o_ind, o_st)
     np.testing.assert_array_equal(g_ind, o_ind)
     np.testing.assert_array_equal(g_st, o_st)
+
+
+def static_grid(seed, grid=(12, 10, 8), lo=(-100.0, -100.0, -100.0), hi=(100.0, 100.0, 100.0), far=400.0):
+    """A baked static Hi-Z: per voxel and direction layer, the distance past which an
+    object counts as hidden (uniform in [0, far])."""
+    rng = np.random.default_rng(seed)
+    tex = rng.uniform(0.0, far, grid[0] * grid[1] * grid[2] * 6).astype(np.float32)
+    return {"texels": tex, "grid": grid, "min": lo, "max": hi}
+
+
+@pytest.mark.parametrize("mode", ["separate", "fused"])
+def test_static_hiz_matches_oracle(cuda, mode):
+    """occlusion_cull.wgsl:222-259: the static test after the dynamic one keeps a draw."""
+    w, inst, aabbs, draws = _scene()
+    view = w.views[0]
+    hz, _ = gpu_hiz(view.depth)
+    sh = static_grid(5, far=150.0)
+    g_ind, g_st = _gpu_instance(w, inst, aabbs, draws, hz=hz, mode=mode, static_hiz=sh)
+    levels = O.hiz_build(view.depth)
+    o_ind, o_st = O.indirect_dispatch(view.camera, inst, draws, aabbs)
+    O.occlusion_cull(view.camera, view.width, view.height, levels, inst, draws, o_ind, o_st, static_hiz=sh)
+    np.testing.assert_array_equal(g_ind, o_ind)
+    np.testing.assert_array_equal(g_st, o_st)
+    d_ind, d_st = O.indirect_dispatch(view.camera, inst, draws, aabbs)
+    O.occlusion_cull(view.camera, view.width, view.height, levels, inst, draws, d_ind, d_st)
+    assert o_st[4] > d_st[4], "the static grid should hide draws the dynamic pyramid keeps"
+
+
+def test_static_hiz_edge_cases_and_switch_off(cuda):
+    """A flat world box (division by zero: clamped), a one-voxel grid, then the branch off."""
+    w, inst, aabbs, draws = _scene()
+    view = w.views[0]
+    hz, _ = gpu_hiz(view.depth)
+    levels = O.hiz_build(view.depth)
+    for sh in (static_grid(6, grid=(5, 7, 3), lo=(-100.0, 0.0, -100.0), hi=(100.0, 0.0, 100.0)),
+               static_grid(7, grid=(1, 1, 1), far=150.0)):
+        g_ind, g_st = _gpu_instance(w, inst, aabbs, draws, hz=hz, mode="fused", static_hiz=sh)
+        o_ind, o_st = O.indirect_dispatch(view.camera, inst, draws, aabbs)
+        O.occlusion_cull(view.camera, view.width, view.height, levels, inst, draws, o_ind, o_st, static_hiz=sh)
+        np.testing.assert_array_equal(g_ind, o_ind)
+        np.testing.assert_array_equal(g_st, o_st)
+    import torch
+    from helio_b200 import passes as P
+
+    st = torch.zeros(8, dtype=torch.int32, device="cuda")
+    oc = P.OcclusionCullPass(view.width, view.height, st)
+    oc.set_static_hiz(torch.from_numpy(static_grid(8)["texels"]).cuda(), (12, 10, 8), (-100.0,) * 3, (100.0,) * 3)
+    oc.set_static_hiz(None)
+    g_ind, g_st = _gpu_instance(w, inst, aabbs, draws, hz=hz, mode="separate")
+    o_ind, o_st = O.indirect_dispatch(view.camera, inst, draws, aabbs)
+    O.occlusion_cull(view.camera, view.width, view.height, levels, inst, draws, o_ind, o_st)
+    np.testing.assert_array_equal(g_ind, o_ind)
