@@ -334,6 +334,8 @@ __device__ void phase_setup(const BatchParams& P) {
             c.hiz_mip_count = V.hiz_mip_count;
             c.pad[0] = c.pad[1] = 0u;
             P.cviews[v] = c;
+            __threadfence();
+            atomicAdd(P.setup_done, 1u);  // the select units wait for every view
         }
         __syncwarp();
     }
@@ -889,51 +891,76 @@ __device__ __forceinline__ void stamp(const BatchParams& P, int k) {
     }
 }
 
+// The views' select constants and reject boxes into shared memory, once the view setup
+// has published all of them (thread 0 waits, bounded, for the counter).
+__device__ void load_sel_views(const BatchParams& P, char* sm) {
+    if (threadIdx.x == 0) {
+        uint32_t polls = 0;
+        while (ld_cg(P.setup_done) < P.view_count) {
+            if (++polls > kSpinLimit) {
+                atomicOr(P.error, kBatchErrTimeout);
+                break;
+            }
+            __nanosleep(polls < 256 ? 64 : 256);
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    SelView* s_sv = reinterpret_cast<SelView*>(sm + kSmSelViews);
+    for (uint32_t k = threadIdx.x; k < P.view_count; k += kBatchThreads) {
+        const CullView* cvp = P.cviews + k;
+        SelView sv;
+        const uint4* src = reinterpret_cast<const uint4*>(&cvp->planes);
+        uint4* dst = reinterpret_cast<uint4*>(&sv.planes);
+        for (int w = 0; w < 6; ++w) dst[w] = __ldcg(src + w);
+        sv.pos_near = __ldcg(&cvp->pos_near);
+        sv.focal = __ldcg(&cvp->focal);
+        sv.thr = __ldcg(&cvp->lod_threshold_px);
+        const QuotientBound qb = quotient_bound(sv.thr);
+        sv.thr_lo = qb.lo;
+        sv.thr_hi = qb.hi;
+        sv.pad = make_float4(0.f, 0.f, 0.f, 0.f);
+        s_sv[k] = sv;
+        SelBox bx;
+        for (int i = 0; i < 3; ++i) {
+            bx.lo[i] = __ldcg(&P.views[k].reject_box[i]);
+            bx.hi[i] = __ldcg(&P.views[k].reject_box[3 + i]);
+        }
+        bx.pad[0] = bx.pad[1] = 0u;
+        reinterpret_cast<SelBox*>(sm + kSmSelBox)[k] = bx;
+    }
+    __syncthreads();
+}
+
 __global__ void __launch_bounds__(kBatchThreads, 3) batch_kernel(BatchParams P) {
     extern __shared__ __align__(16) char sm[];
     uint32_t* s_tmp = reinterpret_cast<uint32_t*>(sm + kSmMisc);
 
     stamp(P, 0);
     phase_setup(P);
-    grid_sync(P);
+    // No barrier: the Hi-Z units need nothing from the view setup, and a CTA waits for
+    // the published views only before its first select unit (load_sel_views).
     stamp(P, 1);
 
     // Phase 1: Hi-Z tiles and object chunks share one work list.
     {
-        SelView* s_sv = reinterpret_cast<SelView*>(sm + kSmSelViews);
-        for (uint32_t k = threadIdx.x; k < P.view_count; k += kBatchThreads) {
-            const CullView* cvp = P.cviews + k;
-            SelView sv;
-            const uint4* src = reinterpret_cast<const uint4*>(&cvp->planes);
-            uint4* dst = reinterpret_cast<uint4*>(&sv.planes);
-            for (int w = 0; w < 6; ++w) dst[w] = __ldcg(src + w);
-            sv.pos_near = __ldcg(&cvp->pos_near);
-            sv.focal = __ldcg(&cvp->focal);
-            sv.thr = __ldcg(&cvp->lod_threshold_px);
-            const QuotientBound qb = quotient_bound(sv.thr);
-            sv.thr_lo = qb.lo;
-            sv.thr_hi = qb.hi;
-            sv.pad = make_float4(0.f, 0.f, 0.f, 0.f);
-            s_sv[k] = sv;
-            SelBox bx;
-            for (int i = 0; i < 3; ++i) {
-                bx.lo[i] = __ldcg(&P.views[k].reject_box[i]);
-                bx.hi[i] = __ldcg(&P.views[k].reject_box[3 + i]);
-            }
-            bx.pad[0] = bx.pad[1] = 0u;
-            reinterpret_cast<SelBox*>(sm + kSmSelBox)[k] = bx;
+        for (uint32_t k = threadIdx.x; k < P.view_count; k += kBatchThreads)
             reinterpret_cast<uint32_t*>(sm + kSmTileBegin)[k] = P.views[k].hiz_pair_begin;
-        }
         // Hi-Z tiles (memory bound) and select units (arithmetic bound) are spread
         // evenly through one work queue, so that the CTAs sharing an SM overlap the two
         // kinds of work and CTAs that draw cheap units draw more of them. Thread 0
-        // claims the next unit while the block works on the current one. Unit u is a
-        // select unit iff floor((u + 1) S / U) > floor(u S / U).
+        // claims the next unit while the block works on the current one. The first h0
+        // units are Hi-Z tiles (two per CTA: time for the view setup to finish); after
+        // them, unit h0 + u is a select unit iff floor((u + 1) S / U) > floor(u S / U)
+        // over the U units that remain.
         const uint32_t group_cap = min(max(P.select_views, 1u), kSelectMaxViews);
         const uint32_t vgroups = (P.view_count + group_cap - 1) / group_cap;
         const uint32_t gsize = (P.view_count + vgroups - 1) / vgroups;  // balanced view groups
         const uint32_t sel_units = P.object_chunks * vgroups;
         const uint32_t units = P.hiz_tiles + sel_units;
+        const uint32_t h0 = min(P.hiz_tiles, 2u * gridDim.x);
+        const uint32_t rest = units - h0;
+        bool have_views = false;  // uniform over the CTA
         volatile uint32_t* s_unit = s_tmp + 8;
         if (threadIdx.x == 0) {
             *s_unit = atomicAdd(P.work, 1u);
@@ -946,12 +973,17 @@ __global__ void __launch_bounds__(kBatchThreads, 3) batch_kernel(BatchParams P) 
             if (u >= units) break;
             uint32_t next = 0;
             if (threadIdx.x == 0) next = atomicAdd(P.work, 1u);
-            const uint32_t sel_before = (uint32_t)((uint64_t)u * sel_units / units);
-            const bool is_hiz = (uint32_t)((uint64_t)(u + 1) * sel_units / units) == sel_before;
+            const uint32_t ur = u >= h0 ? u - h0 : 0u;
+            const uint32_t sel_before = u >= h0 ? (uint32_t)((uint64_t)ur * sel_units / rest) : 0u;
+            const bool is_hiz = u < h0 || (uint32_t)((uint64_t)(ur + 1) * sel_units / rest) == sel_before;
             asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
             if (is_hiz) {
-                phase_hiz_tile(P, u - sel_before, sm);
+                phase_hiz_tile(P, u < h0 ? u : h0 + ur - sel_before, sm);
             } else {
+                if (!have_views) {
+                    load_sel_views(P, sm);
+                    have_views = true;
+                }
                 const uint32_t chunk = sel_before / vgroups, vg = sel_before - chunk * vgroups;
                 phase_select_chunk(P, chunk, vg * gsize, min(P.view_count, (vg + 1) * gsize), sm);
             }

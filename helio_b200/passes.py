@@ -428,7 +428,9 @@ class BatchedCull:
 
     def phase_times(self, stream=None) -> dict:
         """Device microseconds of each phase of the last execute, then the largest
-        per-CTA busy time on Hi-Z tiles and on object chunks within phase 1."""
+        per-CTA busy time on Hi-Z tiles and on object chunks within phase 1. view_setup is
+        CTA 0's part of the view setup (the other CTAs start on Hi-Z tiles meanwhile), and
+        hiz_and_select runs from there to the end of phase 1."""
         arr = (C.c_double * 9)()
         n = N.u32(0)
         N.check(self._lib.helio_batch_get_phase_times(self._h, arr, 9, C.byref(n), _stream_ptr(stream)))
