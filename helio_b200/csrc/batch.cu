@@ -579,18 +579,6 @@ __device__ void phase_expand(const BatchParams& P, char* sm) {
     uint32_t* s_tmp = reinterpret_cast<uint32_t*>(sm + kSmMisc);
     const uint32_t V = P.view_count, C = P.object_chunks, tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
-    // Hi-Z levels 7.. of each view, by warp 0 of CTA v (mod grid), from the level 6
-    // that phase 1 wrote; the test phase reads them after the next barrier.
-    if (warp == 0) {
-        const HizJob& J = *reinterpret_cast<const HizJob*>(sm + kSmHizJob);
-        for (uint32_t v = blockIdx.x; v < V; v += gridDim.x) {
-            if (P.views[v].hiz.mip_count <= 7u) continue;
-            load_hiz_job(P, v, sm);
-            __syncwarp();
-            hiz_tail_warp(J);
-            __syncwarp();
-        }
-    }
     // Padded first span of every view (a multiple of 32).
     {
         uint32_t padded = 0;
@@ -606,6 +594,20 @@ __device__ void phase_expand(const BatchParams& P, char* sm) {
         if (blockIdx.x == 0)
             for (uint32_t v = tid; v <= V; v += kBatchThreads) P.view_span_start[v] = s_vstart[v];
         if (tid == 0 && total > P.span_capacity) atomicOr(P.error, kBatchErrSpanCapacity);
+    }
+    // Hi-Z levels 7.. of each view, by warp 0 of CTA v (mod grid), from the level 6
+    // that phase 1 wrote (after the view starts, whose block barriers would otherwise
+    // hold the CTA's other warps for the tail); the test phase reads them after the
+    // next barrier.
+    if (warp == 0) {
+        const HizJob& J = *reinterpret_cast<const HizJob*>(sm + kSmHizJob);
+        for (uint32_t v = blockIdx.x; v < V; v += gridDim.x) {
+            if (P.views[v].hiz.mip_count <= 7u) continue;
+            load_hiz_job(P, v, sm);
+            __syncwarp();
+            hiz_tail_warp(J);
+            __syncwarp();
+        }
     }
     const VgSceneDev& S = P.scene;
     const uint32_t n_units = V * C;
