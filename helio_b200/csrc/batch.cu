@@ -53,6 +53,7 @@ struct SelBox {
 
 // Dynamic shared memory layout (bytes).
 constexpr uint32_t kSelectMaxViews = 32;  // views per select unit, at most
+constexpr uint32_t kExpandBatch = 8;       // (view, chunk) units per claim of the expansion queue
 static_assert(kSelectMaxViews * 8 <= kBatchThreads, "one thread per (view, mask word) in the write-out");
 constexpr size_t kSmSelViews = 0;                                               // SelView[kBatchMaxViews]
 constexpr size_t kSmSelBox = kSmSelViews + sizeof(SelView) * kBatchMaxViews;    // SelBox[kBatchMaxViews]
@@ -611,19 +612,24 @@ __device__ void phase_expand(const BatchParams& P, char* sm) {
     }
     const VgSceneDev& S = P.scene;
     const uint32_t n_units = V * C;
-    const uint32_t gw = blockIdx.x * (kBatchThreads / 32) + warp, GW = gridDim.x * (kBatchThreads / 32);
-    // Units are dealt out strided (lane k of warp w looks at unit w + k * W) so that the
-    // heavy consecutive chunks of a large view spread over many warps.
-    // A warp takes 32 units at a time (lane l: unit w + (k0 + l) * W) and flattens
-    // their visible lists into one sequence: round r gives lane i the entry
-    // 32 r + i, so the list and object loads of every unit are in flight together
-    // (two round trips per round instead of two per unit). The spans of an entry go to
-    // its unit's first span + the spans of the unit's earlier entries: a scan of the
-    // span counts within the round, less the scan before the unit's first entry in the
-    // round, plus what the unit wrote in earlier rounds (carried by the unit's lane).
-    for (uint32_t k0 = 0; gw + (size_t)k0 * GW < n_units; k0 += 32u) {
-        const size_t u = gw + (size_t)(k0 + lane) * GW;
-        const bool live = u < n_units;
+    // Warps claim batches of kExpandBatch units from a queue; batch b holds the units
+    // b + k * NB (lane k < kExpandBatch), strided so that the heavy consecutive chunks of
+    // a large view spread over many batches, and small enough that warps which drew light
+    // batches draw more of them. A warp flattens its batch's visible lists into one
+    // sequence: round r gives lane i the entry 32 r + i, so the list and object loads of
+    // every unit are in flight together (two round trips per round instead of two per
+    // unit). The spans of an entry go to its unit's first span + the spans of the unit's
+    // earlier entries: a scan of the span counts within the round, less the scan before
+    // the unit's first entry in the round, plus what the unit wrote in earlier rounds
+    // (carried by the unit's lane).
+    const uint32_t NB = (n_units + kExpandBatch - 1) / kExpandBatch;
+    for (;;) {
+        uint32_t bq = 0;
+        if (lane == 0) bq = atomicAdd(P.expand_work, 1u);
+        bq = __shfl_sync(0xffffffffu, bq, 0);
+        if (bq >= NB) break;
+        const size_t u = bq + (size_t)lane * NB;
+        const bool live = (uint32_t)lane < kExpandBatch && u < n_units;
         const uint32_t vis = live ? ld_cg(P.chunk_vis + u) : 0u;
         if (!__any_sync(0xffffffffu, vis != 0u)) continue;
         const uint32_t v = live ? (uint32_t)(u / C) : 0u, ch = live ? (uint32_t)(u - (size_t)v * C) : 0u;
@@ -638,7 +644,7 @@ __device__ void phase_expand(const BatchParams& P, char* sm) {
             const uint32_t jfirst = __shfl_sync(0xffffffffu, first_e, j);
             const uint32_t jv = __shfl_sync(0xffffffffu, v, j), jch = __shfl_sync(0xffffffffu, ch, j);
             const uint32_t jpos = __shfl_sync(0xffffffffu, pos, j), jdone = __shfl_sync(0xffffffffu, written, j);
-            const size_t ju = gw + (size_t)(k0 + (uint32_t)j) * GW;
+            const size_t ju = bq + (size_t)j * NB;
             uint32_t count = 0, first = 0, inst = 0, lod = 0, o = 0;
             if (e < total) {
                 const uint32_t en = __ldcg(P.vis_list + ju * kBatchChunk + (e - jfirst));
