@@ -58,6 +58,7 @@ struct BatchParams {
     uint32_t* work;           // [1] phase-1 work queue head, zero before the launch
     uint32_t* setup_done;     // [1] views whose constants are published, zero before the launch
     uint32_t* expand_work;    // [1] expansion work queue head, zero before the launch
+    uint32_t* test_work;      // [1] meshlet-test work queue head, zero before the launch
     uint32_t* chunk_counts;   // [view_count * object_chunks] active spans per (view, chunk)
     uint32_t* chunk_vis;      // [view_count * object_chunks] visible objects per (view, chunk)
     uint16_t* vis_list;       // [view_count * object_chunks * kBatchChunk] per (view, chunk): its

@@ -69,7 +69,8 @@ struct helio_batch {
     uint32_t* work() const { return barrier() + 3; }
     uint32_t* setup_done() const { return barrier() + 4; }
     uint32_t* expand_work() const { return barrier() + 5; }
-    size_t stamps_offset() const { return ((16u * view_count + 6u) * 4u + 7u) & ~(size_t)7u; }
+    uint32_t* test_work() const { return barrier() + 6; }
+    size_t stamps_offset() const { return ((16u * view_count + 7u) * 4u + 7u) & ~(size_t)7u; }
     unsigned long long* stamps() const {
         return reinterpret_cast<unsigned long long*>(clear.as<char>() + stamps_offset());
     }
@@ -150,7 +151,7 @@ int32_t plan_batch(const helio_batch_config& cfg, const helio_vg_scene* sc, uint
     p.need[kBufLevels] = level_floats * sizeof(float);
     p.need[kBufIndirect] = p.out_offset[n] * sizeof(HelioDrawIndexedIndirectArgs);
     p.need[kBufDraws] = p.out_offset[n] * sizeof(HelioGpuVgDraw);
-    p.need[kBufClear] = (((16u * n + 6u) * 4u + 7u) & ~(size_t)7u) + helio::kBatchPhaseStamps * 8u;
+    p.need[kBufClear] = (((16u * n + 7u) * 4u + 7u) & ~(size_t)7u) + helio::kBatchPhaseStamps * 8u;
     p.need[kBufViews] = n * sizeof(helio::BatchViewDev);
     p.need[kBufCViews] = n * sizeof(helio::CullView);
     p.need[kBufLod] = (size_t)n * (p.lod_pitch ? p.lod_pitch : helio::kBatchChunk);
@@ -487,6 +488,7 @@ int32_t helio_batch_execute(helio_batch* b, void* stream) {
     P.work = b->work();
     P.setup_done = b->setup_done();
     P.expand_work = b->expand_work();
+    P.test_work = b->test_work();
     P.chunk_counts = b->chunk_counts.as<uint32_t>();
     P.chunk_vis = b->chunk_vis.as<uint32_t>();
     P.vis_list = b->vis_list.as<uint16_t>();
