@@ -53,6 +53,7 @@ struct SelBox {
 
 // Dynamic shared memory layout (bytes).
 constexpr uint32_t kSelectMaxViews = 32;  // views per select unit, at most
+constexpr uint32_t kHizTailUnits = 3;      // Hi-Z units per CTA held back for the end of the work queue
 constexpr uint32_t kExpandBatch = 8;       // (view, chunk) units per claim of the expansion queue
 static_assert(kSelectMaxViews * 8 <= kBatchThreads, "one thread per (view, mask word) in the write-out");
 constexpr size_t kSmSelViews = 0;                                               // SelView[kBatchMaxViews]
@@ -968,16 +969,18 @@ __global__ void __launch_bounds__(kBatchThreads, 3) batch_kernel(BatchParams P) 
         // evenly through one work queue, so that the CTAs sharing an SM overlap the two
         // kinds of work and CTAs that draw cheap units draw more of them. Thread 0
         // claims the next unit while the block works on the current one. The first h0
-        // units are Hi-Z tiles (two per CTA: time for the view setup to finish); after
-        // them, unit h0 + u is a select unit iff floor((u + 1) S / U) > floor(u S / U)
-        // over the U units that remain.
+        // units are Hi-Z tiles (two per CTA: time for the view setup to finish); the
+        // last h1 units are Hi-Z tiles too (the cheaper kind, so that the queue ends on
+        // short units); between them, unit h0 + u is a select unit iff
+        // floor((u + 1) S / U) > floor(u S / U) over the U units in between.
         const uint32_t group_cap = min(max(P.select_views, 1u), kSelectMaxViews);
         const uint32_t vgroups = (P.view_count + group_cap - 1) / group_cap;
         const uint32_t gsize = (P.view_count + vgroups - 1) / vgroups;  // balanced view groups
         const uint32_t sel_units = P.object_chunks * vgroups;
         const uint32_t units = P.hiz_tiles + sel_units;
         const uint32_t h0 = min(P.hiz_tiles, 2u * gridDim.x);
-        const uint32_t rest = units - h0;
+        const uint32_t h1 = min(P.hiz_tiles - h0, kHizTailUnits * gridDim.x);
+        const uint32_t rest = units - h0 - h1;
         bool have_views = false;  // uniform over the CTA
         volatile uint32_t* s_unit = s_tmp + 8;
         if (threadIdx.x == 0) {
@@ -991,12 +994,14 @@ __global__ void __launch_bounds__(kBatchThreads, 3) batch_kernel(BatchParams P) 
             if (u >= units) break;
             uint32_t next = 0;
             if (threadIdx.x == 0) next = atomicAdd(P.work, 1u);
-            const uint32_t ur = u >= h0 ? u - h0 : 0u;
-            const uint32_t sel_before = u >= h0 ? (uint32_t)((uint64_t)ur * sel_units / rest) : 0u;
-            const bool is_hiz = u < h0 || (uint32_t)((uint64_t)(ur + 1) * sel_units / rest) == sel_before;
+            const bool mid = u >= h0 && u - h0 < rest;
+            const uint32_t ur = mid ? u - h0 : 0u;
+            const uint32_t sel_before = mid ? (uint32_t)((uint64_t)ur * sel_units / rest) : 0u;
+            const bool is_hiz = !mid || (uint32_t)((uint64_t)(ur + 1) * sel_units / rest) == sel_before;
             asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
             if (is_hiz) {
-                phase_hiz_tile(P, u < h0 ? u : h0 + ur - sel_before, sm);
+                // Prefix tiles 0..h0-1, then the middle's tiles, then the last h1 tiles.
+                phase_hiz_tile(P, u < h0 ? u : (mid ? h0 + ur - sel_before : u - sel_units), sm);
             } else {
                 if (!have_views) {
                     load_sel_views(P, sm);
