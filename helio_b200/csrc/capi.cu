@@ -185,6 +185,7 @@ struct helio_vg_pass {
     uint64_t last_version = 0, last_instance_version = 0;
     bool have_version = false;
     uint32_t num_tiles = 0;
+    uint32_t items_per_warp = 32;
     size_t scratch_clear_bytes = 0;
     size_t view_offset = 0;
 };
@@ -622,7 +623,8 @@ int32_t helio_vg_prepare(helio_vg_pass* p, const helio_vg_frame_data* f, void* s
             p->capacity = cap;
         }
         p->max_draw_count = bounded;
-        p->num_tiles = helio::vg_cull_tiles(p->work_item_count);
+        p->items_per_warp = helio::vg_cull_items_per_warp(p->work_item_count);
+        p->num_tiles = helio::vg_cull_tiles(p->work_item_count, p->items_per_warp);
         // scratch: counters (16 words) | tile counts (both cleared per execute) | warp counts |
         //          window bits | view constants (16-byte aligned)
         p->scratch_clear_bytes = 64 + (size_t)p->num_tiles * 4;
@@ -709,6 +711,7 @@ int32_t helio_vg_execute(helio_vg_pass* p, const HelioGpuCameraUniforms* camera_
     cp.scratch.bits = cp.scratch.warp_counts + (size_t)p->num_tiles * helio::kCullWarps;
     cp.capacity = p->max_draw_count;  // min(draw_capacity, buffer lengths), vg_cull.wgsl:248-251
     cp.num_tiles = p->num_tiles;
+    cp.items_per_warp = p->items_per_warp;
     helio::launch_vg_cull(cp, s);
     HELIO_CK(cudaGetLastError());
     return HELIO_OK;

@@ -63,8 +63,8 @@ struct ViewSetupParams {
 };
 
 constexpr uint32_t kCullWarps = 8;                       // warps per CTA tile
-constexpr uint32_t kCullItemsPerTile = kCullWarps * 32;  // one work item per lane
 constexpr uint32_t kWindowsPerWarp = 64;                 // 32 items x 64 meshlets / 32 lanes
+constexpr uint32_t kCullTargetWarps = 148u * 32u;        // warps that keep every SM busy
 
 // Scratch of one cull launch. tile_counts must be zero before the test kernel
 // (it accumulates per-warp counts); warp_counts and bits are written before
@@ -90,9 +90,22 @@ struct VgCullParams {
     VgCullScratch scratch;
     uint32_t capacity;
     uint32_t num_tiles;
+    uint32_t items_per_warp;  // 1, 2, 4, ..., 32: warp w takes work items [w * ipw, (w + 1) * ipw)
 };
 
-inline uint32_t vg_cull_tiles(uint32_t work_items) { return (work_items + kCullItemsPerTile - 1) / kCullItemsPerTile; }
+// Work items per warp of the single-view cull: 32 (one per lane) when the scene has
+// enough items to fill every SM with warps, fewer for small scenes, so that their
+// windows spread over more warps instead of running in series on few. The draw order
+// is the item order for every choice.
+inline uint32_t vg_cull_items_per_warp(uint32_t work_items) {
+    uint32_t ipw = 32;
+    while (ipw > 1 && (uint64_t)work_items < (uint64_t)kCullTargetWarps * ipw) ipw >>= 1;
+    return ipw;
+}
+inline uint32_t vg_cull_tiles(uint32_t work_items, uint32_t items_per_warp) {
+    const uint32_t per_tile = kCullWarps * items_per_warp;
+    return (work_items + per_tile - 1) / per_tile;
+}
 
 void launch_pack_meshlets(const HelioGpuMeshletEntry* aos, uint32_t n, float4* bounds, float4* cone, float4* axis,
                           uint4* draw, cudaStream_t stream);

@@ -227,8 +227,9 @@ __global__ void __launch_bounds__(kCullWarps * 32) vg_cull_test_kernel(VgCullPar
     const VgSceneDev& S = P.scene;
     const uint32_t tile = blockIdx.x;
     for (int k = lane; k < kBitWordsPerWarp; k += 32) s_bits[warp][k] = 0u;
-    const uint32_t w_idx = tile * kCullItemsPerTile + warp * 32 + lane;
-    const WarpItems it = load_warp_items(S, P.sel, w_idx);
+    const bool mine = (uint32_t)lane < P.items_per_warp;
+    const uint32_t w_idx = (tile * kCullWarps + warp) * P.items_per_warp + lane;
+    const WarpItems it = load_warp_items(S, P.sel, mine ? w_idx : 0xFFFFFFFFu);
 
     // View constants are staged only when some warp of the tile has work.
     if (__syncthreads_or(it.total > 0u)) {
@@ -271,7 +272,7 @@ __global__ void __launch_bounds__(kCullWarps * 32) vg_cull_test_kernel(VgCullPar
         for (uint32_t k = lane; k < windows; k += 32) P.scratch.bits[wslot * kWindowsPerWarp + k] = s_bits[warp][k];
     }
     // Per-work-item visibility words: bits [off, off + n) of the warp's window bits.
-    if (P.visibility && w_idx < S.work_item_count) {
+    if (P.visibility && mine && w_idx < S.work_item_count) {
         uint32_t lo = 0, hi = 0;
         if (it.n) {
             const uint32_t w0 = it.off >> 5, sh = it.off & 31u;
@@ -320,8 +321,8 @@ __global__ void __launch_bounds__(kCullWarps * 32) vg_cull_emit_kernel(VgCullPar
     for (int w = 0; w < warp; ++w) base += P.scratch.warp_counts[wslot0 + w];
 
     const VgSceneDev& S = P.scene;
-    const uint32_t w_idx = tile * kCullItemsPerTile + warp * 32 + lane;
-    const WarpItems it = load_warp_items(S, P.sel, w_idx);
+    const uint32_t w_idx = (tile * kCullWarps + warp) * P.items_per_warp + lane;
+    const WarpItems it = load_warp_items(S, P.sel, (uint32_t)lane < P.items_per_warp ? w_idx : 0xFFFFFFFFu);
     const uint32_t windows = (it.total + 31u) >> 5;
     const uint32_t* wbits = P.scratch.bits + (wslot0 + warp) * kWindowsPerWarp;
     for (uint32_t win = 0; win < windows; ++win) {
