@@ -1,6 +1,6 @@
 // oracle.cpp — CPU restatement of Helio's GPU visibility path.
 //
-// TEST INFRASTRUCTURE ONLY (the checker): loaded by tests/, __graft_entry__.smoke()
+// TEST INFRASTRUCTURE ONLY (the reference the CUDA path is compared with): loaded by tests/, __graft_entry__.smoke()
 // and bench.py's CPU-baseline / reference arm. Never linked into or called by the
 // product library.
 //

@@ -1,7 +1,7 @@
 /*
  * oracle.h — CPU restatement of Helio's GPU visibility path.
  *
- * TEST INFRASTRUCTURE ONLY. This library is the checker for the CUDA path: it
+ * TEST INFRASTRUCTURE ONLY. This library is what the CUDA path is compared with: it
  * may be loaded by tests/, by __graft_entry__.smoke() and by bench.py's CPU
  * baseline / reference arm, and by nothing else. The product library
  * (helio_b200/lib/libhelio_cull.so) never links, loads or calls it.

@@ -1,7 +1,8 @@
 """ctypes front-end of the CPU oracle (oracle.cpp).
 
 TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and bench.py's
-CPU-baseline / reference arm, as the checker. The product package never imports it.
+CPU-baseline / reference arm, to compare the CUDA path with. The product package never
+imports it.
 
 Besides the raw restatements, ``run_view`` runs the whole single-view pipeline of the
 reference (Hi-Z build → object select → meshlet cull with canonical compaction) on

@@ -1,6 +1,6 @@
 """The oracle's restatements of the shadow cull (shadow_cull.wgsl) and of the static Hi-Z
 branch (occlusion_cull.wgsl:222-259) on hand-built cases whose answers follow from the
-shaders' text, on the CPU: these pin the checker that the GPU parity tests compare with."""
+shaders' text, on the CPU: these pin the oracle that the GPU parity tests compare with."""
 import numpy as np
 
 from oracle import oracle as O
