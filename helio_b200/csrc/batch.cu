@@ -67,6 +67,11 @@ constexpr size_t kSmHizM3 = kSmHizJob + ((sizeof(HizJob) + 15) / 16) * 16;    //
 constexpr size_t kSmMisc = kSmHizM3 + 2 * 8 * 9 * 4;                          // u32[64]
 constexpr size_t kSmTileBegin = kSmMisc + 64 * 4;                             // u32[kBatchMaxViews]
 constexpr size_t kSmTotal = kSmTileBegin + 4 * kBatchMaxViews;
+// An attached shadow cull's stages use the select units' LOD tile region, which no
+// other part of phases 1..3 touches while they run.
+constexpr size_t kSmShadow = kSmSelLod;
+static_assert(kSmShadow % 16 == 0 && sizeof(ShadowSmem) <= kSelectMaxViews * kBatchChunk,
+              "the shadow stages' shared memory fits the LOD tile region");
 // Phases 2..6 reuse the region from offset 0.
 constexpr size_t kSmTestViews = 0;                                       // CullView per warp
 constexpr size_t kSmTestBits = kSmTestViews + sizeof(CullView) * 8;      // u32[8][66]
@@ -682,6 +687,19 @@ __device__ void phase_expand(const BatchParams& P, char* sm) {
         for (uint32_t p = s_vstart[v] + end + tid; p < s_vstart[v + 1]; p += kBatchThreads)
             if (p < P.span_capacity) P.spans[p] = make_uint4(0u, v << 16, 0u, 0u);
     }
+    // The attached shadow cull's placement: after their expansion, CTAs claim blocks of
+    // 256 draws from a queue, so that CTAs whose warps finished early take more.
+    if (P.shadow_blocks) {
+        volatile uint32_t* s_claim = s_tmp + 20;
+        for (;;) {
+            __syncthreads();  // every thread has read the previous claim
+            if (tid == 0) *s_claim = atomicAdd(P.shadow_work, 1u);
+            __syncthreads();
+            const uint32_t b = *s_claim;
+            if (b >= P.shadow_blocks) break;
+            shadow_place_block(P.shadow, b, 0u, kShadowFaces, *reinterpret_cast<ShadowSmem*>(sm + kSmShadow));
+        }
+    }
 }
 
 // The 32 spans of a group (lane = span): meshlet range and packing offsets.
@@ -951,7 +969,7 @@ __device__ void load_sel_views(const BatchParams& P, char* sm) {
     __syncthreads();
 }
 
-__global__ void __launch_bounds__(kBatchThreads, 3) batch_kernel(BatchParams P) {
+__global__ void __launch_bounds__(kBatchThreads, 3) batch_kernel(const __grid_constant__ BatchParams P) {
     extern __shared__ __align__(16) char sm[];
     uint32_t* s_tmp = reinterpret_cast<uint32_t*>(sm + kSmMisc);
 
@@ -989,11 +1007,27 @@ __global__ void __launch_bounds__(kBatchThreads, 3) batch_kernel(BatchParams P) 
         }
         __syncthreads();
         unsigned long long t_hiz = 0, t_sel = 0, t0, t1;
+        // An attached shadow cull's S test blocks are spread evenly through the queue
+        // (they need neither the view setup nor the pyramid): with K = (units + S) / S,
+        // queue position q is shadow block (q + 1) / K - 1 when K divides q + 1 and that
+        // block exists, else unit q - min(q / K, S) below.
+        const uint32_t S = P.shadow_blocks;
+        const uint32_t queue = units + S;
+        const uint32_t K = S ? queue / S : 1u;
         for (;;) {
-            const uint32_t u = *s_unit;
-            if (u >= units) break;
+            const uint32_t q = *s_unit;
+            if (q >= queue) break;
             uint32_t next = 0;
             if (threadIdx.x == 0) next = atomicAdd(P.work, 1u);
+            if (S && (q + 1u) % K == 0u && (q + 1u) / K <= S) {
+                shadow_test_block(P.shadow, (q + 1u) / K - 1u, 0u, kShadowFaces,
+                                  *reinterpret_cast<ShadowSmem*>(sm + kSmShadow));
+                __syncthreads();  // every thread has read *s_unit
+                if (threadIdx.x == 0) *s_unit = next;
+                __syncthreads();
+                continue;
+            }
+            const uint32_t u = S ? q - min(q / K, S) : q;
             const bool mid = u >= h0 && u - h0 < rest;
             const uint32_t ur = mid ? u - h0 : 0u;
             const uint32_t sel_before = mid ? (uint32_t)((uint64_t)ur * sel_units / rest) : 0u;
@@ -1023,6 +1057,11 @@ __global__ void __launch_bounds__(kBatchThreads, 3) batch_kernel(BatchParams P) 
     }
     grid_sync(P);
     stamp(P, 2);
+    // The attached shadow cull's scan: CTA j takes the j-th dirty face (and clears face
+    // j's count when face j is clean); done before the phase's last barrier.
+    if (P.shadow_blocks)
+        for (uint32_t j = blockIdx.x; j < kShadowFaces; j += gridDim.x)
+            shadow_scan_face(P.shadow, j, *reinterpret_cast<ShadowSmem*>(sm + kSmShadow));
 
     grid_exclusive_scan(P, P.chunk_counts, P.chunk_offs, P.view_count * P.object_chunks, s_tmp);
     stamp(P, 3);

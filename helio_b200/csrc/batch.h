@@ -4,6 +4,7 @@
 
 #include "common.cuh"
 #include "kernels.h"
+#include "shadow_device.cuh"
 #include "vg.h"
 
 namespace helio {
@@ -73,6 +74,12 @@ struct BatchParams {
     uint32_t* group_bits;     // [span_capacity / 32 * kWindowsPerWarp] window ballots
     uint32_t* span_vis;       // [span_capacity * 2] per-span visibility words, or null
     unsigned long long* phase_ns;  // [kBatchPhaseStamps] %globaltimer at launch and after each phase
+    // An attached per-face shadow cull (helio_batch_attach_shadow): its test stage runs
+    // as the first shadow_blocks units of phase 1, its scan in phase 2 and its placement
+    // in phase 3. shadow_blocks = 0: none.
+    ShadowDev shadow;
+    uint32_t shadow_blocks;
+    uint32_t* shadow_work;    // [1] placement queue head of the shadow cull, zero before the launch
 };
 
 // [0..7] phase boundaries, [8] / [9] largest per-CTA time spent on Hi-Z tiles /

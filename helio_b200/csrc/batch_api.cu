@@ -10,6 +10,7 @@
 #include "batch.h"
 #include "host_util.h"
 #include "kernels.h"
+#include "shadow_host.h"
 #include "vg.h"
 
 using helio::as_stream;
@@ -52,6 +53,7 @@ struct helio_batch {
     uint32_t grid = 0, object_chunks = 0, hiz_tiles = 0, span_capacity = 0, lod_pitch = 0;
     std::vector<size_t> out_offset;  // first draw of each view in out_indirect / out_draws
     bool prepared = false;
+    helio_shadow_cull_pass* shadow = nullptr;  // attached per-face shadow cull, or null
 
     // Buffer k of the plan's order (kBuf* below).
     DevBuf& buf(int k) {
@@ -70,7 +72,8 @@ struct helio_batch {
     uint32_t* setup_done() const { return barrier() + 4; }
     uint32_t* expand_work() const { return barrier() + 5; }
     uint32_t* test_work() const { return barrier() + 6; }
-    size_t stamps_offset() const { return ((16u * view_count + 7u) * 4u + 7u) & ~(size_t)7u; }
+    uint32_t* shadow_work() const { return barrier() + 7; }
+    size_t stamps_offset() const { return ((16u * view_count + 8u) * 4u + 7u) & ~(size_t)7u; }
     unsigned long long* stamps() const {
         return reinterpret_cast<unsigned long long*>(clear.as<char>() + stamps_offset());
     }
@@ -151,7 +154,7 @@ int32_t plan_batch(const helio_batch_config& cfg, const helio_vg_scene* sc, uint
     p.need[kBufLevels] = level_floats * sizeof(float);
     p.need[kBufIndirect] = p.out_offset[n] * sizeof(HelioDrawIndexedIndirectArgs);
     p.need[kBufDraws] = p.out_offset[n] * sizeof(HelioGpuVgDraw);
-    p.need[kBufClear] = (((16u * n + 7u) * 4u + 7u) & ~(size_t)7u) + helio::kBatchPhaseStamps * 8u;
+    p.need[kBufClear] = (((16u * n + 8u) * 4u + 7u) & ~(size_t)7u) + helio::kBatchPhaseStamps * 8u;
     p.need[kBufViews] = n * sizeof(helio::BatchViewDev);
     p.need[kBufCViews] = n * sizeof(helio::CullView);
     p.need[kBufLod] = (size_t)n * (p.lod_pitch ? p.lod_pitch : helio::kBatchChunk);
@@ -466,12 +469,19 @@ int32_t helio_batch_pack_draws(const helio_batch* b, HelioDrawIndexedIndirectArg
     return HELIO_OK;
 }
 
+int32_t helio_batch_attach_shadow(helio_batch* b, helio_shadow_cull_pass* pass) {
+    HELIO_ARG(b, "null pointer");
+    b->shadow = pass;
+    return HELIO_OK;
+}
+
 int32_t helio_batch_execute(helio_batch* b, void* stream) {
     HELIO_ARG(b, "null pointer");
     if (!b->prepared) return helio_fail(HELIO_ERR_RESOURCE, "batch executed before prepare");
     cudaStream_t s = as_stream(stream);
     HELIO_CK(cudaMemsetAsync(b->clear.ptr, 0, b->clear_bytes, s));
-    if (b->scene->object_count == 0) return HELIO_OK;
+    // No launch for an empty scene: an attached shadow cull then runs on its own.
+    if (b->scene->object_count == 0) return b->shadow ? helio_shadow_cull_execute(b->shadow, stream) : HELIO_OK;
     helio::BatchParams P{};
     P.scene = b->scene->dev();
     P.views = b->views.as<helio::BatchViewDev>();
@@ -502,6 +512,9 @@ int32_t helio_batch_execute(helio_batch* b, void* stream) {
     P.group_bits = b->group_bits.as<uint32_t>();
     P.span_vis = (b->cfg.flags & HELIO_BATCH_SPAN_VISIBILITY) ? b->span_vis.as<uint32_t>() : nullptr;
     P.phase_ns = b->stamps();
+    P.shadow_blocks = 0;
+    P.shadow_work = b->shadow_work();
+    if (b->shadow && helio::shadow_dev(b->shadow, &P.shadow)) P.shadow_blocks = P.shadow.blocks;
     const uint32_t grid = (b->cfg.max_ctas && b->cfg.max_ctas < b->grid) ? b->cfg.max_ctas : b->grid;
     // The cull kernel takes the same share of the device as the select kernel.
     const uint32_t full = helio::batch_max_grid(), cull_full = helio::batch_cull_max_grid();

@@ -315,6 +315,7 @@ CULL_EXPORTS = {
     "helio_shadow_cull_execute": (i32, [vp, vp]),
     "helio_shadow_cull_publish": (i32, [vp, C.POINTER(ShadowCullOutputs)]),
     "helio_shadow_cull_destroy": (None, [vp]),
+    "helio_batch_attach_shadow": (i32, [vp, vp]),
 }
 
 _cull = None

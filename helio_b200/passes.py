@@ -417,6 +417,12 @@ class BatchedCull:
         arr = (N.GpuCameraUniforms * len(cameras))(*cameras)
         N.check(self._lib.helio_batch_set_cameras(self._h, len(cameras), arr, _stream_ptr(stream)))
 
+    def attach_shadow(self, shadow: "ShadowCullPass | None") -> None:
+        """Runs a prepared ShadowCullPass inside this batch's launches from the next
+        execute on (helio_batch_attach_shadow); its outputs stay the pass's. None detaches."""
+        N.check(self._lib.helio_batch_attach_shadow(self._h, shadow._h if shadow is not None else None))
+        self._shadow = shadow  # kept alive while attached
+
     def execute(self, stream=None) -> None:
         N.check(self._lib.helio_batch_execute(self._h, _stream_ptr(stream)))
 

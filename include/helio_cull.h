@@ -701,6 +701,16 @@ int32_t helio_shadow_cull_execute(helio_shadow_cull_pass* pass, void* stream);
 int32_t helio_shadow_cull_publish(const helio_shadow_cull_pass* pass, helio_shadow_cull_outputs* out);
 void helio_shadow_cull_destroy(helio_shadow_cull_pass* pass);
 
+/* Folds a prepared shadow cull pass into a batch: from the next helio_batch_execute on,
+ * the pass's test, scan and placement run as units of the batch's own phases (the
+ * persistent launch's work queue and barriers) instead of three launches of their own,
+ * with the outputs of helio_shadow_cull_execute, read with helio_shadow_cull_publish.
+ * The pass stays the caller's: it must stay alive, and its inputs valid, while it is
+ * attached; a pass with no face or no draw in use does nothing, as in the standalone
+ * form (lib.rs:261-263). pass = NULL detaches. The attached pass's parameters are
+ * read at each execute (a CUDA graph captures them, as it captures the views). */
+int32_t helio_batch_attach_shadow(helio_batch* batch, helio_shadow_cull_pass* pass);
+
 /* ════════════════════════════════════════════════════════════════════════════
  * VG input producer: rebuild_vg_buffers on the device
  *   (crates/helio/src/scene/virtual_geometry/rebuild.rs:18-58, 98-172)

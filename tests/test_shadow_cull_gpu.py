@@ -95,3 +95,78 @@ def test_clean_faces_keep_their_records_and_full_faces_count_on(cuda):
     _, ref_counts3, ran = O.shadow_cull(mats, inst2, src2, b, 0, dst=ref_dst2, counts=ref_counts2)
     assert not ran
     np.testing.assert_array_equal(counts3, ref_counts3)
+
+
+def test_shadow_cull_folded_into_a_batch(cuda):
+    """helio_batch_attach_shadow: the pass's stages run as units of the batch's phases.
+    Two frames (the second with other draws and only the even faces dirty): the pass's
+    outputs equal the oracle's and the standalone pass's, the batch's own outputs equal
+    those of the same batch without the pass, and detaching restores the plain batch."""
+    import torch
+    from helio_b200 import scene as S
+    from helio_b200.passes import BatchedCull, ShadowCullPass, VgScene
+
+    def dev(a):
+        return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+    w = S.config(3, scale=0.03)
+    views = w.views[:6]
+    vs = VgScene()
+    vs.upload(S.frame_data(w.scene))
+    depths = [dev(v.depth) for v in views]
+    specs = [{"camera": v.camera, "depth": d, "alias_mip0": True, "lod_threshold_px": v.lod_threshold_px}
+             for v, d in zip(views, depths)]
+
+    def batch_outputs(b):
+        out = []
+        for i in range(len(views)):
+            o = b.view_outputs(i)
+            c = u32(o["counters"])
+            n = int(min(c[0], o["capacity"]))
+            out.append((c, u32(o["indirect"])[:n], u32(o["draws"])[:n]))
+        return out
+
+    plain = BatchedCull(len(views))
+    plain.prepare(vs, specs)
+    plain.execute()
+    torch.cuda.synchronize()
+    want = batch_outputs(plain)
+
+    mats, nf = shadow_faces(5)
+    frames = [(shadow_scene(5, 6000, 20000, spread=150.0), np.arange(256) < nf),
+              (shadow_scene(6, 6000, 9000, spread=150.0), (np.arange(256) < nf) & (np.arange(256) % 2 == 0))]
+    folded, alone = ShadowCullPass(), Gpu()
+    b = BatchedCull(len(views))
+    b.prepare(vs, specs)
+    b.attach_shadow(folded)
+    ref_dst = ref_counts = None
+    for (inst, src), dirty_b in frames:
+        dirty = dirty_b.astype(np.uint32)
+        keep = (dev(mats), dev(inst.view(np.uint8)), dev(src.view(np.int32)), dev(dirty.view(np.int32)))
+        folded.prepare(*keep, nf)
+        b.execute()
+        torch.cuda.synchronize()
+        b.status()
+        o = folded.outputs()
+        dst, counts = u32(o["face_indirect"]), u32(o["face_counts"])
+        ref_dst, ref_counts, ran = O.shadow_cull(mats, inst, src, dirty, nf, dst=ref_dst, counts=ref_counts)
+        assert ran and ref_counts[:nf].sum() > 0
+        check_frame(dst, counts, ref_dst, ref_counts, range(nf))
+        a_dst, a_counts = alone.run(mats, inst, src, dirty, nf)
+        np.testing.assert_array_equal(counts, a_counts)
+        for f in range(nf):
+            n = min(int(counts[f]), 4096)
+            np.testing.assert_array_equal(dst[f * 4096:f * 4096 + n], a_dst[f * 4096:f * 4096 + n])
+        for (c, ind, dr), (wc, wind, wdr) in zip(batch_outputs(b), want):
+            np.testing.assert_array_equal(c, wc)
+            np.testing.assert_array_equal(ind, wind)
+            np.testing.assert_array_equal(dr, wdr)
+    b.attach_shadow(None)
+    before = u32(folded.outputs()["face_counts"]).copy()
+    b.execute()
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(u32(folded.outputs()["face_counts"]), before)
+    for (c, ind, dr), (wc, wind, wdr) in zip(batch_outputs(b), want):
+        np.testing.assert_array_equal(c, wc)
+        np.testing.assert_array_equal(ind, wind)
+        np.testing.assert_array_equal(dr, wdr)
