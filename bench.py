@@ -68,6 +68,7 @@ def parse_args():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="batched3: skip the per-view plain comparison")
+    ap.add_argument("--no-fold", action="store_true", help="shadow: skip the pass folded into the 85-view batch")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="bound of the CPU baseline sample")
     ap.add_argument("--requests", type=int, default=1000, help="serve4: timed requests (after --warmup x 20)")
     ap.add_argument("--rate", type=float, default=2000.0, help="serve4: arrival rate (requests/s)")
@@ -1094,6 +1095,7 @@ def run_shadow(args, rank, world, local_rank):
                "h2d_bytes_per_step": int(hs.numel() * 4), "d2h_bytes_per_step": 256 * 4,
                "ms_per_step": e2e_ms / args.steps,
                "form": "the draw records copied in from pinned host memory, the cull, the 256 counts copied out"}
+    folded = None if args.no_fold else shadow_fold_times(timer, dev, p, args.steps, args.warmup)
     cpu = None
     if rank == 0 and world == 1:
         v, runs, t = shadow_cpu(mats, nf, inst, src, dirty, args.cpu_seconds)
@@ -1110,8 +1112,35 @@ def run_shadow(args, rank, world, local_rank):
                    "timing": ("CUDA-graph replay" if graphed else "eager launches") + ", CUDA events",
                    "parallelism": f"replica x{world}" if world > 1 else "single GPU"},
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches_per_step * args.steps),
-        "clocks": clk,
+        "clocks": clk, "folded": folded,
     }
+
+
+def shadow_fold_times(timer, dev, p, steps: int, warmup: int) -> dict:
+    """Device ms per step (median, graph replay, L2 flushed) of the 85-view batch of the
+    batched3 workload alone, of the batch followed by the standalone shadow pass `p`, and
+    of the batch with `p` folded into its launches (helio_batch_attach_shadow)."""
+    import torch
+    from helio_b200 import scene as S
+    from helio_b200.passes import BatchedCull, VgScene
+
+    wl = S.config(3)
+    vs = VgScene()
+    vs.upload(S.frame_data(wl.scene))
+    depths = [torch.from_numpy(v.depth).to(dev) for v in wl.views]
+    b = BatchedCull(len(wl.views))
+    b.prepare(vs, [{"camera": v.camera, "depth": t, "alias_mip0": True, "lod_threshold_px": v.lod_threshold_px}
+                   for v, t in zip(wl.views, depths)])
+    out = {"form": "85-view batch of the batched3 workload (two cooperative launches) with the shadow step"}
+    for name, fn in (("batch_ms", b.execute), ("batch_then_shadow_ms", lambda: (b.execute(), p.execute()))):
+        ms, _ = timer.run(fn, steps, warmup)
+        out[name] = float(np.median(ms))
+    b.attach_shadow(p)
+    ms, _ = timer.run(b.execute, steps, warmup)
+    out["batch_with_folded_shadow_ms"] = float(np.median(ms))
+    b.status()
+    b.attach_shadow(None)
+    return out
 
 
 def run_reference(args):
