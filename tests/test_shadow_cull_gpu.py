@@ -97,11 +97,13 @@ def test_clean_faces_keep_their_records_and_full_faces_count_on(cuda):
     np.testing.assert_array_equal(counts3, ref_counts3)
 
 
-def test_shadow_cull_folded_into_a_batch(cuda):
+@pytest.mark.parametrize("max_ctas", [0, 37])
+def test_shadow_cull_folded_into_a_batch(cuda, max_ctas):
     """helio_batch_attach_shadow: the pass's stages run as units of the batch's phases.
     Two frames (the second with other draws and only the even faces dirty): the pass's
     outputs equal the oracle's and the standalone pass's, the batch's own outputs equal
-    those of the same batch without the pass, and detaching restores the plain batch."""
+    those of the same batch without the pass, and detaching restores the plain batch.
+    With 37 CTAs every CTA scans several faces and places several blocks."""
     import torch
     from helio_b200 import scene as S
     from helio_b200.passes import BatchedCull, ShadowCullPass, VgScene
@@ -126,7 +128,7 @@ def test_shadow_cull_folded_into_a_batch(cuda):
             out.append((c, u32(o["indirect"])[:n], u32(o["draws"])[:n]))
         return out
 
-    plain = BatchedCull(len(views))
+    plain = BatchedCull(len(views), max_ctas=max_ctas)
     plain.prepare(vs, specs)
     plain.execute()
     torch.cuda.synchronize()
@@ -136,7 +138,7 @@ def test_shadow_cull_folded_into_a_batch(cuda):
     frames = [(shadow_scene(5, 6000, 20000, spread=150.0), np.arange(256) < nf),
               (shadow_scene(6, 6000, 9000, spread=150.0), (np.arange(256) < nf) & (np.arange(256) % 2 == 0))]
     folded, alone = ShadowCullPass(), Gpu()
-    b = BatchedCull(len(views))
+    b = BatchedCull(len(views), max_ctas=max_ctas)
     b.prepare(vs, specs)
     b.attach_shadow(folded)
     ref_dst = ref_counts = None
@@ -161,8 +163,15 @@ def test_shadow_cull_folded_into_a_batch(cuda):
             np.testing.assert_array_equal(c, wc)
             np.testing.assert_array_equal(ind, wind)
             np.testing.assert_array_equal(dr, wdr)
-    b.attach_shadow(None)
+    # No face in use: the attached pass does nothing (its counts stay as they were).
+    inst, src = frames[1][0]
+    folded.prepare(dev(mats), dev(inst.view(np.uint8)), dev(src.view(np.int32)),
+                   dev(np.ones(256, np.uint32).view(np.int32)), 0)
     before = u32(folded.outputs()["face_counts"]).copy()
+    b.execute()
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(u32(folded.outputs()["face_counts"]), before)
+    b.attach_shadow(None)
     b.execute()
     torch.cuda.synchronize()
     np.testing.assert_array_equal(u32(folded.outputs()["face_counts"]), before)
