@@ -748,19 +748,16 @@ __device__ void phase_test(const BatchParams& P, uint32_t groups, char* sm) {
     const uint32_t lt = (1u << lane) - 1u;
     const VgSceneDev& S = P.scene;
     uint32_t cached_view = 0xFFFFFFFFu;
-    // Warps claim groups from a queue (a group's work ranges from one window to 64), the
-    // claim of the next group in flight while the current one is tested.
-    uint32_t g = 0;
-    if (lane == 0) g = atomicAdd(P.test_work, 1u);
-    g = __shfl_sync(0xffffffffu, g, 0);
-    for (; g < groups;) {
-        uint32_t claim = 0;
-        if (lane == 0) claim = atomicAdd(P.test_work, 1u);
+    // Warps claim groups from a queue (a group's work ranges from one window to 64) when
+    // they are done with the previous one. (Claiming the next group ahead ties it to a
+    // warp that is still busy: the queue's last groups then wait.)
+    for (;;) {
+        uint32_t g = 0;
+        if (lane == 0) g = atomicAdd(P.test_work, 1u);
+        g = __shfl_sync(0xffffffffu, g, 0);
+        if (g >= groups) break;
         const GroupSpans gs = load_group(P, g);
-        if (gs.view >= P.view_count) {  // never true: every span below the group count is written
-            g = __shfl_sync(0xffffffffu, claim, 0);
-            continue;
-        }
+        if (gs.view >= P.view_count) continue;  // never true: every span below the group count is written
         if (gs.view != cached_view) {
             const uint4* src = reinterpret_cast<const uint4*>(P.cviews + gs.view);
             uint4* dst = reinterpret_cast<uint4*>(&cv);
@@ -829,7 +826,6 @@ __device__ void phase_test(const BatchParams& P, uint32_t groups, char* sm) {
             reinterpret_cast<uint2*>(P.span_vis)[(size_t)g * 32u + lane] = w;
         }
         __syncwarp();
-        g = __shfl_sync(0xffffffffu, claim, 0);
     }
 }
 
