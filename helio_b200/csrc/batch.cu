@@ -750,12 +750,15 @@ __device__ void phase_test(const BatchParams& P, uint32_t groups, char* sm) {
     uint32_t cached_view = 0xFFFFFFFFu;
     // Warps claim groups from a queue (a group's work ranges from one window to 64) when
     // they are done with the previous one. (Claiming the next group ahead ties it to a
-    // warp that is still busy: the queue's last groups then wait.)
+    // warp that is still busy: the queue's last groups then wait.) The queue hands out
+    // the groups from the last view's end backwards: the main view, whose groups are the
+    // lightest, then fills the queue's tail (89.8 against 93.0 us in view order).
     for (;;) {
         uint32_t g = 0;
         if (lane == 0) g = atomicAdd(P.test_work, 1u);
         g = __shfl_sync(0xffffffffu, g, 0);
         if (g >= groups) break;
+        g = groups - 1u - g;
         const GroupSpans gs = load_group(P, g);
         if (gs.view >= P.view_count) continue;  // never true: every span below the group count is written
         if (gs.view != cached_view) {
