@@ -52,3 +52,6 @@ def test_invalid_arguments_are_reported_not_raised(native_built):
     vcfg = N.VgConfig(64, 64, 1, 0, 5, 0)
     assert lib.helio_vg_create(C.byref(vcfg), C.byref(h)) == N.HELIO_ERR_INVALID_ARG
     assert lib.helio_vg_prepare(None, None, None) == N.HELIO_ERR_INVALID_ARG
+    # Folding a shadow cull pass into a batch needs a batch.
+    assert lib.helio_batch_attach_shadow(None, None) == N.HELIO_ERR_INVALID_ARG
+    assert lib.helio_shadow_cull_prepare(None, None) == N.HELIO_ERR_INVALID_ARG
