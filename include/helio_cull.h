@@ -251,20 +251,22 @@ void helio_hiz_destroy(helio_hiz_pass* pass);
  * ones during its frame loop, a plugin whose device-memory use must stay fixed, a
  * frame loop that cannot take an allocation's implicit synchronisation).
  * HiZBuildPass allocates its scratch in create(); this call keeps it — one
- * completion ticket and one job descriptor per view — in a fixed device array
- * inside the library instead:
+ * completion ticket per view — in a fixed device array inside the library instead,
+ * and passes the views' descriptors as the kernel's parameter (no upload):
  *   - at most 32 views per call; every GPU that loads the library holds the array
- *     (about 9 KB) until the process exits; more views are rejected with
+ *     (128 bytes) until the process exits; more views are rejected with
  *     HELIO_ERR_INVALID_ARG;
  *   - every call shares the array and clears the tickets first, so calls whose GPU
  *     work overlaps (other streams or threads) race and must be ordered by the caller;
  *   - the first call on each device looks the array's device address up and caches
  *     it; make that first call before any stream capture.
  * The caller passes each view's depth (device) and one device buffer `levels` of
- * `levels_floats` floats that receives every view's levels one after another
- * (levels 1.. and, unless HELIO_HIZ_ALIAS_MIP0, a copy of level 0); a view needs
- * sum over its levels of pitch * height floats with pitch = width rounded up to
- * 4, each view starting on a 4-float boundary. pyramids_out[v] describes view v.
+ * `levels_floats` floats, 16-byte aligned (else HELIO_ERR_INVALID_ARG), that
+ * receives every view's levels one after another (levels 1.. and, unless
+ * HELIO_HIZ_ALIAS_MIP0, a copy of level 0); a view needs sum over its levels of
+ * pitch * height floats with pitch = width rounded up to 4, each view starting on a
+ * 4-float boundary. pyramids_out[v] describes view v. A CUDA error already pending
+ * on the calling thread is reported as HELIO_ERR_CUDA and left pending.
  * No cudaMalloc, cudaFree or allocating library routine is called. */
 typedef struct helio_hiz_view_input {
     const float* depth; /* device, width x height, row pitch `pitch` floats (0 = width) */

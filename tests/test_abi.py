@@ -55,3 +55,16 @@ def test_invalid_arguments_are_reported_not_raised(native_built):
     # Folding a shadow cull pass into a batch needs a batch.
     assert lib.helio_batch_attach_shadow(None, None) == N.HELIO_ERR_INVALID_ARG
     assert lib.helio_shadow_cull_prepare(None, None) == N.HELIO_ERR_INVALID_ARG
+
+
+def test_noalloc_rejects_misaligned_levels_before_any_launch(native_built):
+    """helio_hiz_build_noalloc stores level 1 as float2 pairs, so a levels pointer that
+    is not 16-byte aligned is refused before any CUDA call (no GPU needed here)."""
+    from helio_b200 import native as N
+
+    lib = N.cull_lib()
+    view = (N.HizViewInput * 1)(N.HizViewInput(0x10000, 64, 64, 64, 0))
+    pyr = (N.HizPyramid * 1)()
+    st = lib.helio_hiz_build_noalloc(1, view, C.c_void_p(0x10000 + 4), 1 << 20, pyr, None)
+    assert st == N.HELIO_ERR_INVALID_ARG
+    assert b"16-byte aligned" in lib.helio_last_error()

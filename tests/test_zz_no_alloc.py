@@ -10,16 +10,23 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 SIZES = [(1920, 1080, 0), (1031, 517, 0), (64, 64, 0), (300, 1, 0), (513, 257, 1)]
+# 32 views, the most one call takes: small probe-like views, a third of them read
+# from depth rows longer than the view (pitch > width), some with level 0 aliased.
+SIZES_32 = [(128 + 9 * i, 64 + 5 * i, i % 4 == 3, 7 * (i % 3)) for i in range(32)]
 
 
-def _views(seed):
+def _views(seed, sizes=SIZES):
+    """(depth view, width, height, alias) per size; a size with a fourth entry k > 0
+    reads its depth from rows of width + k floats."""
     import torch
 
     rng = np.random.default_rng(seed)
     out = []
-    for w, h, alias in SIZES:
-        d = torch.from_numpy(rng.random((h, w), dtype=np.float32)).cuda()
-        out.append((d, w, h, alias))
+    for size in sizes:
+        w, h, alias = size[:3]
+        extra = size[3] if len(size) > 3 else 0
+        full = torch.from_numpy(rng.random((h, w + extra), dtype=np.float32)).cuda()
+        out.append((full[:, :w], w, h, alias))
     return out
 
 
@@ -39,7 +46,7 @@ def _noalloc(views, levels_floats=None):
 
     lib = N.cull_lib()
     n = len(views)
-    inp = (N.HizViewInput * n)(*[N.HizViewInput(d.data_ptr(), w, h, w, N.HELIO_HIZ_ALIAS_MIP0 if a else 0)
+    inp = (N.HizViewInput * n)(*[N.HizViewInput(d.data_ptr(), w, h, d.stride(0), N.HELIO_HIZ_ALIAS_MIP0 if a else 0)
                                  for d, w, h, a in views])
     need = 0
     for _, w, h, a in views:
@@ -74,6 +81,21 @@ def test_noalloc_matches_allocating_pass_on_two_calls(cuda):
             for l, (x, y) in enumerate(zip(levels, ref)):
                 np.testing.assert_array_equal(x.view(np.uint32), y.view(np.uint32),
                                               err_msg=f"call {call} view {w}x{h} level {l}")
+
+
+def test_noalloc_32_views_with_pitched_depth_matches_allocating_pass(cuda):
+    """The whole fixed array in use (32 views, the largest job search), with depth rows
+    longer than the views, on two calls in a row."""
+    for call, seed in enumerate((5, 6)):
+        views = _views(seed, SIZES_32)
+        st, msg, got = _noalloc(views)
+        assert st == 0, msg
+        for (d, w, h, a), levels in zip(views, got):
+            ref = _reference_levels(d, w, h, a)
+            assert len(levels) == len(ref)
+            for l, (x, y) in enumerate(zip(levels, ref)):
+                np.testing.assert_array_equal(x.view(np.uint32), y.view(np.uint32),
+                                              err_msg=f"call {call} view {w}x{h} pitch {d.stride(0)} level {l}")
 
 
 def test_noalloc_rejects_sizes_beyond_its_limits(cuda):
