@@ -67,6 +67,7 @@ def parse_args():
     ap.add_argument("--workload", default="batched3", choices=["batched3", "plain2", "plain1", "plain0", "serve4", "vgbuild", "shadow"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-parity", action="store_true", help="skip the oracle check of the outputs after timing")
     ap.add_argument("--no-plain", action="store_true", help="batched3: skip the per-view plain comparison")
     ap.add_argument("--no-fold", action="store_true", help="shadow: skip the pass folded into the 85-view batch")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="bound of the CPU baseline sample")
@@ -156,6 +157,59 @@ def union_meshlets(scene, lods: np.ndarray) -> int:
 
 # ── Workloads ─────────────────────────────────────────────────────────────────
 
+def _u32(t) -> np.ndarray:
+    return t.cpu().numpy().view(np.uint32)
+
+
+class ParityTally:
+    """Counts the views whose outputs differ from the oracle's (the check is bit-exact:
+    pyramid texels compared as u32 words, every integer output element for element)
+    and sums the oracle's count of decisions inside the 1e-6 relative margin band."""
+
+    def __init__(self):
+        import time as _t
+
+        self.t0 = _t.perf_counter()
+        self.views = 0
+        self.bad_views = 0
+        self.fields = {}
+        self.marginal = {"decisions": 0, "meshlets": 0, "objects": 0}
+        self.tested = 0
+        self.visible = 0
+
+    def add_view(self, got: dict, levels: list, ref: dict, pairs: dict) -> None:
+        self.views += 1
+        bad = []
+        if len(got["levels"]) != len(levels) or any(
+                not np.array_equal(a.view(np.uint32), b.view(np.uint32)) for a, b in zip(got["levels"], levels)):
+            bad.append("levels")
+        for gk, rk in pairs.items():
+            a, b = np.asarray(got[gk]), np.asarray(ref[rk])
+            if rk == "counters":
+                a, b = a[:11], b[:11]
+            if a.shape != b.shape or not np.array_equal(a, b):
+                bad.append(gk)
+        for f in bad:
+            self.fields[f] = self.fields.get(f, 0) + 1
+        self.bad_views += 1 if bad else 0
+        st = ref["stats"]
+        self.marginal["decisions"] += int(st.marginal_decisions)
+        self.marginal["meshlets"] += int(st.marginal_meshlets)
+        self.marginal["objects"] += int(st.marginal_objects)
+        self.tested += int(st.meshlets_tested)
+        self.visible += int(ref["counters"][0])
+
+    def summary(self) -> dict:
+        import time as _t
+
+        return {"views": self.views, "mismatches": self.bad_views, "mismatched_fields": self.fields,
+                "marginal_decisions": self.marginal["decisions"], "marginal_meshlets": self.marginal["meshlets"],
+                "marginal_objects": self.marginal["objects"], "meshlet_tests": self.tested,
+                "visible_meshlets": self.visible, "band": "1e-6 relative",
+                "checker": "the oracle (CPU restatement of the reference shaders), bit-exact",
+                "seconds": round(_t.perf_counter() - self.t0, 2)}
+
+
 class PlainWorkload:
     """Single view through HiZBuildPass + VirtualGeometryPass (the drop-in passes)."""
 
@@ -244,6 +298,28 @@ class PlainWorkload:
 
         return run, h2d, stats
 
+    def parity(self, threads: int) -> dict:
+        """Checker leg (after the timed region): every view's pyramid, selected LODs,
+        counters, indirect args, draw records and visibility words against the oracle."""
+        from oracle import oracle as O
+        from helio_b200 import native as N
+
+        res = ParityTally()
+        for v, depth, cam, hz, vg in self.passes:
+            levels = O.hiz_build(v.depth)
+            o = vg.outputs()
+            c = _u32(o["counters"])
+            n = int(min(c[0], o["capacity"]))
+            got = {"levels": [hz.level(l).cpu().numpy() for l in range(len(levels))], "counters": c,
+                   "selected": _u32(o["objects"])[: len(self.scene.objects), 3].copy(),
+                   "indirect": _u32(o["indirect"])[:n], "draws": _u32(o["draws"])[:n],
+                   "visibility": _u32(o["visibility"])[: len(self.scene.work_items)]}
+            ref = O.run_view(self.scene, v.camera, v.width, v.height, levels, v.lod_threshold_px, o["capacity"], 11,
+                             threads, np.dtype(N.InstanceCullData))
+            res.add_view(got, levels, ref, {"selected": "selected", "counters": "counters", "indirect": "indirect",
+                                            "draws": "draws", "visibility": "visibility"})
+        return res.summary()
+
     def visible_draws(self) -> int:
         tot = 0
         for *_, vg in self.passes:
@@ -320,6 +396,48 @@ class BatchedWorkload:
             draws += int(min(c[0], o["capacity"]))
             lods.append(o["lod"].cpu().numpy()[: len(self.scene.objects)])
         return np.stack(lods), draws
+
+    def parity(self, threads: int) -> dict:
+        """Checker leg (after the timed region): every view of the batch against the
+        oracle: pyramid levels, selected LOD per object, counters, indirect args and
+        draw records in canonical order, and the view's active spans with their
+        visibility words."""
+        from oracle import oracle as O
+        from helio_b200 import native as N
+        from helio_b200.passes import device_view
+
+        res = ParityTally()
+        sp = self.batch.spans()
+        spans, start = _u32(sp["spans"]), _u32(sp["view_span_start"])
+        vis = _u32(sp["visibility"])
+        items, objs = self.scene.work_items, self.scene.objects
+        for i, v in enumerate(self.views):
+            o = self.batch.view_outputs(i)
+            c = _u32(o["counters"])
+            n = int(min(c[0], o["capacity"]))
+            pyr = o["pyramid"]
+            got = {"levels": [device_view(pyr.levels[l], (pyr.height[l], pyr.width[l]), "<f4",
+                                          (pyr.pitch[l] * 4, 4)).cpu().numpy() for l in range(pyr.mip_count)],
+                   "counters": c, "lod": o["lod"].cpu().numpy()[: len(objs)].astype(np.uint32),
+                   "indirect": _u32(o["indirect"])[:n], "draws": _u32(o["draws"])[:n]}
+            levels = O.hiz_build(v.depth)
+            ref = O.run_view(self.scene, v.camera, v.width, v.height, levels, v.lod_threshold_px, o["capacity"], 11,
+                             threads, np.dtype(N.InstanceCullData))
+            # The view's active spans (base below the selected LOD's count) in item order.
+            sel = ref["selected"][items["object_index"]]
+            lod = np.maximum(sel.astype(np.int64) - 1, 0)
+            cnt = np.where(sel > 0, objs["lod_meshlet_counts"][items["object_index"], lod], 0)
+            active = items["local_meshlet_base"] < cnt
+            sv = spans[start[i]:start[i + 1]]
+            real = (sv[:, 1] & 0x7F) > 0
+            got["span_objects"] = sv[real, 3]
+            got["span_visibility"] = vis[start[i]:start[i + 1]][real]
+            ref["span_objects"] = items["object_index"][active]
+            ref["span_visibility"] = ref["visibility"][active]
+            res.add_view(got, levels, ref, {"lod": "selected", "counters": "counters", "indirect": "indirect",
+                                            "draws": "draws", "span_objects": "span_objects",
+                                            "span_visibility": "span_visibility"})
+        return res.summary()
 
     def kernel_bytes(self) -> tuple[dict, int]:
         """Algorithmic bytes of the batched kernel: per view the Hi-Z (depth read + levels
@@ -636,6 +754,11 @@ def run_ours(args, rank, world, local_rank):
                    "sequential": sequential}
 
     cpu = cpu_baseline(wl.wl, args.cpu_seconds) if (rank == 0 and world == 1) else None
+    parity = None
+    if not args.no_parity:
+        # The checker, after everything timed: this rank's views against the oracle.
+        torch.cuda.synchronize()
+        parity = D.sum_parity(wl.parity(max(1, os.cpu_count() or 1)), dev)
     line = {
         "metric": "meshlets culled/s", "value": value, "unit": "meshlets/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
@@ -648,6 +771,7 @@ def run_ours(args, rank, world, local_rank):
         "latency_ms": {"p50": pct(step_ms, 0.5), "p99": pct(step_ms, 0.99)},
         "roofline": roofline, "kernels": kernels, "cpu_baseline": cpu, "e2e": e2e,
         "gpu_launches": int(launches_per_step * args.steps), "clocks": clk, "visible_draws_per_step": visible,
+        "parity": parity,
     }
     line.update(extra)
     return line

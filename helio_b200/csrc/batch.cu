@@ -24,9 +24,11 @@
 //   5  exclusive scan of the group counts
 //   6  emission of each view's draws at slot = position in the view's order
 //
-// Grid barriers and the Hi-Z hand-off use bounded waits: a barrier that is not
-// released after kSpinLimit polls sets kBatchErrTimeout and lets the CTA go on,
-// so the launch always ends; the host then reports HELIO_ERR_TIMEOUT.
+// Grid barriers and the wait for the published views are bounded: a wait that is not
+// released after spin_limit polls sets kBatchErrTimeout and ends its CTA (the others
+// end at their next barrier, and the second launch returns at once), so the launch
+// always ends and reads nothing a timed-out phase left incomplete; the host then
+// reports HELIO_ERR_TIMEOUT.
 
 #include "batch.h"
 #include "hiz_tile.cuh"
@@ -87,21 +89,28 @@ constexpr size_t kSm2Total = kSm2Misc + 64 * 4;
 __device__ __forceinline__ uint32_t ld_cg(const uint32_t* p) { return __ldcg(p); }
 
 // Grid barrier with a bounded wait (all CTAs are co-resident: cooperative launch).
-__device__ void grid_sync(const BatchParams& P) {
+// It releases once gridDim.x + P.barrier_extra CTAs have arrived (barrier_extra is 0
+// except in tests of the bounded wait). Returns false, uniformly over the CTA, when
+// the wait gave up after P.spin_limit polls: kBatchErrTimeout is set and the caller
+// must end the CTA, since the data of the phase before the barrier may be incomplete
+// (the other CTAs then time out at their next barrier and end too).
+__device__ bool grid_sync(const BatchParams& P) {
     __syncthreads();
+    int timed_out = 0;
     if (threadIdx.x == 0) {
         volatile uint32_t* gen = P.barrier + 1;
         const uint32_t g = *gen;
         __threadfence();
-        if (atomicAdd(P.barrier, 1u) == gridDim.x - 1) {
+        if (atomicAdd(P.barrier, 1u) == gridDim.x - 1 + P.barrier_extra) {
             P.barrier[0] = 0u;
             __threadfence();
             atomicAdd(P.barrier + 1, 1u);
         } else {
             uint32_t polls = 0;
             while (*gen == g) {
-                if (++polls > kSpinLimit) {
+                if (++polls > P.spin_limit) {
                     atomicOr(P.error, kBatchErrTimeout);
+                    timed_out = 1;
                     break;
                 }
                 __nanosleep(polls < 256 ? 64 : 256);
@@ -109,7 +118,7 @@ __device__ void grid_sync(const BatchParams& P) {
         }
         __threadfence();
     }
-    __syncthreads();
+    return __syncthreads_or(timed_out) == 0;
 }
 
 __device__ __forceinline__ uint32_t warp_inclusive(uint32_t x) {
@@ -155,7 +164,8 @@ __device__ uint32_t block_exclusive(uint32_t x, uint32_t* s, uint32_t& total) {
 }
 
 // out[i] = sum of in[0..i) for i <= n, over the whole grid (two grid barriers).
-__device__ void grid_exclusive_scan(const BatchParams& P, const uint32_t* in, uint32_t* out, uint32_t n,
+// Returns false when a barrier timed out (the CTA must end).
+__device__ bool grid_exclusive_scan(const BatchParams& P, const uint32_t* in, uint32_t* out, uint32_t n,
                                     uint32_t* s_tmp) {
     const uint32_t G = gridDim.x, b = blockIdx.x, tid = threadIdx.x;
     const uint32_t seg = (n + G - 1) / G;
@@ -164,7 +174,7 @@ __device__ void grid_exclusive_scan(const BatchParams& P, const uint32_t* in, ui
     for (uint32_t i = b0 + tid; i < b1; i += kBatchThreads) sum += ld_cg(in + i);
     sum = block_sum(sum, s_tmp);
     if (tid == 0) P.seg_totals[b] = sum;
-    grid_sync(P);
+    if (!grid_sync(P)) return false;
     uint32_t base = 0;
     for (uint32_t k = tid; k < b; k += kBatchThreads) base += ld_cg(P.seg_totals + k);
     base = block_sum(base, s_tmp);
@@ -177,7 +187,7 @@ __device__ void grid_exclusive_scan(const BatchParams& P, const uint32_t* in, ui
         base += total;
     }
     if (b == G - 1 && tid == 0) out[n] = base;
-    grid_sync(P);
+    return grid_sync(P);
 }
 
 // ── Reject box of a view ──────────────────────────────────────────────────────
@@ -928,20 +938,23 @@ __device__ __forceinline__ void stamp(const BatchParams& P, int k) {
 }
 
 // The views' select constants and reject boxes into shared memory, once the view setup
-// has published all of them (thread 0 waits, bounded, for the counter).
-__device__ void load_sel_views(const BatchParams& P, char* sm) {
+// has published all of them (thread 0 waits, bounded, for the counter). Returns false,
+// uniformly over the CTA, when the wait gave up (kBatchErrTimeout set; the CTA must end).
+__device__ bool load_sel_views(const BatchParams& P, char* sm) {
+    int timed_out = 0;
     if (threadIdx.x == 0) {
         uint32_t polls = 0;
         while (ld_cg(P.setup_done) < P.view_count) {
-            if (++polls > kSpinLimit) {
+            if (++polls > P.spin_limit) {
                 atomicOr(P.error, kBatchErrTimeout);
+                timed_out = 1;
                 break;
             }
             __nanosleep(polls < 256 ? 64 : 256);
         }
         __threadfence();
     }
-    __syncthreads();
+    if (__syncthreads_or(timed_out)) return false;
     SelView* s_sv = reinterpret_cast<SelView*>(sm + kSmSelViews);
     for (uint32_t k = threadIdx.x; k < P.view_count; k += kBatchThreads) {
         const CullView* cvp = P.cviews + k;
@@ -966,6 +979,7 @@ __device__ void load_sel_views(const BatchParams& P, char* sm) {
         reinterpret_cast<SelBox*>(sm + kSmSelBox)[k] = bx;
     }
     __syncthreads();
+    return true;
 }
 
 __global__ void __launch_bounds__(kBatchThreads, 3) batch_kernel(const __grid_constant__ BatchParams P) {
@@ -1037,7 +1051,7 @@ __global__ void __launch_bounds__(kBatchThreads, 3) batch_kernel(const __grid_co
                 phase_hiz_tile(P, u < h0 ? u : (mid ? h0 + ur - sel_before : u - sel_units), sm);
             } else {
                 if (!have_views) {
-                    load_sel_views(P, sm);
+                    if (!load_sel_views(P, sm)) return;
                     have_views = true;
                 }
                 const uint32_t chunk = sel_before / vgroups, vg = sel_before - chunk * vgroups;
@@ -1054,7 +1068,7 @@ __global__ void __launch_bounds__(kBatchThreads, 3) batch_kernel(const __grid_co
             atomicMax(P.phase_ns + 9, t_sel);
         }
     }
-    grid_sync(P);
+    if (!grid_sync(P)) return;
     stamp(P, 2);
     // The attached shadow cull's scan: CTA j takes the j-th dirty face (and clears face
     // j's count when face j is clean); done before the phase's last barrier.
@@ -1062,7 +1076,7 @@ __global__ void __launch_bounds__(kBatchThreads, 3) batch_kernel(const __grid_co
         for (uint32_t j = blockIdx.x; j < kShadowFaces; j += gridDim.x)
             shadow_scan_face(P.shadow, j, *reinterpret_cast<ShadowSmem*>(sm + kSmShadow));
 
-    grid_exclusive_scan(P, P.chunk_counts, P.chunk_offs, P.view_count * P.object_chunks, s_tmp);
+    if (!grid_exclusive_scan(P, P.chunk_counts, P.chunk_offs, P.view_count * P.object_chunks, s_tmp)) return;
     stamp(P, 3);
     phase_expand(P, sm);
 }
@@ -1073,14 +1087,16 @@ __global__ void __launch_bounds__(kBatchThreads, 3) batch_kernel(const __grid_co
 __global__ void __launch_bounds__(kBatchThreads, 4) batch_cull_kernel(BatchParams P) {
     extern __shared__ __align__(16) char sm[];
     uint32_t* s_tmp = reinterpret_cast<uint32_t*>(sm + kSm2Misc);
+    // A barrier of the first launch gave up: its span list may be incomplete.
+    if (ld_cg(P.error) & kBatchErrTimeout) return;
     stamp(P, 4);
     const uint32_t total_spans = min(ld_cg(P.view_span_start + P.view_count), P.span_capacity);
     const uint32_t groups = total_spans >> 5;
     phase_test(P, groups, sm);
-    grid_sync(P);
+    if (!grid_sync(P)) return;
     stamp(P, 5);
 
-    grid_exclusive_scan(P, P.group_counts, P.group_offs, groups, s_tmp);
+    if (!grid_exclusive_scan(P, P.group_counts, P.group_offs, groups, s_tmp)) return;
     stamp(P, 6);
     phase_emit(P, groups);
     // End of the launch: the latest block end (no barrier needed).

@@ -55,6 +55,8 @@ struct BatchParams {
     uint32_t object_chunks;   // ceil(object_count / kBatchChunk)
     uint32_t hiz_tiles;       // Hi-Z units of all views: pairs of horizontally consecutive tiles
     uint32_t* barrier;        // [2] arrival count (zero before the launch), generation
+    uint32_t spin_limit;      // polls before a bounded wait gives up (kSpinLimit by default)
+    uint32_t barrier_extra;   // arrivals a grid barrier waits for beyond the grid (0; tests only)
     uint32_t* error;          // [1] kBatchErr* bits, zero before the launch
     uint32_t* work;           // [1] phase-1 work queue head, zero before the launch
     uint32_t* setup_done;     // [1] views whose constants are published, zero before the launch

@@ -54,6 +54,8 @@ struct helio_batch {
     std::vector<size_t> out_offset;  // first draw of each view in out_indirect / out_draws
     bool prepared = false;
     helio_shadow_cull_pass* shadow = nullptr;  // attached per-face shadow cull, or null
+    uint32_t spin_limit = helio::kSpinLimit;  // helio_batch_set_wait_limit
+    uint32_t barrier_extra = 0;
 
     // Buffer k of the plan's order (kBuf* below).
     DevBuf& buf(int k) {
@@ -494,6 +496,8 @@ int32_t helio_batch_execute(helio_batch* b, void* stream) {
     P.object_chunks = b->object_chunks;
     P.hiz_tiles = b->hiz_tiles;
     P.barrier = b->barrier();
+    P.spin_limit = b->spin_limit;
+    P.barrier_extra = b->barrier_extra;
     P.error = b->error();
     P.work = b->work();
     P.setup_done = b->setup_done();
@@ -567,6 +571,13 @@ int32_t helio_batch_get_spans(const helio_batch* b, helio_batch_span_list* out) 
     out->view_span_start = b->view_span_start.as<uint32_t>();
     out->span_capacity = b->span_capacity;
     out->view_count = b->view_count;
+    return HELIO_OK;
+}
+
+int32_t helio_batch_set_wait_limit(helio_batch* b, uint32_t max_polls, uint32_t extra_arrivals) {
+    HELIO_ARG(b, "null pointer");
+    b->spin_limit = max_polls ? max_polls : helio::kSpinLimit;
+    b->barrier_extra = extra_arrivals;
     return HELIO_OK;
 }
 

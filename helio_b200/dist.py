@@ -66,3 +66,27 @@ def sum_over_ranks(value: int, device=None) -> int:
     t = torch.tensor([int(value)], dtype=torch.int64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.SUM)
     return int(t.item())
+
+
+def sum_parity(summary: dict | None, device=None) -> dict | None:
+    """Merges per-rank parity summaries (counts summed, mismatched fields merged, the
+    slowest rank's check time) so that rank 0 reports the whole job's check."""
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return summary
+    parts: list = [None] * dist.get_world_size()
+    dist.all_gather_object(parts, summary)
+    parts = [p for p in parts if p]
+    if not parts:
+        return None
+    out = dict(parts[0])
+    for k in ("views", "mismatches", "marginal_decisions", "marginal_meshlets", "marginal_objects", "meshlet_tests",
+              "visible_meshlets"):
+        out[k] = sum(int(p.get(k, 0)) for p in parts)
+    fields: dict = {}
+    for p in parts:
+        for f, n in p.get("mismatched_fields", {}).items():
+            fields[f] = fields.get(f, 0) + n
+    out["mismatched_fields"] = fields
+    out["seconds"] = max(float(p.get("seconds", 0.0)) for p in parts)
+    out["ranks"] = len(parts)
+    return out

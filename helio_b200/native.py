@@ -286,6 +286,7 @@ CULL_EXPORTS = {
     "helio_batch_execute": (i32, [vp, vp]),
     "helio_batch_get_view_outputs": (i32, [vp, u32, C.POINTER(BatchViewOutputs)]),
     "helio_batch_get_spans": (i32, [vp, C.POINTER(BatchSpanList)]),
+    "helio_batch_set_wait_limit": (i32, [vp, u32, u32]),
     "helio_batch_status": (i32, [vp, vp]),
     "helio_batch_get_phase_times": (i32, [vp, C.POINTER(C.c_double), u32, C.POINTER(u32), vp]),
     "helio_batch_estimate_bytes": (i32, [C.POINTER(BatchConfig), vp, u32, C.POINTER(BatchView), C.POINTER(u64)]),

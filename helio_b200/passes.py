@@ -429,6 +429,11 @@ class BatchedCull:
     def status(self, stream=None) -> None:
         N.check(self._lib.helio_batch_status(self._h, _stream_ptr(stream)))
 
+    def set_wait_limit(self, max_polls: int = 0, extra_arrivals: int = 0) -> None:
+        """Bounds of the device waits (0 = default, about 1 s); extra_arrivals > 0 makes
+        every grid barrier wait for CTAs that never arrive (tests of the bounded waits)."""
+        N.check(self._lib.helio_batch_set_wait_limit(self._h, max_polls, extra_arrivals))
+
     PHASES = ("view_setup", "hiz_and_select", "span_count_scan", "span_expand", "meshlet_test",
               "group_count_scan", "emit", "max_cta_hiz_busy", "max_cta_select_busy")
 

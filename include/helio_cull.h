@@ -556,6 +556,16 @@ int32_t helio_batch_get_phase_times(helio_batch* batch, double* us_out, uint32_t
 /* Synchronises `stream`; HELIO_ERR_TIMEOUT if a bounded grid barrier gave up,
  * HELIO_ERR_CAPACITY if the active spans exceeded max_spans (outputs incomplete). */
 int32_t helio_batch_status(helio_batch* batch, void* stream);
+/* Bounds of the batch's device waits (the reference has no device-side waits: its
+ * passes are separate dispatches, crates/helio-core/src/graph/execution.rs:504-598).
+ * Every grid barrier and the wait for the published views give up after max_polls
+ * polls (0 = the default, about 1 s), set the timeout bit and end their CTA; the
+ * second launch then returns at once, and helio_batch_status reports
+ * HELIO_ERR_TIMEOUT (that execute's outputs are invalid; the next execute starts
+ * clean). extra_arrivals > 0 makes every grid barrier wait for that many CTAs beyond
+ * the grid, which never arrive: a way to run the bounded waits out in tests (0 in
+ * normal use). Applies from the next execute. */
+int32_t helio_batch_set_wait_limit(helio_batch* batch, uint32_t max_polls, uint32_t extra_arrivals);
 /* Device bytes helio_batch_prepare would allocate for these views of `scene` (a
  * batch grows its buffers and never shrinks them). For admission against a memory budget. */
 int32_t helio_batch_estimate_bytes(const helio_batch_config* config, const helio_vg_scene* scene, uint32_t view_count,

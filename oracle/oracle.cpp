@@ -78,14 +78,21 @@ uint32_t ceil_log2_exact(float d) {
     return mant == 0u ? e : e + 1u;
 }
 
-// Marginal when d sits within the relative band of a power of two.
-void mip_margin(float d, Marg& mg) {
-    if (!(d >= 1.0f) || d >= 4294967296.0f) return;
-    uint32_t k = ceil_log2_exact(d);
+// Marginal when the mip's argument sits within the relative band of a power of two.
+// `raw` is the value before the max(.., 1) clamp: a clamped 1.0 decides mip 0 however
+// far below 1 the raw value lies, so only a raw value near 1 (or near a higher power
+// of two) makes the mip choice marginal.
+void mip_margin(float raw, Marg& mg) {
+    if (!(raw >= 0.0f) || raw >= 4294967296.0f) return;
+    if (raw < 1.0f) {
+        mg.cmp(raw, 1.0f);
+        return;
+    }
+    uint32_t k = ceil_log2_exact(raw);
     float hi = ldexpf(1.0f, (int)k);
     float lo = ldexpf(1.0f, (int)k - 1);
-    mg.cmp(d, hi);
-    if (k > 0) mg.cmp(d, lo);
+    mg.cmp(raw, hi);
+    if (k > 0) mg.cmp(raw, lo);
 }
 
 float sample_nearest(const helio_hiz_pyramid* hz, float u, float v, uint32_t mip) {
@@ -455,7 +462,7 @@ void oracle_occlusion_cull_static(const HelioGpuCameraUniforms* cam, uint32_t sc
         float r_px = fabsf(((radius / clip[3]) * P11) * half_h);
         float diameter = fmaxf(r_px * 2.0f, 1.0f);
         uint32_t mip = std::min(ceil_log2_exact(diameter), mip_count - 1u);
-        mip_margin(diameter, mg);
+        mip_margin(r_px * 2.0f, mg);
         float uv_half = ndc_r * 0.5f;
         float u0 = clampf(uv_x - uv_half, 0.0f, 1.0f), v0 = clampf(uv_y - uv_half, 0.0f, 1.0f);
         float u1 = clampf(uv_x + uv_half, 0.0f, 1.0f), v1 = clampf(uv_y + uv_half, 0.0f, 1.0f);
@@ -589,7 +596,7 @@ MeshletVerdict cull_one(const CullCtx& C, const HelioGpuMeshletEntry& m,
     // Cone (:159-182)
     float cam_dist_sq = dot3(ctc, ctc);
     float guard = wr * 1.5f;
-    mg.cmp(cam_dist_sq, guard * guard);
+    if (m.cone_cutoff <= 1.0f && cd.cone_cull_enabled != 0u) mg.cmp(cam_dist_sq, guard * guard);
     if (cam_dist_sq > guard * guard && m.cone_cutoff <= 1.0f && cd.cone_cull_enabled != 0u) {
         const float* n = in.normal_mat;
         V3 ax = v3((n[0] * m.cone_axis[0] + n[4] * m.cone_axis[1]) + n[8] * m.cone_axis[2],
@@ -638,7 +645,7 @@ MeshletVerdict cull_one(const CullCtx& C, const HelioGpuMeshletEntry& m,
                 }
                 float half_h = (float)C.u->screen_height * 0.5f;
                 float dpx = fmaxf((ndc_r * half_h) * 2.0f, 1.0f);
-                mip_margin(dpx, mg);
+                mip_margin((ndc_r * half_h) * 2.0f, mg);
                 uint32_t mip = std::min(ceil_log2_exact(dpx), C.u->hiz_mip_count - 1u);
                 float h00 = sample_nearest(C.hiz, u0, v0, mip);
                 float h01 = sample_nearest(C.hiz, u1, v0, mip);

@@ -1,9 +1,16 @@
 """Shared drivers of the CUDA path (through the C-ABI) and of the oracle, for the tests."""
 from __future__ import annotations
 
+import os
+
 import numpy as np
 
 from oracle import oracle as O
+
+
+def oracle_threads() -> int:
+    """Host threads for the oracle's select / cull (its merge is deterministic)."""
+    return max(1, os.cpu_count() or 1)
 
 
 def u32(t) -> np.ndarray:
@@ -70,9 +77,9 @@ def gpu_vg_view(scene, view, hz=None, lod_quality=1, publication_limit=0, counte
     }
 
 
-def oracle_vg_view(scene, view, levels, lod_threshold=2.0, capacity=None, counter_count=11, threads=4):
+def oracle_vg_view(scene, view, levels, lod_threshold=2.0, capacity=None, counter_count=11, threads=None):
     return O.run_view(scene, view.camera, view.width, view.height, levels, lod_threshold, capacity, counter_count,
-                      threads, cull_dtype())
+                      threads or oracle_threads(), cull_dtype())
 
 
 def assert_vg_equal(g, o, counter_count=11):
@@ -179,3 +186,88 @@ def kat_work_spans_library(k: dict):
     m["lod_count"] = 1
     m["max_meshlet_count"] = [mx for _, mx in k["objects"]]
     return S.Library(pool, m, np.arange(n, dtype=np.uint32), np.zeros(n, S.DT_INSTANCE))
+
+
+# ── batched multi-view cull ──────────────────────────────────────────────────
+
+def run_batch(scene, views, span_visibility=True, alias=False, capacities=None, repeats=1, max_ctas=0):
+    import torch
+    from helio_b200 import scene as S
+    from helio_b200.passes import BatchedCull, VgScene
+
+    vs = VgScene()
+    vs.upload(S.frame_data(scene))
+    depths = [torch.from_numpy(np.ascontiguousarray(v.depth)).cuda() for v in views]
+    b = BatchedCull(len(views), span_visibility=span_visibility, max_ctas=max_ctas)
+    specs = []
+    for i, (v, d) in enumerate(zip(views, depths)):
+        spec = {"camera": v.camera, "depth": d, "alias_mip0": alias, "lod_threshold_px": v.lod_threshold_px}
+        if capacities:
+            spec["draw_capacity"] = capacities[i]
+        specs.append(spec)
+    b.prepare(vs, specs)
+    for _ in range(repeats):
+        b.execute()
+    torch.cuda.synchronize()
+    b.status()
+    return b, vs, depths
+
+
+def gather(b, v, n_objects):
+    from helio_b200.passes import device_view
+
+    o = b.view_outputs(v)
+    counters = u32(o["counters"])
+    n = int(min(counters[0], o["capacity"]))
+    p = o["pyramid"]
+    levels = [device_view(p.levels[l], (p.height[l], p.width[l]), "<f4", (p.pitch[l] * 4, 4)).cpu().numpy()
+              for l in range(p.mip_count)]
+    return {"counters": counters, "indirect": u32(o["indirect"])[:n], "draws": u32(o["draws"])[:n],
+            "lod": o["lod"].cpu().numpy()[:n_objects].astype(np.uint32), "levels": levels, "capacity": o["capacity"]}
+
+
+def check_view(scene, view, got, spans_view, vis_view, cap):
+    """One view of a batch against the oracle: every pyramid level, selected LOD per
+    object, counters, indirect args and draws in canonical order, and (when given) the
+    view's active spans and their visibility words. Returns the oracle's statistics."""
+    levels = O.hiz_build(view.depth)
+    for l, (a, r) in enumerate(zip(got["levels"], levels)):
+        np.testing.assert_array_equal(a.view(np.uint32), r.view(np.uint32), err_msg=f"level {l}")
+    ref = O.run_view(scene, view.camera, view.width, view.height, levels, view.lod_threshold_px, cap, 11,
+                     oracle_threads(), cull_dtype())
+    np.testing.assert_array_equal(got["lod"], ref["selected"], err_msg="selected LOD + 1")
+    np.testing.assert_array_equal(got["counters"], ref["counters"], err_msg="counters")
+    np.testing.assert_array_equal(got["indirect"], ref["indirect"], err_msg="indirect")
+    np.testing.assert_array_equal(got["draws"], ref["draws"], err_msg="draws")
+    if spans_view is not None:
+        # active work items (span base below the selected LOD's count), in order
+        items = scene.work_items
+        sel = ref["selected"][items["object_index"]]
+        lod = np.maximum(sel.astype(np.int64) - 1, 0)
+        cnt = np.where(sel > 0, scene.objects["lod_meshlet_counts"][items["object_index"], lod], 0)
+        active = items["local_meshlet_base"] < cnt
+        real = spans_view[(spans_view[:, 1] & 0x7F) > 0]
+        assert len(real) == int(active.sum())
+        np.testing.assert_array_equal(real[:, 3], items["object_index"][active], err_msg="span objects")
+        if vis_view is not None:
+            np.testing.assert_array_equal(vis_view[(spans_view[:, 1] & 0x7F) > 0], ref["visibility"][active],
+                                          err_msg="span visibility")
+    return ref["stats"]
+
+
+def check_batch(w, views, **kw):
+    """Runs a batch over `views` of workload w and checks every view against the oracle."""
+    b, vs, _ = run_batch(w.scene, views, **kw)
+    sp = b.spans()
+    spans = u32(sp["spans"])
+    start = u32(sp["view_span_start"])
+    vis = u32(sp["visibility"]) if "visibility" in sp else None
+    totals = {"marginal_decisions": 0, "meshlets_tested": 0}
+    for i, v in enumerate(views):
+        got = gather(b, i, len(w.scene.objects))
+        sv = spans[start[i]:start[i + 1]]
+        st = check_view(w.scene, v, got, sv, vis[start[i]:start[i + 1]] if vis is not None else None, got["capacity"])
+        totals["marginal_decisions"] += st.marginal_decisions
+        totals["meshlets_tested"] += st.meshlets_tested
+    b._parity_stats = totals
+    return b

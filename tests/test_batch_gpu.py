@@ -4,84 +4,9 @@ the canonical (object, span, lane) order, and the per-span visibility words."""
 import numpy as np
 import pytest
 
-from helpers import benchmark_scene, cull_dtype, u32
-from oracle import oracle as O
+from helpers import benchmark_scene, check_batch as _check_batch, check_view, gather, run_batch, u32
 
 pytestmark = pytest.mark.gpu
-
-
-def run_batch(scene, views, span_visibility=True, alias=False, capacities=None, repeats=1, max_ctas=0):
-    import torch
-    from helio_b200 import scene as S
-    from helio_b200.passes import BatchedCull, VgScene
-
-    vs = VgScene()
-    vs.upload(S.frame_data(scene))
-    depths = [torch.from_numpy(np.ascontiguousarray(v.depth)).cuda() for v in views]
-    b = BatchedCull(len(views), span_visibility=span_visibility, max_ctas=max_ctas)
-    specs = []
-    for i, (v, d) in enumerate(zip(views, depths)):
-        spec = {"camera": v.camera, "depth": d, "alias_mip0": alias, "lod_threshold_px": v.lod_threshold_px}
-        if capacities:
-            spec["draw_capacity"] = capacities[i]
-        specs.append(spec)
-    b.prepare(vs, specs)
-    for _ in range(repeats):
-        b.execute()
-    torch.cuda.synchronize()
-    b.status()
-    return b, vs, depths
-
-
-def gather(b, v, n_objects):
-    from helio_b200.passes import device_view
-
-    o = b.view_outputs(v)
-    counters = u32(o["counters"])
-    n = int(min(counters[0], o["capacity"]))
-    p = o["pyramid"]
-    levels = [device_view(p.levels[l], (p.height[l], p.width[l]), "<f4", (p.pitch[l] * 4, 4)).cpu().numpy()
-              for l in range(p.mip_count)]
-    return {"counters": counters, "indirect": u32(o["indirect"])[:n], "draws": u32(o["draws"])[:n],
-            "lod": o["lod"].cpu().numpy()[:n_objects].astype(np.uint32), "levels": levels, "capacity": o["capacity"]}
-
-
-def check_view(scene, view, got, spans_view, vis_view, cap):
-    levels = O.hiz_build(view.depth)
-    for l, (a, r) in enumerate(zip(got["levels"], levels)):
-        np.testing.assert_array_equal(a.view(np.uint32), r.view(np.uint32), err_msg=f"level {l}")
-    ref = O.run_view(scene, view.camera, view.width, view.height, levels, view.lod_threshold_px, cap, 11, 4,
-                     cull_dtype())
-    np.testing.assert_array_equal(got["lod"], ref["selected"], err_msg="selected LOD + 1")
-    np.testing.assert_array_equal(got["counters"], ref["counters"], err_msg="counters")
-    np.testing.assert_array_equal(got["indirect"], ref["indirect"], err_msg="indirect")
-    np.testing.assert_array_equal(got["draws"], ref["draws"], err_msg="draws")
-    if spans_view is not None:
-        # active work items (span base below the selected LOD's count), in order
-        items = scene.work_items
-        sel = ref["selected"][items["object_index"]]
-        lod = np.maximum(sel.astype(np.int64) - 1, 0)
-        cnt = np.where(sel > 0, scene.objects["lod_meshlet_counts"][items["object_index"], lod], 0)
-        active = items["local_meshlet_base"] < cnt
-        real = spans_view[(spans_view[:, 1] & 0x7F) > 0]
-        assert len(real) == int(active.sum())
-        np.testing.assert_array_equal(real[:, 3], items["object_index"][active], err_msg="span objects")
-        if vis_view is not None:
-            np.testing.assert_array_equal(vis_view[(spans_view[:, 1] & 0x7F) > 0], ref["visibility"][active],
-                                          err_msg="span visibility")
-
-
-def _check_batch(w, views, **kw):
-    b, vs, _ = run_batch(w.scene, views, **kw)
-    sp = b.spans()
-    spans = u32(sp["spans"])
-    start = u32(sp["view_span_start"])
-    vis = u32(sp["visibility"]) if "visibility" in sp else None
-    for i, v in enumerate(views):
-        got = gather(b, i, len(w.scene.objects))
-        sv = spans[start[i]:start[i + 1]]
-        check_view(w.scene, v, got, sv, vis[start[i]:start[i + 1]] if vis is not None else None, got["capacity"])
-    return b
 
 
 def test_batch_85_views_matches_oracle(cuda):

@@ -46,7 +46,7 @@ def exact_cone_dot(scene, cam_pos):
 
 def test_cone_cutoff_on_the_boundary():
     from helio_b200 import scene as S
-    from test_batch_gpu import gather, run_batch
+    from helpers import gather, run_batch
 
     w = S.config(1, scale=0.05)
     sc, view = w.scene, w.views[0]

@@ -54,7 +54,7 @@ def boundary_workload():
 
 
 def test_threshold_boundary_single_view_and_batched():
-    from test_batch_gpu import gather, run_batch
+    from helpers import gather, run_batch
 
     w, levels, ref, visible = boundary_workload()
     scene, view = w.scene, w.views[0]

@@ -55,7 +55,7 @@ def boundary_scene(views, seed=7):
 
 def test_reject_box_keeps_every_visible_pair():
     from helio_b200 import scene as S
-    from test_batch_gpu import gather, run_batch
+    from helpers import gather, run_batch
 
     mv = S.multiview_set(11, depth=True, scale=0.05)
     views = [mv[0], mv[1], mv[5], mv[6], mv[21], mv[30]]  # main, a cascade, two spots, two probes

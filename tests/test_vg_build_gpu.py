@@ -144,7 +144,7 @@ def test_built_scene_culls_like_the_oracle(cuda):
     import torch
     from helio_b200 import scene as S
     from helio_b200.passes import BatchedCull, VgScene
-    from test_batch_gpu import check_view, gather
+    from helpers import check_view, gather
 
     w = S.config(1, scale=0.05)
     lib = S.library_from_scene(w.scene, free_slots=0.2, seed=3)
