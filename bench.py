@@ -32,9 +32,11 @@ Workloads
 CUDA events on the launching stream, L2 flushed between timed steps. `e2e` runs the
 same step through the C-ABI with host buffers: every view's depth and camera copied
 in from pinned memory and the counters and visible draws copied out, inside the
-timed region. Multi-GPU (torchrun): every rank runs its own replica of the workload
-(independent frames, no collective on the data path): weak scaling, time = max over
-ranks. `--impl reference` times the CPU restatement of the reference shaders (the
+timed region. Multi-GPU (torchrun), with no collective on the data path and time =
+max over ranks: batched3 splits its 85 views across the GPUs by estimated cost, every
+GPU holding the scene (strong scaling); serve4 assigns the requests of one stream to
+the GPUs by cost as they arrive (weak scaling: the stream's rate grows with the GPU
+count); the single-view workloads run one replica per GPU (weak scaling). `--impl reference` times the CPU restatement of the reference shaders (the
 oracle) on the host cores, on rank 0 only.
 """
 from __future__ import annotations
@@ -213,6 +215,8 @@ class ParityTally:
 class PlainWorkload:
     """Single view through HiZBuildPass + VirtualGeometryPass (the drop-in passes)."""
 
+    sharded = False  # one view: several GPUs run replicas
+
     def __init__(self, name, dev):
         import torch
         from helio_b200 import scene as S
@@ -331,16 +335,25 @@ class PlainWorkload:
 class BatchedWorkload:
     """85 views against one device-resident scene in one cooperative launch."""
 
-    def __init__(self, dev, with_plain=True):
+    sharded = True  # several GPUs split the 85 views
+
+    def __init__(self, dev, with_plain=True, rank=0, world=1):
         import torch
+        from helio_b200 import dist as D
         from helio_b200 import scene as S
         from helio_b200.passes import BatchedCull, HiZBuildPass, VgScene, VirtualGeometryPass, camera_bytes
 
         self.name = "batched3"
         self.wl = S.config(3)
         self.scene = self.wl.scene
-        self.views = self.wl.views
+        self.all_views = self.wl.views
+        # Several GPUs: every rank holds the scene and culls its cost-balanced share of
+        # the 85 views in a batch of its own (no collective on the data path).
+        self.mine = D.shard_views(self.all_views, self.scene.lod0_total, world, rank) if world > 1 else \
+            list(range(len(self.all_views)))
+        self.views = [self.all_views[i] for i in self.mine]
         self.units = self.scene.lod0_total * len(self.views)
+        self.total_units = self.scene.lod0_total * len(self.all_views)
         self.vscene = VgScene()
         self.vscene.upload(S.frame_data(self.scene))
         # Every view's depth in one device buffer (each slice starts 16-byte aligned), so
@@ -386,7 +399,7 @@ class BatchedWorkload:
     def describe(self):
         return (f"batched3: {len(self.scene.objects)} instances x {self.scene.lod0_meshlets} LOD0 meshlets "
                 f"(10M), 85 views (1x 3840x2160, 4x 2048^2 orthographic, 16x 512^2 spot, 64x 128^2 probe), "
-                f"one cooperative launch, Hi-Z level 0 = the view's depth")
+                f"one cooperative launch per GPU, Hi-Z level 0 = the view's depth")
 
     def outputs(self):
         lods, draws = [], 0
@@ -591,8 +604,8 @@ class BatchedWorkload:
         return t0.elapsed_time(t1), int(host_in.numel()) * 4, d2h // steps
 
 
-def build_workload(name, dev, with_plain):
-    return BatchedWorkload(dev, with_plain) if name == "batched3" else PlainWorkload(name, dev)
+def build_workload(name, dev, with_plain, rank=0, world=1):
+    return BatchedWorkload(dev, with_plain, rank, world) if name == "batched3" else PlainWorkload(name, dev)
 
 
 # ── Timing ────────────────────────────────────────────────────────────────────
@@ -663,7 +676,10 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     lib = N.cull_lib()
-    wl = build_workload(args.workload, dev, not args.no_plain)
+    wl = build_workload(args.workload, dev, not args.no_plain, rank, world)
+    # Units of the whole job per step: the 85 views once when they are split across
+    # GPUs (strong scaling), every rank's replica otherwise (weak scaling).
+    job_units = D.sum_over_ranks(wl.units, dev) if world > 1 else wl.units
     timer = Timer(dev)
 
     wl.step()
@@ -680,7 +696,7 @@ def run_ours(args, rank, world, local_rank):
     step_ms, graphed = timer.run(wl.step, args.steps, args.warmup)
     clk = clocks.stop()
     total_ms = D.max_over_ranks(sum(step_ms), dev)
-    value = wl.units * args.steps * world / (total_ms / 1e3)
+    value = job_units * args.steps / (total_ms / 1e3)
 
     # Per-kernel device time (event profiler around every launch, eager, queued ahead).
     lib.helio_profiler_reset()
@@ -722,7 +738,7 @@ def run_ours(args, rank, world, local_rank):
     if getattr(wl, "plain", None) is not None:
         plain_ms, plain_graphed = timer.run(wl.plain, max(3, args.steps // 4), args.warmup)
         pm = D.max_over_ranks(sum(plain_ms), dev) / len(plain_ms)
-        extra["plain_per_view"] = {"ms_per_step": pm, "value": wl.units / (pm / 1e3), "unit": "meshlets/s",
+        extra["plain_per_view"] = {"ms_per_step": pm, "value": job_units / (pm / 1e3), "unit": "meshlets/s",
                                    "graph": plain_graphed, "views": len(wl.views),
                                    "batched_speedup": pm / (total_ms / args.steps)}
 
@@ -740,14 +756,14 @@ def run_ours(args, rank, world, local_rank):
             ee[k][1].record()
         torch.cuda.synchronize()
         e2e_ms = D.max_over_ranks(float(sum(a.elapsed_time(b) for a, b in ee)), dev)
-        e2e = {"value": wl.units * args.steps * world / (e2e_ms / 1e3), "unit": "meshlets/s",
+        e2e = {"value": job_units * args.steps / (e2e_ms / 1e3), "unit": "meshlets/s",
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": int(stats["d2h"] / args.steps),
                "ms_per_step": e2e_ms / args.steps, "form": "one frame at a time (copy in, cull, copy out)"}
         if hasattr(wl, "e2e_pipelined"):
             pms, ph2d, pd2h = wl.e2e_pipelined(args.steps, max(args.warmup, 3))
             pms = D.max_over_ranks(pms, dev)
             sequential = e2e
-            e2e = {"value": wl.units * args.steps * world / (pms / 1e3), "unit": "meshlets/s",
+            e2e = {"value": job_units * args.steps / (pms / 1e3), "unit": "meshlets/s",
                    "h2d_bytes_per_step": ph2d, "d2h_bytes_per_step": pd2h, "ms_per_step": pms / args.steps,
                    "form": "a stream of frames: frame k+1's depths copied in on a second stream while frame k is "
                            "culled and its draws copied out (inputs of 121 MB per frame exceed L2)",
@@ -762,12 +778,16 @@ def run_ours(args, rank, world, local_rank):
     line = {
         "metric": "meshlets culled/s", "value": value, "unit": "meshlets/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator)",
-        "config": {"workload": wl.describe(), "views": len(wl.views), "lod0_meshlets_per_view": wl.scene.lod0_total,
+        "scaling": "strong" if wl.sharded else "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded generator)",
+        "config": {"workload": wl.describe(), "views": len(getattr(wl, "all_views", wl.views)),
+                   "lod0_meshlets_per_view": wl.scene.lod0_total,
                    "l2": "flushed between timed steps (256 MB write, then 256 MB read)",
                    "timing": ("CUDA-graph replay of the whole step" if graphed else "eager launches") +
                              ", CUDA events on the launching stream",
-                   "parallelism": f"replica x{world}" if world > 1 else "single GPU"},
+                   "parallelism": ("single GPU" if world == 1 else
+                                   f"views split by estimated cost over {world} GPUs (scene replicated)"
+                                   if wl.sharded else f"replica x{world}")},
         "latency_ms": {"p50": pct(step_ms, 0.5), "p99": pct(step_ms, 0.99)},
         "roofline": roofline, "kernels": kernels, "cpu_baseline": cpu, "e2e": e2e,
         "gpu_launches": int(launches_per_step * args.steps), "clocks": clk, "visible_draws_per_step": visible,
@@ -833,8 +853,14 @@ def run_serve(args, rank, world, local_rank):
     ids = [loop.add_scene(vs) for vs in vgs]
     warm = max(3, args.warmup) * 20
     total = warm + args.requests
-    # Replicas: rank r serves every world-th request of the same stream (weak scaling).
-    reqs = S.serving_requests(total * world, args.rate * world)[rank::world]
+    # Several GPUs: one stream at world times the rate (weak scaling), each request
+    # assigned on arrival to the GPU with the least estimated work so far.
+    reqs = S.serving_requests(total * world, args.rate * world)
+    if world > 1:
+        costs = [sum(D.view_cost(pool[p].width, pool[p].height, scenes[r.scene].lod0_total) for p in r.views)
+                 for r in reqs]
+        owner = D.assign_online(costs, world)
+        reqs = [r for r, o in zip(reqs, owner) if o == rank]
     specs = [[{"camera": pool[p].camera, "depth": depths[p], "alias_mip0": True,
                "lod_threshold_px": pool[p].lod_threshold_px} for p in r.views] for r in reqs]
     units = [scenes[r.scene].lod0_total * len(r.views) for r in reqs]
@@ -935,7 +961,8 @@ def run_serve(args, rank, world, local_rank):
                              "batch's completion event; value = served (view, LOD0 meshlet) pairs / (last "
                              "completion - first arrival)",
                    "l2": "not flushed: the request stream itself exceeds L2 (scenes of up to 2M instances)",
-                   "parallelism": f"replica x{world}" if world > 1 else "single GPU"},
+                   "parallelism": (f"requests assigned by estimated cost over {world} GPUs (scenes replicated)"
+                                   if world > 1 else "single GPU")},
         "latency_ms": {"p50": pct(lat, 0.5), "p99": pct(lat, 0.99), "mean": statistics.mean(lat)},
         "capacity_requests_per_s": capacity_rps, "low_load": low_load,
         "plain_per_request": plain, "cpu_baseline": cpu, "e2e": None, "roofline": None,

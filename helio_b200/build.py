@@ -25,7 +25,7 @@ CUDA_HOME = Path(os.environ.get("CUDA_HOME", "/usr/local/cuda"))
 NVCC = str(CUDA_HOME / "bin" / "nvcc")
 
 CUDA_SOURCES = ["capi.cu", "hiz.cu", "instance_cull.cu", "vg_cull.cu", "noalloc.cu", "batch.cu", "batch_api.cu", "serve.cu", "vg_build.cu", "shadow_cull.cu"]
-HEADERS = ["common.cuh", "kernels.h", "vg.h", "instance_cull.h", "hiz_tile.cuh", "vg_device.cuh", "host_util.h", "batch.h",
+HEADERS = ["common.cuh", "tma.cuh", "kernels.h", "vg.h", "instance_cull.h", "hiz_tile.cuh", "vg_device.cuh", "host_util.h", "batch.h",
            "shadow_device.cuh", "shadow_host.h"]
 
 # IEEE binary32 without contraction, correctly rounded division / square root,

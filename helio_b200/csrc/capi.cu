@@ -149,8 +149,10 @@ int32_t check_pyramid(const helio_hiz_pyramid* hiz) {
 struct helio_hiz_pass {
     uint32_t width = 0, height = 0, flags = 0;
     DevBuf levels;
-    DevBuf ticket;
+    DevBuf ticket;  // [0] last-tile ticket, [1] device error word (kDevTimeout, sticky)
     helio::HizJob job{};
+    alignas(64) CUtensorMap depth_map{};  // level 0 in 64x64 boxes, when use_tma
+    bool use_tma = false;
     const float* depth = nullptr;
     uint32_t depth_pitch = 0;
     uint64_t camera_generation = 0, prev_generation = 0;
@@ -342,6 +344,9 @@ int32_t helio_hiz_prepare(helio_hiz_pass* p, const float* depth_dev, uint32_t de
     size_t floats = helio::hiz_layout(p->width, p->height, pitch, copy, &p->job);
     HELIO_CK(p->levels.ensure(floats * sizeof(float)));
     helio::hiz_assign(&p->job, depth_dev, p->levels.as<float>());
+    p->use_tma = (p->flags & HELIO_HIZ_NO_TMA) == 0u &&
+                 helio::encode_float_tile_map(&p->depth_map, depth_dev, p->width, p->height, pitch, helio::kHizTile,
+                                              helio::kHizTile);
     p->depth = depth_dev;
     p->depth_pitch = pitch;
     p->camera_generation = camera_generation;
@@ -357,8 +362,21 @@ int32_t helio_hiz_execute(helio_hiz_pass* p, void* stream) {
         return HELIO_OK;
     p->first_frame = false;
     p->prev_generation = p->camera_generation;
-    helio::launch_hiz_build_single(p->job, p->ticket.as<uint32_t>(), as_stream(stream));
+    if (p->use_tma)
+        helio::launch_hiz_build_tma(p->depth_map, p->job, p->ticket.as<uint32_t>(), p->ticket.as<uint32_t>() + 1,
+                                    as_stream(stream));
+    else
+        helio::launch_hiz_build_single(p->job, p->ticket.as<uint32_t>(), as_stream(stream));
     HELIO_CK(cudaGetLastError());
+    return HELIO_OK;
+}
+
+int32_t helio_hiz_device_status(const helio_hiz_pass* p, void* stream) {
+    HELIO_ARG(p, "null pointer");
+    uint32_t err = 0;
+    HELIO_CK(cudaMemcpyAsync(&err, p->ticket.as<uint32_t>() + 1, 4, cudaMemcpyDeviceToHost, as_stream(stream)));
+    HELIO_CK(cudaStreamSynchronize(as_stream(stream)));
+    if (err & helio::kDevTimeout) return fail(HELIO_ERR_TIMEOUT, "a Hi-Z tile load never completed (bounded wait)");
     return HELIO_OK;
 }
 

@@ -236,6 +236,27 @@ __device__ __forceinline__ void hiz_tile_levels456(const HizJob& J, uint32_t til
     }
 }
 
+// Warp 0, after its tile's level 6 is written: level 6 is written by warp 0 only, so
+// warp 0 alone takes the job's ticket; the warp of the last tile of the job (over all
+// CTAs) builds levels 7.. from level 6 and leaves the ticket at zero.
+__device__ __forceinline__ void hiz_ticket_tail(const HizJob& J, uint32_t job, uint32_t* tickets) {
+    const int lane = threadIdx.x & 31;
+    __threadfence();
+    __syncwarp();
+    uint32_t last = 0u;
+    if (lane == 0) {
+        const uint32_t tiles = J.tiles_x * J.tiles_y;
+        const uint32_t t = atomicAdd(&tickets[job], 1u);
+        last = (t + 1 == tiles) ? 1u : 0u;
+        if (last) tickets[job] = 0u;  // every other tile of this job has already taken its ticket
+    }
+    last = __shfl_sync(0xffffffffu, last, 0);
+    if (last) {
+        __threadfence();
+        hiz_tail_warp(J);
+    }
+}
+
 // Tile `tile` (flat index within job J, whose ticket is tickets[job]) by all 256
 // threads of the CTA. s_m3 is an 8x9 shared scratch. Warps 1..7 return right
 // after the level-3 barrier; warp 0 finishes levels 4..6 and, if this CTA is the
@@ -253,24 +274,7 @@ __device__ __forceinline__ void hiz_tile(const HizJob& J, uint32_t job, uint32_t
     if ((threadIdx.x >> 5) != 0) return;  // levels 4.. and the tail need only warp 0
     hiz_tile_levels456(J, tile, s_m3);
     if (J.mip_count <= 7 || tickets == nullptr) return;
-
-    // Tail: level 6 is written by warp 0 only, so warp 0 alone takes the ticket;
-    // the warp of the last CTA of this job builds levels 7.. from level 6.
-    const int lane = threadIdx.x & 31;
-    __threadfence();
-    __syncwarp();
-    uint32_t last = 0u;
-    if (lane == 0) {
-        const uint32_t tiles = J.tiles_x * J.tiles_y;
-        const uint32_t t = atomicAdd(&tickets[job], 1u);
-        last = (t + 1 == tiles) ? 1u : 0u;
-        if (last) tickets[job] = 0u;  // every other CTA of this job has already taken its ticket
-    }
-    last = __shfl_sync(0xffffffffu, last, 0);
-    if (last) {
-        __threadfence();
-        hiz_tail_warp(J);
-    }
+    hiz_ticket_tail(J, job, tickets);
 }
 
 }  // namespace helio

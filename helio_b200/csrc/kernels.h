@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cstdint>
+#include <cuda.h>  // CUtensorMap
 #include <cuda_runtime.h>
 
 #include "../../include/helio_cull.h"
@@ -40,5 +41,16 @@ void launch_hiz_build(const HizJob* jobs_dev, uint32_t n_jobs, uint32_t total_ti
                       uint32_t* tickets_dev, cudaStream_t stream);
 // One view, job passed by value (tile_begin must be 0).
 void launch_hiz_build_single(const HizJob& job, uint32_t* ticket_dev, cudaStream_t stream);
+
+// Tensor map of a 2-D float array (width x height, row pitch in floats) read in boxes of
+// box_w x box_h; false when TMA cannot address it (base not 16-byte aligned, pitch not a
+// multiple of 4 floats) or the driver offers no encoder.
+bool encode_float_tile_map(CUtensorMap* map, const float* base, uint32_t width, uint32_t height, uint32_t pitch,
+                           uint32_t box_w, uint32_t box_h);
+// One view whose level 0 is addressed by `src` (encode_float_tile_map of job.depth,
+// 64x64 boxes): a persistent grid with TMA tile loads. error_dev[0] gets kDevTimeout if
+// a tile never lands (bounded wait).
+void launch_hiz_build_tma(const CUtensorMap& src, const HizJob& job, uint32_t* ticket_dev, uint32_t* error_dev,
+                          cudaStream_t stream);
 
 }  // namespace helio

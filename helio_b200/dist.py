@@ -2,7 +2,8 @@
 
 Views (and serving requests) are independent units, so the path shards without any
 collective on the data path: each rank owns a subset of the views (balanced by
-estimated cost) of a scene that every rank holds resident. The only collectives are
+estimated cost, shard_views) of a scene that every rank holds resident, and culls
+them in one batch of its own. The only collectives are
 timing and result bookkeeping on the host side (max over ranks of a step time,
 gathers of per-rank counts), which run on whatever backend the process group has
 (NCCL on GPUs, gloo in the CPU tests).
@@ -46,9 +47,39 @@ def shard_by_cost(costs: list[float], world: int) -> list[list[int]]:
     return [sorted(x) for x in out]
 
 
+def assign_online(costs: list[float], world: int) -> list[int]:
+    """Owner rank of each unit of a stream, in arrival order: the rank with the least
+    cost assigned so far (ties to the lower rank). Units are not reordered, so a
+    rank's units keep their arrival order; every rank computes the same owners."""
+    loads = [0.0] * world
+    owner = []
+    for c in costs:
+        r = min(range(world), key=lambda k: (loads[k], k))
+        owner.append(r)
+        loads[r] += c
+    return owner
+
+
 def view_cost(width: int, height: int, lod0_meshlets: int) -> float:
     """Cost estimate of one view: Hi-Z bytes plus the scene's object / meshlet test work."""
     return 8.0 * width * height + 4.0 * lod0_meshlets
+
+
+def shard_views(views: list, lod0_meshlets: int, world: int, rank: int) -> list[int]:
+    """Indices of the views that `rank` culls: the cost-balanced share (shard_by_cost
+    over view_cost) of a view set whose scene every rank holds resident. Every rank
+    computes the same partition, so no exchange is needed."""
+    costs = [view_cost(v.width, v.height, lod0_meshlets) for v in views]
+    return shard_by_cost(costs, world)[rank]
+
+
+def gather_objects(obj, device=None) -> list:
+    """Every rank's `obj`, in rank order (a list of one element for one rank)."""
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return [obj]
+    parts: list = [None] * dist.get_world_size()
+    dist.all_gather_object(parts, obj)
+    return parts
 
 
 def max_over_ranks(value: float, device=None) -> float:

@@ -30,6 +30,7 @@ HELIO_MEM_DEVICE = 1
 HELIO_VG_CLEAR_INDIRECT = 1
 HELIO_HIZ_MAX_MIPS = 12
 HELIO_HIZ_ALIAS_MIP0 = 1
+HELIO_HIZ_NO_TMA = 2
 HELIO_VG_COUNTER_COUNT = 11
 HELIO_VG_DEFAULT_PUBLICATION_LIMIT = 262144
 HELIO_LOD_LOW, HELIO_LOD_MEDIUM, HELIO_LOD_HIGH, HELIO_LOD_ULTRA = 0, 1, 2, 3
@@ -254,6 +255,7 @@ CULL_EXPORTS = {
     "helio_hiz_execute": (i32, [vp, vp]),
     "helio_hiz_resize": (i32, [vp, u32, u32]),
     "helio_hiz_publish": (i32, [vp, C.POINTER(HizPyramid)]),
+    "helio_hiz_device_status": (i32, [vp, vp]),
     "helio_hiz_destroy": (None, [vp]),
     "helio_hiz_build_noalloc": (i32, [u32, C.POINTER(HizViewInput), vp, C.c_size_t, C.POINTER(HizPyramid), vp]),
     "helio_indirect_dispatch_create": (i32, [vp, C.POINTER(vp)]),

@@ -105,9 +105,10 @@ def camera_bytes(cam: N.GpuCameraUniforms) -> np.ndarray:
 class HiZBuildPass:
     """Hi-Z pyramid (max reduction, standard Z) built by one fused launch."""
 
-    def __init__(self, width: int, height: int, alias_mip0: bool = False):
+    def __init__(self, width: int, height: int, alias_mip0: bool = False, tma: bool = True):
         self._lib = N.cull_lib()
-        cfg = N.HizConfig(width, height, N.HELIO_HIZ_ALIAS_MIP0 if alias_mip0 else 0)
+        flags = (N.HELIO_HIZ_ALIAS_MIP0 if alias_mip0 else 0) | (0 if tma else N.HELIO_HIZ_NO_TMA)
+        cfg = N.HizConfig(width, height, flags)
         h = C.c_void_p()
         N.check(self._lib.helio_hiz_create(C.byref(cfg), C.byref(h)))
         self._h = h
@@ -125,6 +126,10 @@ class HiZBuildPass:
 
     def execute(self, stream=None) -> None:
         N.check(self._lib.helio_hiz_execute(self._h, _stream_ptr(stream)))
+
+    def device_status(self, stream=None) -> None:
+        """Raises if a bounded device wait of an earlier execute gave up (synchronises)."""
+        N.check(self._lib.helio_hiz_device_status(self._h, _stream_ptr(stream)))
 
     def on_resize(self, width: int, height: int) -> None:
         N.check(self._lib.helio_hiz_resize(self._h, width, height))

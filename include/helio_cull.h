@@ -215,6 +215,10 @@ int32_t helio_instance_cull_data(const HelioGpuInstanceData* instances_dev, uint
 /* Level 0 is the caller's depth buffer itself instead of a copy (saves 8 B/px).
  * Only valid while the depth buffer is not overwritten before the pyramid is read. */
 #define HELIO_HIZ_ALIAS_MIP0 1u
+/* Read level 0 with 128-bit loads instead of TMA tile loads (the same results; for
+ * comparing the two). Depth that TMA cannot address (not 16-byte aligned, or a row
+ * pitch that is not a multiple of 4 floats) always takes the 128-bit-load path. */
+#define HELIO_HIZ_NO_TMA 2u
 
 typedef struct helio_hiz_config {
     uint32_t width;
@@ -241,6 +245,10 @@ int32_t helio_hiz_create(const helio_hiz_config* config, helio_hiz_pass** out);
 int32_t helio_hiz_prepare(helio_hiz_pass* pass, const float* depth_dev, uint32_t depth_pitch,
                           uint64_t camera_generation);
 int32_t helio_hiz_execute(helio_hiz_pass* pass, void* stream);
+/* Synchronises `stream`; HELIO_ERR_TIMEOUT if a TMA tile load of an earlier execute
+ * never completed (its bounded wait gave up; sticky for the pass). The reference's
+ * dispatches have no device-side waits (crates/helio-pass-hiz/src/lib.rs:503-531). */
+int32_t helio_hiz_device_status(const helio_hiz_pass* pass, void* stream);
 int32_t helio_hiz_resize(helio_hiz_pass* pass, uint32_t width, uint32_t height);
 int32_t helio_hiz_publish(const helio_hiz_pass* pass, helio_hiz_pyramid* out);
 void helio_hiz_destroy(helio_hiz_pass* pass);

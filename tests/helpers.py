@@ -24,8 +24,9 @@ def cull_dtype():
     return np.dtype(N.InstanceCullData)
 
 
-def gpu_hiz(depth: np.ndarray, alias: bool = False, pitch: int | None = None):
-    """Builds the pyramid on the GPU; returns (pass, list of numpy levels)."""
+def gpu_hiz(depth: np.ndarray, alias: bool = False, pitch: int | None = None, tma: bool = True):
+    """Builds the pyramid on the GPU; returns (pass, list of numpy levels). tma=False
+    forces the 128-bit-load path (depth TMA cannot address takes it anyway)."""
     import torch
     from helio_b200.passes import HiZBuildPass
 
@@ -36,10 +37,11 @@ def gpu_hiz(depth: np.ndarray, alias: bool = False, pitch: int | None = None):
         d = buf[:, :w]
     else:
         d = torch.from_numpy(np.ascontiguousarray(depth)).cuda()
-    hz = HiZBuildPass(w, h, alias_mip0=alias)
+    hz = HiZBuildPass(w, h, alias_mip0=alias, tma=tma)
     hz.prepare(d)
     hz.execute()
     torch.cuda.synchronize()
+    hz.device_status()
     pyr = hz.publish()
     levels = [hz.level(l).cpu().numpy().copy() for l in range(pyr.mip_count)]
     hz._keep = d

@@ -39,6 +39,39 @@ def test_hiz_alias_and_pitch(cuda, w, h):
     assert len(ref) == min(O.mip_levels(w, h), 12)
 
 
+@pytest.mark.parametrize("w,h", [(64, 64), (1000, 999), (1920, 1080), (3840, 2160), (256, 4096), (8192, 8)])
+def test_hiz_tma_and_plain_loads_agree(cuda, w, h):
+    """The TMA tile-load path (persistent grid, several tiles in flight per CTA) and the
+    128-bit-load path give the oracle's pyramid, with and without the level-0 copy."""
+    rng = np.random.default_rng(w * 31 + h)
+    depth = rng.random((h, w), dtype=np.float32)
+    ref = O.hiz_build(depth)
+    for alias in (False, True):
+        for tma in (True, False):
+            hz, g = gpu_hiz(depth, alias=alias, tma=tma)
+            _levels_equal(g, ref)
+
+
+def test_hiz_tma_repeated_launches_and_pitch(cuda):
+    """Many TMA launches over a depth with a longer (16-byte multiple) row pitch: the
+    ticket resets itself and rows past the width are never read into the pyramid."""
+    import torch
+    from helio_b200.passes import HiZBuildPass
+
+    rng = np.random.default_rng(4)
+    depth = rng.random((517, 1030), dtype=np.float32)
+    buf = torch.full((517, 1036), 5.0, dtype=torch.float32, device="cuda")
+    buf[:, :1030] = torch.from_numpy(depth).cuda()
+    hz = HiZBuildPass(1030, 517)
+    hz.prepare(buf[:, :1030])
+    for _ in range(20):
+        hz.execute()
+    torch.cuda.synchronize()
+    hz.device_status()
+    got = [hz.level(l).cpu().numpy() for l in range(hz.publish().mip_count)]
+    _levels_equal(got, O.hiz_build(depth))
+
+
 def test_hiz_workload_depth(cuda):
     from helio_b200 import scene as S
 
