@@ -21,6 +21,8 @@ Workloads
                       40 GB HBM budget and batched continuously (helio_serve); reports
                       p50/p99 latency beside meshlets/s, and the same stream served one
                       request at a time through the plain single-view passes.
+  instances           the instance-level passes (IndirectDispatchPass + OcclusionCullPass,
+                      fused launch) over 2M draws against the 3840x2160 view; draws/s.
   shadow              the per-face shadow cull: 100,000 movable draws against 44 dirty
                       shadow faces (4 cascades, 16 spot lights, 4 point lights x 6 faces);
                       draw-face tests per second.
@@ -66,7 +68,7 @@ def parse_args():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
-    ap.add_argument("--workload", default="batched3", choices=["batched3", "plain2", "plain1", "plain0", "serve4", "vgbuild", "shadow"])
+    ap.add_argument("--workload", default="batched3", choices=["batched3", "plain2", "plain1", "plain0", "instances", "serve4", "vgbuild", "shadow"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-parity", action="store_true", help="skip the oracle check of the outputs after timing")
@@ -265,7 +267,8 @@ class PlainWorkload:
         cnt = np.where(sp1 > 0, obj["lod_meshlet_counts"][np.arange(len(obj)), np.maximum(sp1 - 1, 0)], 0)
         n = np.clip(cnt[items["object_index"].astype(np.int64)] - items["local_meshlet_base"].astype(np.int64), 0, 64)
         tested, active = int(n.sum()), int((n > 0).sum())
-        return {"hiz_build": hiz_bytes(v.width, v.height, True), "vg_select": 164 * len(obj),
+        hz = hiz_bytes(v.width, v.height, True)  # the TMA form or the 128-bit-load form, whichever ran
+        return {"hiz_build_tma": hz, "hiz_build": hz, "vg_select": 164 * len(obj),
                 "vg_cull_test": 24 * len(items) + 80 * active + 44 * tested, "vg_cull_emit": 48 * visible}, visible
 
     def e2e(self):
@@ -458,16 +461,20 @@ class BatchedWorkload:
         (176 B per object: 96 B object fields, 64 B model, 16 B InstanceCullData), 44 B
         per meshlet of the union over views of each object's selected LOD range, 32 B per
         active span (16 B written, 16 B read) plus 8 B of span visibility, and 48 B per
-        visible draw (12 B read, 36 B written)."""
+        visible draw (12 B read, 36 B written). Split by launch: batch_kernel (phases 0-3:
+        Hi-Z, LOD bytes, objects, span records written), batch_cull_kernel (phases 4-6:
+        meshlets, span records read, visibility, draws)."""
         lods, visible = self.outputs()
         spans = sum(active_spans(self.scene, lods[v])[0] for v in range(len(self.views)))
-        b = sum(hiz_bytes(v.width, v.height, False) for v in self.views)
-        b += lods.size  # LOD bytes
-        b += 176 * len(self.scene.objects)
-        b += 44 * union_meshlets(self.scene, lods)
-        b += 40 * spans
-        b += 48 * visible
-        return {"batch_cull": b}, visible
+        k1 = sum(hiz_bytes(v.width, v.height, False) for v in self.views)
+        k1 += lods.size  # LOD bytes
+        k1 += 176 * len(self.scene.objects)
+        k1 += 16 * spans  # span records written by the expansion
+        k2 = 44 * union_meshlets(self.scene, lods) + 24 * spans + 48 * visible
+        return {"batch_kernel": k1, "batch_cull_kernel": k2}, visible
+
+    # The two cooperative launches of one step, reported together as the step's roofline.
+    step_kernels = ("batch_kernel", "batch_cull_kernel")
 
     def e2e(self):
         """The step through the C-ABI with host buffers: all depths in (one pinned
@@ -604,7 +611,136 @@ class BatchedWorkload:
         return t0.elapsed_time(t1), int(host_in.numel()) * 4, d2h // steps
 
 
+
+class InstanceWorkload:
+    """The instance-level passes (IndirectDispatchPass frustum + sub-pixel test, then
+    OcclusionCullPass's 4-tap Hi-Z test against the previous frame's pyramid) in their
+    fused launch over 2M draws, one per instance, of a scene with configuration 2's
+    distributions (64 Gaussian blobs in a 2 km cube), seen by configuration 2's
+    3840x2160 view."""
+
+    sharded = False
+    metric, unit = "instance draws culled/s", "draws/s"
+    DRAWS = 2_000_000
+
+    def __init__(self, dev):
+        import torch
+        from helio_b200 import passes as P
+        from helio_b200 import scene as S
+
+        self.name = "instances"
+        sc = S.make_scene(S.SEED_BASE + 6, self.DRAWS, 1, 1, 1, 1000.0, 64, 20.0, lod_error_mode=1)
+        self.view = S.config(2, scale=1.0).views[0]
+        self.inst, self.aabbs, self.draws = sc.instances, sc.aabbs, sc.draw_calls
+        self.views = [self.view]
+        self.units = len(self.draws)
+        up = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.uint8)).to(dev)
+        self.cam = up(P.camera_bytes(self.view.camera))
+        self.t_inst, self.t_aabb, self.t_draw = up(self.inst), up(self.aabbs), up(self.draws)
+        self.indirect = torch.zeros(len(self.draws) * 5, dtype=torch.int32, device=dev)
+        self.stats = torch.zeros(8, dtype=torch.int32, device=dev)
+        self.sb = P.scene_buffers(self.cam, self.t_inst, self.t_draw, self.t_aabb, self.indirect)
+        self.sb.instance_count = len(self.inst)
+        self.sb.draw_count = len(self.draws)
+        self.depth = torch.from_numpy(self.view.depth).to(dev)
+        self.hz = P.HiZBuildPass(self.view.width, self.view.height)
+        self.hz.prepare(self.depth)
+        self.hz.execute()
+        self.fr = P.IndirectDispatchPass(self.stats)
+        self.oc = P.OcclusionCullPass(self.view.width, self.view.height, self.stats)
+        self.fr.prepare(self.view.camera, len(self.draws))
+        self.oc.prepare(len(self.draws))
+        torch.cuda.synchronize()
+
+    def step(self):
+        from helio_b200 import passes as P
+
+        self.stats.zero_()
+        P.fused_instance_cull(self.fr, self.oc, self.sb, self.hz.publish(), 1)
+
+    def describe(self):
+        return (f"instances: IndirectDispatchPass + OcclusionCullPass (fused launch) over {len(self.draws)} draws "
+                f"of a 2 km scene in 64 blobs, 3840x2160 view, previous frame's Hi-Z resident")
+
+    def kernel_bytes(self) -> tuple[dict, int]:
+        """Per draw: the 20-byte draw call, the instance's bounds and flags (20 B), the
+        32-byte AABB read and the 20-byte indirect record written; the Hi-Z taps are
+        L2-resident and not counted."""
+        visible = int(_u32(self.stats)[3]) - int(_u32(self.stats)[4])
+        return {"instance_cull_fused": 92 * len(self.draws)}, visible
+
+    def e2e(self):
+        """Per frame through the C-ABI: the camera and the frame's depth copied in, the
+        Hi-Z build, the fused cull, the indirect records and statistics copied out."""
+        import torch
+        from helio_b200 import passes as P
+
+        host_depth = torch.from_numpy(self.view.depth).pin_memory()
+        host_cam = torch.from_numpy(P.camera_bytes(self.view.camera)).pin_memory()
+        host_ind = torch.empty_like(self.indirect, device="cpu").pin_memory()
+        host_st = torch.empty(8, dtype=torch.int32).pin_memory()
+        h2d = int(host_depth.numel()) * 4 + int(host_cam.numel())
+        stats = {"d2h": 0}
+
+        def run():
+            self.depth.copy_(host_depth, non_blocking=True)
+            self.cam.copy_(host_cam, non_blocking=True)
+            self.hz.execute()
+            self.step()
+            host_ind.copy_(self.indirect, non_blocking=True)
+            host_st.copy_(self.stats, non_blocking=True)
+            torch.cuda.current_stream().synchronize()
+            stats["d2h"] += int(self.indirect.numel()) * 4 + 32
+
+        return run, h2d, stats
+
+    def parity(self, threads: int) -> dict:
+        """Checker leg: the indirect records and statistics against the oracle's two
+        passes (the fused launch must equal frustum then occlusion)."""
+        from oracle import oracle as O
+
+        t0 = time.perf_counter()
+        levels = O.hiz_build(self.view.depth)
+        ind, st = O.indirect_dispatch(self.view.camera, self.inst, self.draws, self.aabbs)
+        ost = O.occlusion_cull(self.view.camera, self.view.width, self.view.height, levels, self.inst, self.draws,
+                               ind, st)
+        g_ind = _u32(self.indirect).reshape(-1, 5)
+        g_st = _u32(self.stats)
+        bad = {}
+        if not np.array_equal(g_ind, ind):
+            bad["indirect"] = int((g_ind != ind).any(axis=1).sum())
+        if not np.array_equal(g_st, st):
+            bad["stats"] = 1
+        return {"views": 1, "mismatches": 1 if bad else 0, "mismatched_fields": bad,
+                "marginal_decisions": int(ost.marginal_decisions), "marginal_meshlets": 0, "marginal_objects": 0,
+                "meshlet_tests": 0, "visible_meshlets": int(st[3]) - int(st[4]), "band": "1e-6 relative",
+                "checker": "the oracle (CPU restatement of the reference shaders), bit-exact",
+                "seconds": round(time.perf_counter() - t0, 2)}
+
+    def cpu_baseline(self, seconds: float) -> dict:
+        """The oracle's restatement of both passes, one host thread (as the shaders'
+        per-draw work), on the whole draw list."""
+        from oracle import oracle as O
+
+        levels = O.hiz_build(self.view.depth)
+        t0 = time.perf_counter()
+        n = 0
+        while True:
+            ind, st = O.indirect_dispatch(self.view.camera, self.inst, self.draws, self.aabbs)
+            O.occlusion_cull(self.view.camera, self.view.width, self.view.height, levels, self.inst, self.draws,
+                             ind, st)
+            n += 1
+            if time.perf_counter() - t0 >= seconds or n >= 20:
+                break
+        dt = time.perf_counter() - t0
+        return {"value": n * len(self.draws) / dt, "unit": "draws/s", "cores": 1, "kind": "port",
+                "sample": f"{n} pass(es) of both passes over all {len(self.draws)} draws, one thread, {dt:.1f} s",
+                "seconds": dt}
+
+
 def build_workload(name, dev, with_plain, rank=0, world=1):
+    if name == "instances":
+        return InstanceWorkload(dev)
     return BatchedWorkload(dev, with_plain, rank, world) if name == "batched3" else PlainWorkload(name, dev)
 
 
@@ -680,6 +816,7 @@ def run_ours(args, rank, world, local_rank):
     # Units of the whole job per step: the 85 views once when they are split across
     # GPUs (strong scaling), every rank's replica otherwise (weak scaling).
     job_units = D.sum_over_ranks(wl.units, dev) if world > 1 else wl.units
+    metric, unit = getattr(wl, "metric", "meshlets culled/s"), getattr(wl, "unit", "meshlets/s")
     timer = Timer(dev)
 
     wl.step()
@@ -719,6 +856,15 @@ def run_ours(args, rank, world, local_rank):
             entry["achieved_gbs"] = kb[name] / (ms / max(n, 1) / 1e3) / 1e9
         kernels[name] = entry
     dom = max((k for k in kernels if "achieved_gbs" in kernels[k]), key=lambda k: kernels[k]["share"])
+    step_kernels = [k for k in getattr(wl, "step_kernels", ()) if k in kernels and k in kb]
+    if step_kernels:
+        # A step of several launches: its bytes over the sum of their average durations.
+        us = sum(kernels[k]["avg_us"] for k in step_kernels)
+        dom = " + ".join(step_kernels)
+        kernels[dom] = {"launches": min(kernels[k]["launches"] for k in step_kernels), "avg_us": us,
+                        "share": sum(kernels[k]["share"] for k in step_kernels),
+                        "algorithmic_bytes_per_launch": float(sum(kb[k] for k in step_kernels)),
+                        "achieved_gbs": sum(kb[k] for k in step_kernels) / (us / 1e6) / 1e9}
     peak, peak_kind = peaks()
     traffic = None
     tfile = ROOT / "profiles" / "dram_traffic.json"
@@ -756,7 +902,7 @@ def run_ours(args, rank, world, local_rank):
             ee[k][1].record()
         torch.cuda.synchronize()
         e2e_ms = D.max_over_ranks(float(sum(a.elapsed_time(b) for a, b in ee)), dev)
-        e2e = {"value": job_units * args.steps / (e2e_ms / 1e3), "unit": "meshlets/s",
+        e2e = {"value": job_units * args.steps / (e2e_ms / 1e3), "unit": unit,
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": int(stats["d2h"] / args.steps),
                "ms_per_step": e2e_ms / args.steps, "form": "one frame at a time (copy in, cull, copy out)"}
         if hasattr(wl, "e2e_pipelined"):
@@ -769,19 +915,21 @@ def run_ours(args, rank, world, local_rank):
                            "culled and its draws copied out (inputs of 121 MB per frame exceed L2)",
                    "sequential": sequential}
 
-    cpu = cpu_baseline(wl.wl, args.cpu_seconds) if (rank == 0 and world == 1) else None
+    cpu = None
+    if rank == 0 and world == 1:
+        cpu = wl.cpu_baseline(args.cpu_seconds) if hasattr(wl, "cpu_baseline") else cpu_baseline(wl.wl, args.cpu_seconds)
     parity = None
     if not args.no_parity:
         # The checker, after everything timed: this rank's views against the oracle.
         torch.cuda.synchronize()
         parity = D.sum_parity(wl.parity(max(1, os.cpu_count() or 1)), dev)
     line = {
-        "metric": "meshlets culled/s", "value": value, "unit": "meshlets/s", "n_gpus": world,
+        "metric": metric, "value": value, "unit": unit, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
         "scaling": "strong" if wl.sharded else "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded generator)",
         "config": {"workload": wl.describe(), "views": len(getattr(wl, "all_views", wl.views)),
-                   "lod0_meshlets_per_view": wl.scene.lod0_total,
+                   "lod0_meshlets_per_view": wl.scene.lod0_total if hasattr(wl, "scene") else None,
                    "l2": "flushed between timed steps (256 MB write, then 256 MB read)",
                    "timing": ("CUDA-graph replay of the whole step" if graphed else "eager launches") +
                              ", CUDA events on the launching stream",
@@ -1324,6 +1472,32 @@ def run_reference(args):
                                  "sample": "each step: one rebuild of the full library by the oracle's restatement "
                                            "of rebuild_vg_buffers (single thread, as the reference)"},
                 "e2e": {"value": v, "unit": "slots/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if args.workload == "instances":
+        from oracle import oracle as O
+
+        sc = S.make_scene(S.SEED_BASE + 6, InstanceWorkload.DRAWS, 1, 1, 1, 1000.0, 64, 20.0, lod_error_mode=1)
+        view = S.config(2).views[0]
+        levels = O.hiz_build(view.depth)
+
+        def one():
+            ind, st = O.indirect_dispatch(view.camera, sc.instances, sc.draw_calls, sc.aabbs)
+            O.occlusion_cull(view.camera, view.width, view.height, levels, sc.instances, sc.draw_calls, ind, st)
+
+        for _ in range(args.warmup):
+            one()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            one()
+        t = time.perf_counter() - t0
+        v = args.steps * len(sc.draw_calls) / t
+        return {"metric": "instance draws culled/s", "value": v, "unit": "draws/s", "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded generator)", "impl": "reference", "config": {"workload": "instances"},
+                "cpu_baseline": {"value": v, "unit": "draws/s", "cores": 1, "kind": "port",
+                                 "sample": "each step: all draws through the oracle's restatement of "
+                                           "indirect_dispatch.wgsl and occlusion_cull.wgsl (single thread)"},
+                "e2e": {"value": v, "unit": "draws/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     if args.workload == "serve4":
         # The reference has no serving loop; its per-view cull, restated, on the smallest
         # serving scene and the 85-view mix.

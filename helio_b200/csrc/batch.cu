@@ -1223,12 +1223,12 @@ cudaError_t launch_coop(const void* fn, uint32_t grid, size_t smem, const BatchP
 cudaError_t launch_batch(const BatchParams& p, uint32_t grid, uint32_t cull_grid, cudaStream_t stream) {
     cudaError_t e = cudaFuncSetAttribute(batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmTotal);
     if (e != cudaSuccess) return e;
-    helio_launch_begin("batch_cull", stream);
+    helio_launch_begin("batch_kernel", stream);
     e = launch_coop(reinterpret_cast<const void*>(batch_kernel), grid, kSmTotal, p, stream);
-    if (e == cudaSuccess) {
-        helio_launch_note();
-        e = launch_coop(reinterpret_cast<const void*>(batch_cull_kernel), cull_grid, kSm2Total, p, stream);
-    }
+    helio_launch_end(stream);
+    if (e != cudaSuccess) return e;
+    helio_launch_begin("batch_cull_kernel", stream);
+    e = launch_coop(reinterpret_cast<const void*>(batch_cull_kernel), cull_grid, kSm2Total, p, stream);
     helio_launch_end(stream);
     return e;
 }

@@ -25,7 +25,7 @@ namespace {
 // `single` is used when jobs == nullptr (one view, job passed by value);
 // otherwise jobs[] holds n_jobs views. The job is copied to shared memory so
 // that its level arrays can be indexed at run time.
-__global__ void __launch_bounds__(256) hiz_build_kernel(HizJob single, const HizJob* __restrict__ jobs,
+__global__ void __launch_bounds__(256, 3) hiz_build_kernel(HizJob single, const HizJob* __restrict__ jobs,
                                                         uint32_t n_jobs, uint32_t* tickets) {
     __shared__ float s_m3[8][9];
     __shared__ HizJob s_J;
@@ -111,9 +111,23 @@ __global__ void __launch_bounds__(256, 3) hiz_build_tma_kernel(const __grid_cons
         hiz_tile_levels123(J, t, v, s_m3);
         if (J.mip_count <= 3) continue;
         __syncthreads();
-        if (warp == 0) {
-            hiz_tile_levels456(J, t, s_m3);
-            if (J.mip_count > 7) hiz_ticket_tail(J, 0u, ticket);
+        if (warp == 0) hiz_tile_levels456(J, t, s_m3);
+    }
+    // Levels 7..: every CTA takes one ticket after its last tile (one fence per CTA,
+    // not per tile: warp 0 wrote all of this CTA's level-6 texels); the CTA that takes
+    // the last ticket builds the tail with all 8 warps.
+    if (J.mip_count > 7) {
+        __shared__ uint32_t s_last;
+        if (tid == 0) {
+            __threadfence();
+            const uint32_t last = (atomicAdd(ticket, 1u) + 1u == G) ? 1u : 0u;
+            if (last) *ticket = 0u;  // every other CTA has taken its ticket
+            s_last = last;
+        }
+        __syncthreads();
+        if (s_last) {
+            __threadfence();
+            hiz_tail<8, 2>(J);
         }
     }
     // A wait that gave up leaves later loads in flight: wait for them (bounded) before

@@ -37,56 +37,67 @@ __device__ __forceinline__ float hiz_red4(float a, float b, float c, float d, bo
 
 constexpr int kHizTailBuf = 2304;  // floats per shared tail buffer
 
-// Levels 7.. of one pyramid, built by one warp (lane = threadIdx.x & 31). A source
-// level that lives only in global memory is read in batches of 8 texels per lane
-// (32 loads in flight); levels that fit are kept in shared memory for the next step.
-static __device__ __noinline__ void hiz_tail_warp(const HizJob& J) {
-    __shared__ float bufA[kHizTailBuf];
-    __shared__ float bufB[kHizTailBuf];
-    const uint32_t lane = threadIdx.x & 31u;
-    float* cur = nullptr;  // shared copy of the current source level (or null)
+// Levels 7.. of one pyramid, built from level 6 by kWarps warps (warp index w =
+// (threadIdx.x >> 5) % kWarps; every thread of those warps calls it). The level loop is
+// unrolled so that J's per-level fields are read at fixed offsets, and each level is
+// walked by rows: warp w takes rows w, w + kWarps, ... in rounds of kRows rows per lane
+// (kRows x 4 loads in flight), lanes take the columns, so no index needs a division.
+// Level 7 reads level 6 from global memory (written by other CTAs, through L2); a level
+// that fits a shared buffer is kept there for the next level.
+template <int kWarps, int kRows>
+__device__ __forceinline__ void hiz_tail_sync() {
+    if (kWarps == 1) __syncwarp();
+    else __syncthreads();
+}
+
+template <int kWarps, int kRows>
+static __device__ __noinline__ void hiz_tail_in(const HizJob& J, float* bufA, float* bufB) {
+    const uint32_t lane = threadIdx.x & 31u, w = (threadIdx.x >> 5) % (uint32_t)kWarps;
+    const uint32_t mips = J.mip_count;
+    float* cur = nullptr;  // shared copy of the current source level (or null: read global)
     float* nxt = bufA;
-    for (uint32_t l = 7; l < J.mip_count; ++l) {
+#pragma unroll
+    for (int l = 7; l < HELIO_HIZ_MAX_MIPS; ++l) {
+        if ((uint32_t)l >= mips) break;
         const uint32_t sw = J.lw[l - 1], sh = J.lh[l - 1], sp = J.lpitch[l - 1];
         const uint32_t dw = J.lw[l], dh = J.lh[l], dp = J.lpitch[l];
         const float* __restrict__ src = J.levels[l - 1];
         float* __restrict__ dst = J.levels[l];
-        const uint32_t n = dw * dh;
-        const bool fits = (size_t)n <= (size_t)kHizTailBuf;
-        for (uint32_t base = lane; base < n; base += 32u * 8u) {
-            float s[8][4];
+        const bool fits = (size_t)dw * dh <= (size_t)kHizTailBuf;
+        for (uint32_t y0 = w; y0 < dh; y0 += (uint32_t)(kWarps * kRows)) {
+            for (uint32_t x = lane; x < dw; x += 32u) {
+                const uint32_t x0 = 2u * x, x1 = min(x0 + 1u, sw - 1u);
+                float q[kRows][4];
 #pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                const uint32_t i = base + 32u * j;
-                if (i < n) {
-                    const uint32_t y = i / dw, x = i - y * dw;
-                    const uint32_t x0 = 2 * x, y0 = 2 * y;
-                    const uint32_t x1 = min(x0 + 1, sw - 1), y1 = min(y0 + 1, sh - 1);
-                    if (cur) {
-                        s[j][0] = cur[y0 * sw + x0];
-                        s[j][1] = cur[y0 * sw + x1];
-                        s[j][2] = cur[y1 * sw + x0];
-                        s[j][3] = cur[y1 * sw + x1];
-                    } else {
-                        s[j][0] = __ldcg(src + (size_t)y0 * sp + x0);
-                        s[j][1] = __ldcg(src + (size_t)y0 * sp + x1);
-                        s[j][2] = __ldcg(src + (size_t)y1 * sp + x0);
-                        s[j][3] = __ldcg(src + (size_t)y1 * sp + x1);
+                for (int r = 0; r < kRows; ++r) {
+                    const uint32_t y = y0 + (uint32_t)(kWarps * r);
+                    if (y < dh) {
+                        const uint32_t ya = 2u * y, yb = min(ya + 1u, sh - 1u);
+                        if (cur) {
+                            q[r][0] = cur[ya * sw + x0];
+                            q[r][1] = cur[ya * sw + x1];
+                            q[r][2] = cur[yb * sw + x0];
+                            q[r][3] = cur[yb * sw + x1];
+                        } else {
+                            q[r][0] = __ldcg(src + (size_t)ya * sp + x0);
+                            q[r][1] = __ldcg(src + (size_t)ya * sp + x1);
+                            q[r][2] = __ldcg(src + (size_t)yb * sp + x0);
+                            q[r][3] = __ldcg(src + (size_t)yb * sp + x1);
+                        }
+                    }
+                }
+#pragma unroll
+                for (int r = 0; r < kRows; ++r) {
+                    const uint32_t y = y0 + (uint32_t)(kWarps * r);
+                    if (y < dh) {
+                        const float v = fmaxf(fmaxf(q[r][0], q[r][1]), fmaxf(q[r][2], q[r][3]));
+                        dst[(size_t)y * dp + x] = v;
+                        if (fits) nxt[y * dw + x] = v;
                     }
                 }
             }
-#pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                const uint32_t i = base + 32u * j;
-                if (i < n) {
-                    const uint32_t y = i / dw, x = i - y * dw;
-                    const float v = fmaxf(fmaxf(s[j][0], s[j][1]), fmaxf(s[j][2], s[j][3]));
-                    dst[(size_t)y * dp + x] = v;
-                    if (fits) nxt[i] = v;
-                }
-            }
         }
-        __syncwarp();
+        hiz_tail_sync<kWarps, kRows>();
         if (fits) {
             cur = nxt;
             nxt = (nxt == bufA) ? bufB : bufA;
@@ -95,6 +106,17 @@ static __device__ __noinline__ void hiz_tail_warp(const HizJob& J) {
         }
     }
 }
+
+// The tail with its two shared buffers declared here (bufA / bufB of kHizTailBuf floats).
+template <int kWarps, int kRows>
+static __device__ __forceinline__ void hiz_tail(const HizJob& J) {
+    __shared__ float bufA[kHizTailBuf];
+    __shared__ float bufB[kHizTailBuf];
+    hiz_tail_in<kWarps, kRows>(J, bufA, bufB);
+}
+
+// The tail by one warp (lane = threadIdx.x & 31).
+static __device__ __forceinline__ void hiz_tail_warp(const HizJob& J) { hiz_tail<1, 3>(J); }
 
 // Level 0 of tile `tile` of job J into v (4x4 per thread; 256 threads cover 64x64);
 // outside the image the block reads 0 (those texels are never used).
