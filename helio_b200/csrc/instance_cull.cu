@@ -5,9 +5,11 @@
 //   crates/helio-pass-indirect-dispatch/shaders/indirect_dispatch.wgsl:79-176
 //   crates/helio-pass-occlusion-cull/shaders/occlusion_cull.wgsl:101-259 (the static
 //     Hi-Z branch, :222-259, when the pass has a baked grid: static_hiz_occludes)
-// One thread per draw call. Statistics are aggregated per warp (ballot + popc)
-// before one atomic per warp and slot; the totals equal the reference's
-// per-thread atomics.
+// One thread per draw call, in a grid-stride loop over the draws. Statistics are
+// aggregated per warp (ballot + popc) and per block before one atomic per block and
+// slot; the totals equal the reference's per-thread atomics.
+
+#include <algorithm>
 
 #include "common.cuh"
 #include "kernels.h"
@@ -69,17 +71,11 @@ __device__ bool static_hiz_occludes(const InstanceCullParams& P, F3 center, F3 c
     return dist > fadd(occ, 0.1f);
 }
 
+// One draw (indirect_dispatch.wgsl:100-176 and / or occlusion_cull.wgsl:146-220):
+// writes its indirect record and returns which statistics it adds to (bit s = slot s).
 template <bool kFrustum, bool kOcclusion>
-__global__ void __launch_bounds__(256) instance_cull_kernel(InstanceCullParams P) {
-    __shared__ HizView s_hiz;
-    if (kOcclusion) {
-        if (threadIdx.x == 0) copy_hiz(P.hiz, s_hiz);
-        __syncthreads();
-    }
-    const uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool active = idx < P.draw_count;
-    const int lane = threadIdx.x & 31;
-
+__device__ __forceinline__ uint32_t cull_draw(const InstanceCullParams& P, const HizView& s_hiz, uint32_t idx,
+                                              bool active) {
     bool c_total = false, c_frustum = false, c_subpixel = false, c_visible = false, c_shadow = false,
          c_shadow_vis = false, c_occ = false, c_shadow_occ = false;
 
@@ -215,23 +211,58 @@ __global__ void __launch_bounds__(256) instance_cull_kernel(InstanceCullParams P
         }
     }
 
-    // Warp-aggregated statistics (same totals as one atomic per thread).
     const bool conds[8] = {c_total, c_frustum, c_subpixel, c_visible, c_occ, c_shadow, c_shadow_vis, c_shadow_occ};
+    uint32_t bits = 0u;
 #pragma unroll
-    for (int s = 0; s < 8; ++s) {
-        const bool used = kFrustum ? (s != 4 && s != 7) : (s == 4 || s == 7);
-        if (!used && !(kFrustum && kOcclusion)) continue;
-        const uint32_t n = __popc(__ballot_sync(0xffffffffu, conds[s]));
-        if (lane == 0 && n) atomicAdd(P.stats + s, n);
+    for (int k = 0; k < 8; ++k) bits |= conds[k] ? (1u << k) : 0u;
+    return bits;
+}
+
+// Grid-stride over the draws, one thread per draw per round. The statistics are summed
+// per warp (ballot + popc) in lane 0's registers, per block in shared memory, and added
+// to the global counters once per block and slot: the totals equal the reference's
+// one atomic per thread, without thousands of atomics on the same 8 words.
+template <bool kFrustum, bool kOcclusion>
+__global__ void __launch_bounds__(256) instance_cull_kernel(InstanceCullParams P) {
+    __shared__ HizView s_hiz;
+    __shared__ uint32_t s_stats[8];
+    if (threadIdx.x < 8) s_stats[threadIdx.x] = 0u;
+    if (kOcclusion && threadIdx.x == 0) copy_hiz(P.hiz, s_hiz);
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    uint32_t acc[8] = {0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u};
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < P.draw_count; base += stride) {
+        const uint32_t idx = base + threadIdx.x;
+        const uint32_t bits = cull_draw<kFrustum, kOcclusion>(P, s_hiz, idx, idx < P.draw_count);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) acc[k] += __popc(__ballot_sync(0xffffffffu, (bits >> k) & 1u));
     }
+    if (lane == 0) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const bool used = kFrustum ? (k != 4 && k != 7) : (k == 4 || k == 7);
+            if ((used || (kFrustum && kOcclusion)) && acc[k]) atomicAdd(&s_stats[k], acc[k]);
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < 8 && s_stats[threadIdx.x]) atomicAdd(P.stats + threadIdx.x, s_stats[threadIdx.x]);
 }
 
 }  // namespace
 
 void launch_instance_cull(const InstanceCullParams& p, bool frustum, bool occlusion, cudaStream_t stream) {
     if (p.draw_count == 0) return;
-    const uint32_t blocks = (p.draw_count + 255u) / 256u;
     if (!frustum && !occlusion) return;
+    // Enough blocks to fill every SM 8 deep; each takes its share of the draws.
+    static int sms = 0;
+    if (sms == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms < 1) sms = 1;
+    }
+    const uint32_t blocks = std::min<uint32_t>((p.draw_count + 255u) / 256u, (uint32_t)sms * 8u);
     helio_launch_begin(frustum && occlusion ? "instance_cull_fused" : frustum ? "indirect_dispatch" : "occlusion_cull",
                        stream);
     if (frustum && occlusion) instance_cull_kernel<true, true><<<blocks, 256, 0, stream>>>(p);

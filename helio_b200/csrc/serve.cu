@@ -42,7 +42,7 @@ struct ServeRequest {
     int slot = -1;
     uint32_t first_view = 0, batch_requests = 0;
     bool complete = false;
-    double device_ms = 0.0;
+    double device_ms = 0.0, device_start = 0.0, device_end = 0.0;
 };
 
 struct Slot {
@@ -67,6 +67,7 @@ struct helio_serve {
     std::vector<helio_serve_completion> completions;
     uint64_t next_id = 1, batches = 0;
     uint32_t grid = 0;
+    cudaEvent_t origin = nullptr;  // device time origin of the completions' device times
 
     uint64_t used() const {
         uint64_t u = scene_bytes;
@@ -81,6 +82,7 @@ struct helio_serve {
             if (s.done) cudaEventDestroy(s.done);
             if (s.stream) cudaStreamDestroy(s.stream);
         }
+        if (origin) cudaEventDestroy(origin);
     }
 };
 
@@ -105,8 +107,10 @@ int32_t retire(helio_serve* sv, double now) {
         const cudaError_t q = cudaEventQuery(s.done);
         if (q == cudaErrorNotReady) continue;
         if (q != cudaSuccess) return helio_fail(HELIO_ERR_CUDA, cudaGetErrorString(q));
-        float ms = 0.0f;
+        float ms = 0.0f, t0 = 0.0f, t1 = 0.0f;
         cudaEventElapsedTime(&ms, s.start, s.done);
+        cudaEventElapsedTime(&t0, sv->origin, s.start);
+        cudaEventElapsedTime(&t1, sv->origin, s.done);
         const int32_t st = helio_batch_status(s.batch, s.stream);
         s.running = false;
         for (uint64_t id : s.requests) {
@@ -125,6 +129,8 @@ int32_t retire(helio_serve* sv, double now) {
             c.launch_s = r.launch;
             c.done_s = now;
             c.batch_device_ms = ms;
+            c.device_start_ms = t0;
+            c.device_end_ms = t1;
             sv->completions.push_back(c);
         }
     }
@@ -207,12 +213,16 @@ int32_t helio_serve_create(const helio_serve_config* cfg, helio_serve** out) {
     }
     sv->grid = cfg->ctas_per_slot ? std::min(cfg->ctas_per_slot, full) : std::max(1u, full / cfg->slots);
     sv->slots.resize(cfg->slots);
+    bool ok = cudaEventCreate(&sv->origin) == cudaSuccess;
     for (Slot& s : sv->slots) {
-        if (cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking) != cudaSuccess ||
-            cudaEventCreate(&s.start) != cudaSuccess || cudaEventCreate(&s.done) != cudaSuccess) {
-            delete sv;
-            return helio_fail(HELIO_ERR_CUDA, "stream or event creation failed");
-        }
+        ok = ok && cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking) == cudaSuccess &&
+             cudaEventCreate(&s.start) == cudaSuccess && cudaEventCreate(&s.done) == cudaSuccess;
+    }
+    // The origin of the device times: recorded before any launch of this server.
+    ok = ok && cudaEventRecord(sv->origin, sv->slots[0].stream) == cudaSuccess;
+    if (!ok) {
+        delete sv;
+        return helio_fail(HELIO_ERR_CUDA, "stream or event creation failed");
     }
     *out = sv;
     return HELIO_OK;

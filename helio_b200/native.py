@@ -210,7 +210,7 @@ class ServeRequest(C.Structure):
 class ServeCompletion(C.Structure):
     _fields_ = [("request", u64), ("tag", u64), ("status", i32), ("batch_requests", u32), ("view_count", u32),
                 ("reserved", u32), ("arrival_s", C.c_double), ("launch_s", C.c_double), ("done_s", C.c_double),
-                ("batch_device_ms", C.c_double)]
+                ("batch_device_ms", C.c_double), ("device_start_ms", C.c_double), ("device_end_ms", C.c_double)]
 
 
 class ServePending(C.Structure):
@@ -228,7 +228,7 @@ HELIO_BATCH_SPAN_VISIBILITY = 1
 _SIZES = {GpuCameraUniforms: 368, GpuInstanceData: 144, GpuInstanceAabb: 32, GpuDrawCall: 20,
           DrawIndexedIndirectArgs: 20, GpuMeshletEntry: 64, GpuVgObject: 128, GpuVgDraw: 16, GpuVgWorkItem: 8,
           InstanceCullData: 16, VgFrameData: 80, BatchConfig: 24, ServeConfig: 32, ServeRequest: 32,
-          ServeCompletion: 64, ServeStats: 40}
+          ServeCompletion: 80, ServeStats: 40}
 for _t, _n in _SIZES.items():
     assert C.sizeof(_t) == _n, (_t.__name__, C.sizeof(_t), _n)
 

@@ -634,6 +634,8 @@ typedef struct helio_serve_completion {
     uint32_t reserved;
     double arrival_s, launch_s, done_s; /* caller's clock: arrival, launch, completion seen by a pump */
     double batch_device_ms;             /* device time of the launch that carried it */
+    double device_start_ms, device_end_ms; /* that launch's start and end on the device clock (ms since the
+                                               server was created): launches of different slots overlap */
 } helio_serve_completion;
 
 typedef struct helio_serve_pending {

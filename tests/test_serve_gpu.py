@@ -124,3 +124,75 @@ def test_budget_gates_admission(cuda):
     small = ServeLoop(slots=1, max_views=16, hbm_budget_bytes=1 << 10)
     with pytest.raises(Exception):
         small.add_scene(vgs[2])
+
+
+def test_arrivals_while_running_match_alone(cuda):
+    """Requests submitted while launches are on the device join at the next pump; every
+    result equals the one the request gets alone."""
+    import time
+
+    from helio_b200.passes import ServeLoop
+
+    scenes, vgs, pool, depths, requests = _world(n_requests=30, seed=21)
+    alone, _, _ = _serve(vgs, scenes, pool, depths, requests, slots=1, max_views=32, max_requests_per_batch=1)
+    loop = ServeLoop(slots=3, max_views=16)
+    ids = [loop.add_scene(vs) for vs in vgs]
+    t0 = time.perf_counter()
+    got, comps, submitted_while_running = {}, [], 0
+
+    def drain():
+        for c in loop.completions():  # read and release as a server would
+            assert c["status"] == 0
+            i = c["tag"]
+            got[i] = _collect(loop, c["request"], len(requests[i][1]), len(scenes[requests[i][0]].objects))
+            loop.release(c["request"])
+            comps.append(c)
+
+    for i, (sid, idx) in enumerate(requests):
+        if loop.stats()["running"] > 0:
+            submitted_while_running += 1
+        loop.submit(ids[sid], _spec(pool, depths, idx), time.perf_counter() - t0, tag=i)
+        loop.pump(time.perf_counter() - t0)
+        drain()
+    while len(comps) < len(requests):
+        loop.pump(time.perf_counter() - t0)
+        drain()
+        assert time.perf_counter() - t0 < 120, "serving loop did not finish"
+    assert submitted_while_running > 0, "no request arrived while a launch was on the device"
+    for i in range(len(requests)):
+        _equal(alone[i], got[i], f"request {i}")
+
+
+def test_launches_of_different_slots_overlap_on_the_device(cuda):
+    """Three requests of 32 views over a 5M-meshlet scene, submitted together, go to three
+    slots in one pump; once the slots' buffers are sized, their launches' device
+    intervals (events on the slots' streams) intersect: the batches run on the device at
+    the same time."""
+    import time
+
+    import torch
+    from helio_b200 import scene as S
+    from helio_b200.passes import ServeLoop, VgScene
+
+    sc = S.make_scene(1100, 50000, 100, 4, 0, 100.0, lod_error_mode=1, mesh_library=64)
+    vs = VgScene()
+    vs.upload(S.frame_data(sc))
+    pool = S.multiview_set(78, depth=True, scale=0.5)
+    depths = [torch.from_numpy(np.ascontiguousarray(v.depth)).cuda() for v in pool]
+    loop = ServeLoop(slots=3, max_views=32, max_requests_per_batch=1)
+    sid = loop.add_scene(vs)
+    for rnd in range(2):  # the first round sizes every slot's buffers (allocation is slow and synchronous)
+        for r in range(3):
+            loop.submit(sid, _spec(pool, depths, list(range(1 + 21 * r, 33 + 21 * r))), 0.0, tag=r)
+        assert loop.pump(0.0) == 0 and loop.stats()["running"] == 3
+        comps, t0 = [], time.perf_counter()
+        while len(comps) < 3:
+            loop.pump(time.perf_counter() - t0)
+            comps.extend(loop.completions())
+            assert time.perf_counter() - t0 < 60
+        for c in comps:
+            loop.release(c["request"])
+    assert all(c["status"] == 0 for c in comps)
+    iv = sorted((c["device_start_ms"], c["device_end_ms"]) for c in comps)
+    assert len(set(iv)) == 3
+    assert any(b[0] < a[1] for a, b in zip(iv, iv[1:])), f"no two launches overlapped on the device: {iv}"
