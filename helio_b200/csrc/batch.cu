@@ -852,78 +852,114 @@ __device__ __forceinline__ uint32_t cnt_of(uint32_t lo, uint32_t hi) {
 }
 
 // ── Phase 6: emission, per view, in the canonical order ───────────────────────
+// The loads of one group that do not depend on another group's data: its scan offset,
+// lane k's span and lane k's two window ballots (windows k and k + 32; the ballot row has
+// kWindowsPerWarp entries, read whole and masked to the group's windows later).
+struct EmitLoads {
+    uint32_t goff, bits_lo, bits_hi;
+    ActiveSpan span;
+};
+
+__device__ __forceinline__ EmitLoads emit_loads(const BatchParams& P, uint32_t g) {
+    const int lane = threadIdx.x & 31;
+    EmitLoads e;
+    e.goff = ld_cg(P.group_offs + g);
+    e.span = __ldcg(P.spans + (size_t)g * 32u + lane);
+    const uint32_t* gbits = P.group_bits + (size_t)g * kWindowsPerWarp;
+    e.bits_lo = ld_cg(gbits + lane);
+    e.bits_hi = ld_cg(gbits + lane + 32);
+    return e;
+}
+
 __device__ void phase_emit(const BatchParams& P, uint32_t groups) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const VgSceneDev& S = P.scene;
     const uint32_t gw = blockIdx.x * (kBatchThreads / 32) + warp, GW = gridDim.x * (kBatchThreads / 32);
     // Groups are dealt out strided (lane k of warp w looks at group w + k * W): the heavy
-    // consecutive groups of a large view spread over many warps.
+    // consecutive groups of a large view spread over many warps. A warp's groups are
+    // software-pipelined: the next group's offset, spans and ballots are loaded before the
+    // current group's draws are written, so that those round trips overlap the writes.
     for (uint32_t k0 = 0; gw + (size_t)k0 * GW < groups; k0 += 32u) {
         const size_t gl = gw + (size_t)(k0 + lane) * GW;
         const uint32_t cnt = gl < groups ? ld_cg(P.group_counts + gl) : 0u;
         uint32_t mask = __ballot_sync(0xffffffffu, cnt != 0u);
-        while (mask) {
-            const uint32_t g = gw + (k0 + (__ffs(mask) - 1)) * GW;
+        if (!mask) continue;
+        uint32_t g = gw + (k0 + (__ffs(mask) - 1)) * GW;
+        mask &= mask - 1u;
+        EmitLoads cur = emit_loads(P, g);
+        for (;;) {
+            const bool more = mask != 0u;
+            const uint32_t g_next = more ? gw + (k0 + (__ffs(mask) - 1)) * GW : 0u;
             mask &= mask - 1u;
-            // Round trip 1: the group's spans and its scan offset.
-            const uint32_t goff = ld_cg(P.group_offs + g);
-            const GroupSpans gs = load_group(P, g);
-            if (gs.view >= P.view_count) continue;
-            // Round trip 2: the view's first group, its table entry and every window's ballot.
-            const BatchViewDev& V = P.views[gs.view];
-            const uint32_t first_group = ld_cg(P.view_span_start + gs.view) >> 5;
-            const uint32_t cap = V.capacity;
-            HelioDrawIndexedIndirectArgs* indirect = V.indirect;
-            HelioGpuVgDraw* draws = V.draws;
-            uint32_t* counters = V.counters;
-            const uint32_t windows = (gs.total + 31u) >> 5;
-            const uint32_t* gbits = P.group_bits + (size_t)g * kWindowsPerWarp;
-            const uint32_t bits_lo = (uint32_t)lane < windows ? ld_cg(gbits + lane) : 0u;
-            const uint32_t bits_hi = (uint32_t)lane + 32u < windows ? ld_cg(gbits + lane + 32) : 0u;
-            const uint32_t count = cnt_of(bits_lo, bits_hi);
-            uint32_t slot0 = goff - ld_cg(P.group_offs + first_group);
-            if (lane == 0) {
-                atomicAdd(counters + 0, count);
-                const unsigned long long end = (unsigned long long)slot0 + count;
-                const unsigned long long lo = slot0 > cap ? slot0 : cap;
-                if (end > lo) atomicAdd(counters + 1, (uint32_t)(end - lo));
-            }
-            // Windows in groups of 4: the draw records of 4 windows are loaded before
-            // any of them is written.
-            for (uint32_t w0 = 0; w0 < windows; w0 += 4) {
-                uint4 d[4];
-                uint32_t b[4], mi[4], ji[4], jl[4];
-#pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    const uint32_t win = w0 + k;
-                    const uint32_t src = win < 32u ? bits_lo : bits_hi;
-                    b[k] = win < windows ? __shfl_sync(0xffffffffu, src, win & 31u) : 0u;
-                    const uint32_t s = win * 32u + lane;
-                    const int j = owner_lane(gs.off, s);
-                    const uint32_t j_off = __shfl_sync(0xffffffffu, gs.off, j);
-                    const uint32_t j_first = __shfl_sync(0xffffffffu, gs.first, j);
-                    ji[k] = __shfl_sync(0xffffffffu, gs.inst, j);
-                    jl[k] = __shfl_sync(0xffffffffu, gs.lod, j);
-                    mi[k] = j_first + (s - j_off);
-                    if ((b[k] >> lane) & 1u) d[k] = __ldg(S.m_draw + mi[k]);
+            EmitLoads nxt{};
+            if (more) nxt = emit_loads(P, g_next);
+            // The current group: its spans' packing offsets, then its view's table entry.
+            GroupSpans gs;
+            gs.n = span_n(cur.span);
+            gs.first = cur.span.x;
+            gs.inst = cur.span.z;
+            gs.lod = span_lod(cur.span);
+            gs.view = __shfl_sync(0xffffffffu, span_view(cur.span), 0);
+            const uint32_t inc = warp_inclusive(gs.n);
+            gs.off = inc - gs.n;
+            gs.total = __shfl_sync(0xffffffffu, inc, 31);
+            if (gs.view < P.view_count) {
+                const BatchViewDev& V = P.views[gs.view];
+                const uint32_t first_group = ld_cg(P.view_span_start + gs.view) >> 5;
+                const uint32_t cap = V.capacity;
+                HelioDrawIndexedIndirectArgs* indirect = V.indirect;
+                HelioGpuVgDraw* draws = V.draws;
+                uint32_t* counters = V.counters;
+                const uint32_t windows = (gs.total + 31u) >> 5;
+                const uint32_t bits_lo = (uint32_t)lane < windows ? cur.bits_lo : 0u;
+                const uint32_t bits_hi = (uint32_t)lane + 32u < windows ? cur.bits_hi : 0u;
+                const uint32_t count = cnt_of(bits_lo, bits_hi);
+                uint32_t slot0 = cur.goff - ld_cg(P.group_offs + first_group);
+                if (lane == 0) {
+                    atomicAdd(counters + 0, count);
+                    const unsigned long long end = (unsigned long long)slot0 + count;
+                    const unsigned long long lo = slot0 > cap ? slot0 : cap;
+                    if (end > lo) atomicAdd(counters + 1, (uint32_t)(end - lo));
                 }
+                // Windows in groups of 4: the draw records of 4 windows are loaded before
+                // any of them is written.
+                for (uint32_t w0 = 0; w0 < windows; w0 += 4) {
+                    uint4 d[4];
+                    uint32_t b[4], mi[4], ji[4], jl[4];
 #pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    if ((b[k] >> lane) & 1u) {
-                        const uint32_t slot = slot0 + __popc(b[k] & ((1u << lane) - 1u));
-                        if (slot < cap) {
-                            uint32_t* out = reinterpret_cast<uint32_t*>(indirect + slot);
-                            out[0] = d[k].y;
-                            out[1] = 1u;
-                            out[2] = d[k].x;
-                            out[3] = d[k].z;
-                            out[4] = slot;
-                            reinterpret_cast<uint4*>(draws)[slot] = make_uint4(ji[k], mi[k], jl[k], 0u);
-                        }
+                    for (int k = 0; k < 4; ++k) {
+                        const uint32_t win = w0 + k;
+                        const uint32_t src = win < 32u ? bits_lo : bits_hi;
+                        b[k] = win < windows ? __shfl_sync(0xffffffffu, src, win & 31u) : 0u;
+                        const uint32_t s = win * 32u + lane;
+                        const int j = owner_lane(gs.off, s);
+                        const uint32_t j_off = __shfl_sync(0xffffffffu, gs.off, j);
+                        const uint32_t j_first = __shfl_sync(0xffffffffu, gs.first, j);
+                        ji[k] = __shfl_sync(0xffffffffu, gs.inst, j);
+                        jl[k] = __shfl_sync(0xffffffffu, gs.lod, j);
+                        mi[k] = j_first + (s - j_off);
+                        if ((b[k] >> lane) & 1u) d[k] = __ldg(S.m_draw + mi[k]);
                     }
-                    slot0 += __popc(b[k]);
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        if ((b[k] >> lane) & 1u) {
+                            const uint32_t slot = slot0 + __popc(b[k] & ((1u << lane) - 1u));
+                            if (slot < cap) {
+                                uint32_t* out = reinterpret_cast<uint32_t*>(indirect + slot);
+                                out[0] = d[k].y;
+                                out[1] = 1u;
+                                out[2] = d[k].x;
+                                out[3] = d[k].z;
+                                out[4] = slot;
+                                reinterpret_cast<uint4*>(draws)[slot] = make_uint4(ji[k], mi[k], jl[k], 0u);
+                            }
+                        }
+                        slot0 += __popc(b[k]);
+                    }
                 }
             }
+            if (!more) break;
+            cur = nxt;
         }
     }
 }
