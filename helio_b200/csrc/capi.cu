@@ -705,9 +705,16 @@ int32_t helio_vg_execute(helio_vg_pass* p, const HelioGpuCameraUniforms* camera_
     vs.screen_height = p->cfg.height;
     vs.hiz_mip_count = mip_levels(p->cfg.width, p->cfg.height);  // unclamped, rendering.rs:828-829
     vs.lod_threshold_px = p->lod_threshold;
-    helio::launch_vg_view_setup(vs, s);
 
     helio::VgSelectParams sp{};
+    // The select blocks build the view constants themselves (block 0 publishes them for
+    // the meshlet kernels); only an empty scene, with no select launch, needs the setup launch.
+    if (p->object_count) {
+        sp.compute_view = 1u;
+        sp.setup = vs;
+    } else {
+        helio::launch_vg_view_setup(vs, s);
+    }
     sp.scene = scene;
     sp.view = view;
     sp.sel = p->sel.as<helio::SelRecord>();

@@ -43,15 +43,6 @@ static_assert(sizeof(CullView) % 16 == 0, "CullView is copied as 16-byte words")
 // x = first meshlet of the LOD, y = meshlets in it, z = instance index, w = LOD + 1 (0 = culled).
 using SelRecord = uint4;
 
-struct VgSelectParams {
-    VgSceneDev scene;
-    const CullView* view;
-    SelRecord* sel;     // [object_count]
-    uint32_t* counters; // [counter_count]
-    uint32_t counter_count;
-    uint32_t write_reserved;  // also store LOD + 1 into objects[i].reserved
-};
-
 // Inputs of vg_view_setup_kernel: computes *out from the device camera.
 struct ViewSetupParams {
     const HelioGpuCameraUniforms* camera;
@@ -60,6 +51,20 @@ struct ViewSetupParams {
     uint32_t screen_height;
     uint32_t hiz_mip_count;
     float lod_threshold_px;
+};
+
+struct VgSelectParams {
+    VgSceneDev scene;
+    const CullView* view;
+    SelRecord* sel;     // [object_count]
+    uint32_t* counters; // [counter_count]
+    uint32_t counter_count;
+    uint32_t write_reserved;  // also store LOD + 1 into objects[i].reserved
+    // compute_view = 1: every block builds the view constants from `setup` itself (the
+    // view-setup launch folded in) and block 0 publishes them to setup.out (== view) for
+    // the later kernels; 0: the blocks read them from `view`.
+    uint32_t compute_view;
+    ViewSetupParams setup;
 };
 
 constexpr uint32_t kCullWarps = 8;                       // warps per CTA tile

@@ -90,13 +90,12 @@ __global__ void instance_cull_data_kernel(const HelioGpuInstanceData* __restrict
 
 // ── View constants (one warp per launch) ──────────────────────────────────────
 
-__global__ void __launch_bounds__(32) vg_view_setup_kernel(ViewSetupParams P) {
-    __shared__ Planes s_planes;
-    publish_planes_warp(P.camera->view_proj, s_planes);
-    if (threadIdx.x == 0) {
+// The view constants of P's camera into v (shared memory), by one warp (every lane of
+// the warp calls it; lanes 0..5 build the planes, lane 0 the rest).
+__device__ __forceinline__ void view_setup_warp(const ViewSetupParams& P, CullView& v) {
+    publish_planes_warp(P.camera->view_proj, v.planes);
+    if ((threadIdx.x & 31) == 0) {
         const HelioGpuCameraUniforms* cam = P.camera;
-        CullView v;
-        v.planes = s_planes;
         v.vp = ldg_mat4(cam->view_proj);
         v.pos_near = __ldg(reinterpret_cast<const float4*>(cam->position_near));
         v.p00 = __ldg(&cam->proj[0]);
@@ -107,16 +106,33 @@ __global__ void __launch_bounds__(32) vg_view_setup_kernel(ViewSetupParams P) {
         v.screen_height = P.screen_height;
         v.hiz_mip_count = P.hiz_mip_count;
         v.pad[0] = v.pad[1] = 0u;
-        *P.out = v;
     }
+    __syncwarp();
+}
+
+__global__ void __launch_bounds__(32) vg_view_setup_kernel(ViewSetupParams P) {
+    __shared__ CullView s_view;
+    view_setup_warp(P, s_view);
+    if (threadIdx.x == 0) *P.out = s_view;
 }
 
 // ── Object select: cs_select_objects (vg_cull.wgsl:282-352) ───────────────────
 
 __global__ void __launch_bounds__(256) vg_select_kernel(VgSelectParams P) {
     __shared__ CullView s_view;
-    load_view(P.view, s_view, threadIdx.x, blockDim.x);
-    __syncthreads();
+    if (P.compute_view) {
+        // The view setup folded in: warp 0 builds the constants; block 0 publishes them.
+        if (threadIdx.x < 32) view_setup_warp(P.setup, s_view);
+        __syncthreads();
+        if (blockIdx.x == 0) {
+            const uint4* src = reinterpret_cast<const uint4*>(&s_view);
+            uint4* dst = reinterpret_cast<uint4*>(P.setup.out);
+            for (uint32_t k = threadIdx.x; k < sizeof(CullView) / 16; k += blockDim.x) dst[k] = src[k];
+        }
+    } else {
+        load_view(P.view, s_view, threadIdx.x, blockDim.x);
+        __syncthreads();
+    }
     const Planes& s_planes = s_view.planes;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31;
