@@ -50,8 +50,8 @@ __global__ void __launch_bounds__(256, 3) hiz_build_kernel(HizJob single, const 
     hiz_tile(s_J, s_job, tile - s_J.tile_begin, tickets, s_m3);
 }
 
-// Persistent form for one view whose level 0 TMA can address: CTA b takes tiles b,
-// b + G, b + 2G, ... Thread 0 keeps kHizStages 64x64 tiles in flight (TMA loads into
+// Persistent form for one view whose level 0 TMA can address (4 CTAs per SM): CTA b takes
+// tiles b, b + G, b + 2G, ... Thread 0 keeps kHizStages 64x64 tiles in flight (TMA loads into
 // shared memory, one mbarrier per stage), so each SM keeps several hundred KB of
 // depth reads outstanding while its warps reduce the tile that has landed. The
 // reduction of a tile is the same as in hiz_build_kernel (hiz_tile.cuh), reading the
@@ -59,8 +59,9 @@ __global__ void __launch_bounds__(256, 3) hiz_build_kernel(HizJob single, const 
 constexpr int kHizStages = 3;
 constexpr uint32_t kHizTileBytes = kHizTile * kHizTile * 4u;
 constexpr uint32_t kHizWaitPolls = 1u << 20;  // bounded wait for a landed tile
+static_assert(2 * kHizTailBuf <= kHizStages * kHizTile * kHizTile, "the tail's two level buffers fit the staging");
 
-__global__ void __launch_bounds__(256, 3) hiz_build_tma_kernel(const __grid_constant__ CUtensorMap src,
+__global__ void __launch_bounds__(256, 4) hiz_build_tma_kernel(const __grid_constant__ CUtensorMap src,
                                                                const __grid_constant__ HizJob J, uint32_t* ticket,
                                                                uint32_t* error) {
     extern __shared__ __align__(128) unsigned char s_raw[];  // kHizStages x 64 x 64 floats (+128 B)
@@ -113,6 +114,13 @@ __global__ void __launch_bounds__(256, 3) hiz_build_tma_kernel(const __grid_cons
         __syncthreads();
         if (warp == 0) hiz_tile_levels456(J, t, s_m3);
     }
+    // A wait that gave up leaves later loads in flight: wait for them (bounded) before
+    // the tail reuses the staging buffers or the CTA's shared memory is released.
+    if (tid == 0) {
+        for (uint32_t j = k; j < k + kHizStages; ++j)
+            if (blockIdx.x + j * G < tiles)
+                mbar_wait_bounded(&s_full[j % kHizStages], (j / kHizStages) & 1u, kHizWaitPolls);
+    }
     // Levels 7..: every CTA takes one ticket after its last tile (one fence per CTA,
     // not per tile: warp 0 wrote all of this CTA's level-6 texels); the CTA that takes
     // the last ticket builds the tail with all 8 warps.
@@ -127,15 +135,9 @@ __global__ void __launch_bounds__(256, 3) hiz_build_tma_kernel(const __grid_cons
         __syncthreads();
         if (s_last) {
             __threadfence();
-            hiz_tail<8, 2>(J);
+            // Every tile has landed and been read: the staging buffers hold the tail's levels.
+            hiz_tail_in<8, 2>(J, s_stage, s_stage + kHizTailBuf);
         }
-    }
-    // A wait that gave up leaves later loads in flight: wait for them (bounded) before
-    // the CTA's shared memory is released.
-    if (tid == 0) {
-        for (uint32_t j = k; j < k + kHizStages; ++j)
-            if (blockIdx.x + j * G < tiles)
-                mbar_wait_bounded(&s_full[j % kHizStages], (j / kHizStages) & 1u, kHizWaitPolls);
     }
 }
 
