@@ -11,6 +11,7 @@
 
 #include <cudaTypedefs.h>  // PFN_cuTensorMapEncodeTiled
 
+#include <algorithm>
 #include <mutex>
 
 #include "common.cuh"
@@ -228,19 +229,29 @@ void launch_hiz_build_tma(const CUtensorMap& src, const HizJob& job, uint32_t* t
                           cudaStream_t stream) {
     const uint32_t tiles = job.tiles_x * job.tiles_y;
     if (tiles == 0) return;
-    static int per_sm = 0, sms = 0;
-    static std::once_flag once;
+    // Per device, once: the kernel's shared-memory limit (a per-device attribute) and its
+    // co-resident grid.
+    constexpr int kMaxDevices = 64;
+    static std::mutex mu;
+    static int grid_of[kMaxDevices] = {0};
     const size_t smem = kHizStages * kHizTileBytes + 128;
-    std::call_once(once, [smem] {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaFuncSetAttribute(hiz_build_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hiz_build_tma_kernel, 256, smem);
-        if (per_sm < 1) per_sm = 1;
-        if (sms < 1) sms = 1;
-    });
-    const uint32_t grid = std::min<uint32_t>(tiles, (uint32_t)(per_sm * sms));
+    int dev = 0;
+    cudaGetDevice(&dev);
+    int full = 0;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        if (dev < 0 || dev >= kMaxDevices || grid_of[dev] == 0) {
+            int sms = 0, per_sm = 0;
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            cudaFuncSetAttribute(hiz_build_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hiz_build_tma_kernel, 256, smem);
+            full = std::max(1, sms) * std::max(1, per_sm);
+            if (dev >= 0 && dev < kMaxDevices) grid_of[dev] = full;
+        } else {
+            full = grid_of[dev];
+        }
+    }
+    const uint32_t grid = std::min<uint32_t>(tiles, (uint32_t)full);
     helio_launch_begin("hiz_build_tma", stream);
     hiz_build_tma_kernel<<<grid, 256, smem, stream>>>(src, job, ticket_dev, error_dev);
     helio_launch_end(stream);

@@ -255,13 +255,10 @@ void launch_instance_cull(const InstanceCullParams& p, bool frustum, bool occlus
     if (p.draw_count == 0) return;
     if (!frustum && !occlusion) return;
     // Enough blocks to fill every SM 8 deep; each takes its share of the draws.
-    static int sms = 0;
-    if (sms == 0) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (sms < 1) sms = 1;
-    }
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);  // a cached attribute query
+    if (sms < 1) sms = 1;
     const uint32_t blocks = std::min<uint32_t>((p.draw_count + 255u) / 256u, (uint32_t)sms * 8u);
     helio_launch_begin(frustum && occlusion ? "instance_cull_fused" : frustum ? "indirect_dispatch" : "occlusion_cull",
                        stream);
