@@ -39,7 +39,8 @@ def test_hiz_alias_and_pitch(cuda, w, h):
     assert len(ref) == min(O.mip_levels(w, h), 12)
 
 
-@pytest.mark.parametrize("w,h", [(64, 64), (1000, 999), (1920, 1080), (3840, 2160), (256, 4096), (8192, 8)])
+@pytest.mark.parametrize("w,h", [(64, 64), (1000, 999), (1920, 1080), (3840, 2160), (256, 4096), (8192, 8),
+                                 (4, 1), (4, 4096), (68, 3), (32768, 2), (4100, 130)])
 def test_hiz_tma_and_plain_loads_agree(cuda, w, h):
     """The TMA tile-load path (persistent grid, several tiles in flight per CTA) and the
     128-bit-load path give the oracle's pyramid, with and without the level-0 copy."""
