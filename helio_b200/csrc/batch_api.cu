@@ -114,6 +114,14 @@ struct BatchPlan {
     uint32_t tiles = 0, pairs = 0, grid = 0, object_chunks = 0, span_capacity = 0, lod_pitch = 0;
 };
 
+// CTAs of the meshlet-test launch: the configured count (at most what fits), else the
+// same share of the device as the first launch's `grid` CTAs.
+uint32_t cull_grid_of(const helio_batch_config& cfg, uint32_t grid) {
+    const uint32_t full = helio::batch_max_grid(), cull_full = helio::batch_cull_max_grid();
+    if (cfg.cull_ctas) return std::min(cfg.cull_ctas, std::max(1u, cull_full));
+    return std::max(1u, (uint32_t)((uint64_t)cull_full * grid / std::max(1u, full)));
+}
+
 int32_t plan_batch(const helio_batch_config& cfg, const helio_vg_scene* sc, uint32_t n, const helio_batch_view* views,
                    BatchPlan& p, helio::BatchViewDev* dev) {
     p.level_off.assign(n, 0);
@@ -341,9 +349,10 @@ int32_t helio_batch_autotune(helio_batch* b, uint32_t repeats, helio_batch_tunin
     HELIO_CK(cudaEventCreate(&e0));
     HELIO_CK(cudaEventCreate(&e1));
     const helio_batch_config saved = b->cfg;
-    auto time_cfg = [&](uint32_t views, uint32_t ctas, double& ms) -> int32_t {
+    auto time_cfg = [&](uint32_t views, uint32_t ctas, uint32_t cull_ctas, double& ms) -> int32_t {
         b->cfg.select_views = views;
         b->cfg.max_ctas = ctas;
+        b->cfg.cull_ctas = cull_ctas;
         std::vector<float> t(repeats);
         int32_t st = helio_batch_execute(b, s);  // warm-up
         if (st) return st;
@@ -359,13 +368,14 @@ int32_t helio_batch_autotune(helio_batch* b, uint32_t repeats, helio_batch_tunin
         return HELIO_OK;
     };
     double base = 0.0, best = 1e30;
-    uint32_t best_v = 32, best_c = b->grid, n = 0;
-    int32_t st = time_cfg(saved.select_views, saved.max_ctas, base);
+    uint32_t best_v = 32, best_c = b->grid, best_cc = 0, n = 0;
+    int32_t st = time_cfg(saved.select_views, saved.max_ctas, saved.cull_ctas, base);
+    // Stage 1: the first launch's shape, the meshlet-test launch at its proportional share.
     for (uint32_t v = 8; !st && v <= 32; v += 8) {
         for (uint32_t k = 1; !st && k <= 3; ++k) {
             const uint32_t ctas = std::min<uint32_t>((uint32_t)sms * k, b->grid);
             double ms = 0.0;
-            if ((st = time_cfg(v, ctas, ms))) break;
+            if ((st = time_cfg(v, ctas, 0, ms))) break;
             ++n;
             if (ms < best) {
                 best = ms;
@@ -374,18 +384,31 @@ int32_t helio_batch_autotune(helio_batch* b, uint32_t repeats, helio_batch_tunin
             }
         }
     }
+    // Stage 2: the meshlet-test launch's CTAs per SM at the chosen first launch.
+    const uint32_t cull_full = helio::batch_cull_max_grid();
+    for (uint32_t k = 1; !st && (uint64_t)sms * k <= cull_full; ++k) {
+        double ms = 0.0;
+        if ((st = time_cfg(best_v, best_c, (uint32_t)sms * k, ms))) break;
+        ++n;
+        if (ms < best) {
+            best = ms;
+            best_cc = (uint32_t)sms * k;
+        }
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     b->cfg = saved;
     if (st) return st;
     b->cfg.select_views = best_v;
     b->cfg.max_ctas = best_c;
+    b->cfg.cull_ctas = best_cc;
     // Leave the outputs of the chosen configuration in the buffers.
     if ((st = helio_batch_execute(b, s))) return st;
     HELIO_CK(cudaStreamSynchronize(s));
     std::memset(out, 0, sizeof(*out));
     out->select_views = best_v;
     out->ctas = best_c;
+    out->cull_ctas = best_cc ? best_cc : cull_grid_of(b->cfg, best_c);
     out->candidates = n;
     out->best_ms = best;
     out->default_ms = base;
@@ -520,10 +543,7 @@ int32_t helio_batch_execute(helio_batch* b, void* stream) {
     P.shadow_work = b->shadow_work();
     if (b->shadow && helio::shadow_dev(b->shadow, &P.shadow)) P.shadow_blocks = P.shadow.blocks;
     const uint32_t grid = (b->cfg.max_ctas && b->cfg.max_ctas < b->grid) ? b->cfg.max_ctas : b->grid;
-    // The cull kernel takes the same share of the device as the select kernel.
-    const uint32_t full = helio::batch_max_grid(), cull_full = helio::batch_cull_max_grid();
-    const uint32_t cull_grid = std::max(1u, (uint32_t)((uint64_t)cull_full * grid / std::max(1u, full)));
-    HELIO_CK(helio::launch_batch(P, grid, cull_grid, s));
+    HELIO_CK(helio::launch_batch(P, grid, cull_grid_of(b->cfg, grid), s));
     return HELIO_OK;
 }
 

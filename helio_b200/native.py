@@ -174,11 +174,12 @@ class VgSceneInfo(C.Structure):
 
 
 class BatchConfig(C.Structure):
-    _fields_ = [("max_views", u32), ("flags", u32), ("max_spans", u64), ("max_ctas", u32), ("select_views", u32)]
+    _fields_ = [("max_views", u32), ("flags", u32), ("max_spans", u64), ("max_ctas", u32), ("select_views", u32),
+                ("cull_ctas", u32), ("reserved", u32)]
 
 
 class BatchTuning(C.Structure):
-    _fields_ = [("select_views", u32), ("ctas", u32), ("candidates", u32), ("reserved", u32),
+    _fields_ = [("select_views", u32), ("ctas", u32), ("candidates", u32), ("cull_ctas", u32),
                 ("best_ms", C.c_double), ("default_ms", C.c_double)]
 
 
@@ -227,7 +228,7 @@ HELIO_BATCH_SPAN_VISIBILITY = 1
 
 _SIZES = {GpuCameraUniforms: 368, GpuInstanceData: 144, GpuInstanceAabb: 32, GpuDrawCall: 20,
           DrawIndexedIndirectArgs: 20, GpuMeshletEntry: 64, GpuVgObject: 128, GpuVgDraw: 16, GpuVgWorkItem: 8,
-          InstanceCullData: 16, VgFrameData: 80, BatchConfig: 24, ServeConfig: 32, ServeRequest: 32,
+          InstanceCullData: 16, VgFrameData: 80, BatchConfig: 32, ServeConfig: 32, ServeRequest: 32,
           ServeCompletion: 80, ServeStats: 40}
 for _t, _n in _SIZES.items():
     assert C.sizeof(_t) == _n, (_t.__name__, C.sizeof(_t), _n)

@@ -381,9 +381,10 @@ class BatchedCull:
     per-view deterministic compaction)."""
 
     def __init__(self, max_views: int = N.HELIO_BATCH_MAX_VIEWS, span_visibility: bool = False, max_spans: int = 0,
-                 max_ctas: int = 0):
+                 max_ctas: int = 0, cull_ctas: int = 0):
         self._lib = N.cull_lib()
-        cfg = N.BatchConfig(max_views, N.HELIO_BATCH_SPAN_VISIBILITY if span_visibility else 0, max_spans, max_ctas)
+        cfg = N.BatchConfig(max_views, N.HELIO_BATCH_SPAN_VISIBILITY if span_visibility else 0, max_spans, max_ctas,
+                            0, cull_ctas)
         h = C.c_void_p()
         N.check(self._lib.helio_batch_create(C.byref(cfg), C.byref(h)))
         self._h = h
@@ -406,11 +407,12 @@ class BatchedCull:
 
     def autotune(self, repeats: int = 3, stream=None) -> dict:
         """Times the prepared batch under every launch-shape candidate (views per
-        select unit x CTAs per SM) and keeps the fastest (helio_batch_autotune)."""
+        select unit x CTAs per SM of the first launch, then CTAs per SM of the
+        meshlet-test launch) and keeps the fastest (helio_batch_autotune)."""
         t = N.BatchTuning()
         N.check(self._lib.helio_batch_autotune(self._h, repeats, C.byref(t), _stream_ptr(stream)))
-        return {"select_views": t.select_views, "ctas": t.ctas, "candidates": t.candidates, "best_ms": t.best_ms,
-                "default_ms": t.default_ms}
+        return {"select_views": t.select_views, "ctas": t.ctas, "cull_ctas": t.cull_ctas,
+                "candidates": t.candidates, "best_ms": t.best_ms, "default_ms": t.default_ms}
 
     def set_cameras_device(self, cameras: torch.Tensor, stream=None) -> None:
         """Cameras from a device tensor of view_count x 368 bytes (stream-ordered)."""

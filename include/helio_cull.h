@@ -493,6 +493,9 @@ typedef struct helio_batch_config {
     uint32_t max_ctas;     /* CTAs of the cooperative launch; 0 = as many as fit on the device.
                             * Fewer CTAs leave SMs free for batches launched on other streams. */
     uint32_t select_views; /* views tested per object load in the select (1..32); 0 = 32 */
+    uint32_t cull_ctas;    /* CTAs of the meshlet-test launch; 0 = the same share of the device
+                            * as max_ctas gives the first launch. Capped at what fits. */
+    uint32_t reserved;     /* 0 */
 } helio_batch_config;
 
 /* One view of a batch. */
@@ -579,14 +582,16 @@ int32_t helio_batch_set_wait_limit(helio_batch* batch, uint32_t max_polls, uint3
 int32_t helio_batch_estimate_bytes(const helio_batch_config* config, const helio_vg_scene* scene, uint32_t view_count,
                                    const helio_batch_view* views, uint64_t* bytes);
 /* Launch-shape autotuner: times helio_batch_execute of the prepared views (on
- * `stream`, `repeats` runs per candidate, median) for every candidate of select_views
- * {8, 16, 24, 32} x CTAs {1, 2, 3} per SM (at most the prepared grid), keeps the fastest
- * in the batch's configuration and reports it. Synchronises `stream`. */
+ * `stream`, `repeats` runs per candidate, median) in two stages: every select_views
+ * {8, 16, 24, 32} x CTAs {1, 2, 3} per SM of the first launch (at most the prepared grid),
+ * then, at the fastest of those, the meshlet-test launch at 1, 2, ... CTAs per SM (as many
+ * as fit). Keeps the fastest in the batch's configuration and reports it. Synchronises
+ * `stream`. */
 typedef struct helio_batch_tuning {
     uint32_t select_views;
     uint32_t ctas;
     uint32_t candidates;
-    uint32_t reserved;
+    uint32_t cull_ctas; /* CTAs of the meshlet-test launch chosen */
     double best_ms;
     double default_ms; /* the configuration before tuning */
 } helio_batch_tuning;

@@ -192,7 +192,7 @@ def kat_work_spans_library(k: dict):
 
 # ── batched multi-view cull ──────────────────────────────────────────────────
 
-def run_batch(scene, views, span_visibility=True, alias=False, capacities=None, repeats=1, max_ctas=0):
+def run_batch(scene, views, span_visibility=True, alias=False, capacities=None, repeats=1, max_ctas=0, cull_ctas=0):
     import torch
     from helio_b200 import scene as S
     from helio_b200.passes import BatchedCull, VgScene
@@ -200,7 +200,7 @@ def run_batch(scene, views, span_visibility=True, alias=False, capacities=None, 
     vs = VgScene()
     vs.upload(S.frame_data(scene))
     depths = [torch.from_numpy(np.ascontiguousarray(v.depth)).cuda() for v in views]
-    b = BatchedCull(len(views), span_visibility=span_visibility, max_ctas=max_ctas)
+    b = BatchedCull(len(views), span_visibility=span_visibility, max_ctas=max_ctas, cull_ctas=cull_ctas)
     specs = []
     for i, (v, d) in enumerate(zip(views, depths)):
         spec = {"camera": v.camera, "depth": d, "alias_mip0": alias, "lod_threshold_px": v.lod_threshold_px}
