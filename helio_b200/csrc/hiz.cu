@@ -51,27 +51,135 @@ __global__ void __launch_bounds__(256, 3) hiz_build_kernel(HizJob single, const 
     hiz_tile(s_J, s_job, tile - s_J.tile_begin, tickets, s_m3);
 }
 
-// Persistent form for one view whose level 0 TMA can address (4 CTAs per SM): CTA b takes
-// tiles b, b + G, b + 2G, ... Thread 0 keeps kHizStages 64x64 tiles in flight (TMA loads into
-// shared memory, one mbarrier per stage), so each SM keeps several hundred KB of
-// depth reads outstanding while its warps reduce the tile that has landed. The
-// reduction of a tile is the same as in hiz_build_kernel (hiz_tile.cuh), reading the
-// thread's 4x4 block from shared memory instead of global memory.
-constexpr int kHizStages = 3;
+// Persistent form for one view whose level 0 TMA can address: CTA b takes tiles b, b + G,
+// b + 2G, ... Thread 0 keeps kHizStages 64x64 tiles in flight per CTA (TMA loads into
+// shared memory, one mbarrier per stage). A CTA is 4 warps and warp q reduces quadrant q
+// (32x32 texels; q = 2 * row + column) of a landed tile on its own: each lane holds an
+// 8-row x 4-column block, registers give levels 1 and 2, warp shuffles levels 3..5. The
+// quadrants' level-5 texels meet in shared memory and thread 0 forms the tile's level-6
+// texel after the next tile's barrier, so a tile costs one barrier of 4 warps. Every 2x2
+// step takes its four texels in the order of hiz_build_kernel (top-left, top-right,
+// bottom-left, bottom-right) through hiz_red4, so both forms give identical pyramids.
+constexpr int kHizStages = 2;
+constexpr int kHizTmaThreads = 128;
+constexpr int kHizTmaCtasPerSm = 6;
 constexpr uint32_t kHizTileBytes = kHizTile * kHizTile * 4u;
 constexpr uint32_t kHizWaitPolls = 1u << 20;  // bounded wait for a landed tile
 static_assert(2 * kHizTailBuf <= kHizStages * kHizTile * kHizTile, "the tail's two level buffers fit the staging");
 
-__global__ void __launch_bounds__(256, 4) hiz_build_tma_kernel(const __grid_constant__ CUtensorMap src,
-                                                               const __grid_constant__ HizJob J, uint32_t* ticket,
-                                                               uint32_t* error) {
+// Level 0 of the lane's 8x4 block of quadrant q of the tile at (X0, Y0), when the job
+// does not alias it.
+__device__ __forceinline__ void hiz_quad_copy0(const HizJob& J, uint32_t X0, uint32_t Y0, int q,
+                                               const float (&v)[8][4]) {
+    if (!J.copy_mip0) return;
+    const int lane = threadIdx.x & 31;
+    const uint32_t bx = X0 + 32u * (q & 1) + 4u * (lane & 7), by = Y0 + 32u * (q >> 1) + 8u * (lane >> 3);
+    const uint32_t W = J.lw[0], H = J.lh[0], p0 = J.lpitch[0];
+    float* L0 = J.levels[0];
+    const bool al0 = ((p0 & 3u) == 0u) && ((reinterpret_cast<uintptr_t>(L0) & 15u) == 0u);
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+        if (by + r >= H) break;
+        float* row = L0 + (size_t)(by + r) * p0 + bx;
+        if (al0 && bx + 4 <= W) {
+            *reinterpret_cast<float4*>(row) = make_float4(v[r][0], v[r][1], v[r][2], v[r][3]);
+        } else {
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+                if (bx + c < W) row[c] = v[r][c];
+        }
+    }
+}
+
+// Stores texel (x, y) of level l when it lies inside the level.
+__device__ __forceinline__ void hiz_put(const HizJob& J, int l, uint32_t x, uint32_t y, float m) {
+    if (x < J.lw[l] && y < J.lh[l]) J.levels[l][(size_t)y * J.lpitch[l] + x] = m;
+}
+
+// Levels 1..5 of quadrant q of the tile at (X0, Y0) from the lane's 8x4 block v (lane =
+// 8 * block row + block column); returns the quadrant's level-5 texel in lane 0.
+__device__ __forceinline__ float hiz_quad_levels(const HizJob& J, uint32_t X0, uint32_t Y0, int q,
+                                                 const float (&v)[8][4]) {
+    const int lane = threadIdx.x & 31, lx = lane & 7, ly = lane >> 3;
+    const uint32_t qx = (uint32_t)(q & 1), qy = (uint32_t)(q >> 1);
+    // Level 1: 4 rows x 2 columns per lane.
+    float m1[4][2];
+    {
+        const bool xc = J.lw[0] == 1u, yc = J.lh[0] == 1u;
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int i = 0; i < 2; ++i)
+                m1[j][i] = hiz_red4(v[2 * j][2 * i], v[2 * j][2 * i + 1], v[2 * j + 1][2 * i],
+                                    v[2 * j + 1][2 * i + 1], xc, yc);
+        const uint32_t x1 = (X0 >> 1) + 16u * qx + 2u * lx, y1 = (Y0 >> 1) + 16u * qy + 4u * ly;
+        float* L1 = J.levels[1];
+        const uint32_t p1 = J.lpitch[1];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            if (y1 + j >= J.lh[1]) break;
+            float* row = L1 + (size_t)(y1 + j) * p1 + x1;
+            if (x1 + 2 <= J.lw[1] && ((p1 & 1u) == 0u)) {
+                *reinterpret_cast<float2*>(row) = make_float2(m1[j][0], m1[j][1]);
+            } else {
+                if (x1 < J.lw[1]) row[0] = m1[j][0];
+                if (x1 + 1 < J.lw[1]) row[1] = m1[j][1];
+            }
+        }
+    }
+    if (J.mip_count <= 2) return 0.0f;
+    // Level 2: 2 rows x 1 column per lane.
+    float m2[2];
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+        m2[j] = hiz_red4(m1[2 * j][0], m1[2 * j][1], m1[2 * j + 1][0], m1[2 * j + 1][1], J.lw[1] == 1u,
+                         J.lh[1] == 1u);
+        hiz_put(J, 2, (X0 >> 2) + 8u * qx + lx, (Y0 >> 2) + 8u * qy + 2u * ly + j, m2[j]);
+    }
+    if (J.mip_count <= 3) return 0.0f;
+    // Level 3: the right neighbour is lane + 1 (lanes with an even block column).
+    const float r0 = __shfl_xor_sync(0xffffffffu, m2[0], 1);
+    const float r1 = __shfl_xor_sync(0xffffffffu, m2[1], 1);
+    const float m3 = hiz_red4(m2[0], r0, m2[1], r1, J.lw[2] == 1u, J.lh[2] == 1u);
+    if ((lx & 1) == 0) hiz_put(J, 3, (X0 >> 3) + 4u * qx + (lx >> 1), (Y0 >> 3) + 4u * qy + ly, m3);
+    if (J.mip_count <= 4) return 0.0f;
+    // Level 4: right = lane + 2, below = lane + 8 (lanes with block column % 4 == 0 and
+    // an even block row).
+    const float b4 = __shfl_xor_sync(0xffffffffu, m3, 2);
+    const float c4 = __shfl_xor_sync(0xffffffffu, m3, 8);
+    const float d4 = __shfl_xor_sync(0xffffffffu, m3, 10);
+    const float m4 = hiz_red4(m3, b4, c4, d4, J.lw[3] == 1u, J.lh[3] == 1u);
+    if ((lx & 3) == 0 && (ly & 1) == 0)
+        hiz_put(J, 4, (X0 >> 4) + 2u * qx + (lx >> 2), (Y0 >> 4) + 2u * qy + (ly >> 1), m4);
+    if (J.mip_count <= 5) return 0.0f;
+    // Level 5: right = lane + 4, below = lane + 16 (lane 0).
+    const float b5 = __shfl_xor_sync(0xffffffffu, m4, 4);
+    const float c5 = __shfl_xor_sync(0xffffffffu, m4, 16);
+    const float d5 = __shfl_xor_sync(0xffffffffu, m4, 20);
+    const float m5 = hiz_red4(m4, b5, c5, d5, J.lw[4] == 1u, J.lh[4] == 1u);
+    if (lane == 0) hiz_put(J, 5, (X0 >> 5) + qx, (Y0 >> 5) + qy, m5);
+    return m5;
+}
+
+// Level 6 of tile t from its four quadrants' level-5 texels (one thread).
+__device__ __forceinline__ void hiz_quad_level6(const HizJob& J, uint32_t t, const float* l5) {
+    const uint32_t ty = t / J.tiles_x, tx = t - ty * J.tiles_x;
+    hiz_put(J, 6, tx, ty, hiz_red4(l5[0], l5[1], l5[2], l5[3], J.lw[5] == 1u, J.lh[5] == 1u));
+}
+
+__global__ void __launch_bounds__(kHizTmaThreads, kHizTmaCtasPerSm)
+    hiz_build_tma_kernel(const __grid_constant__ CUtensorMap src, const __grid_constant__ HizJob J, uint32_t* ticket,
+                         uint32_t* error) {
     extern __shared__ __align__(128) unsigned char s_raw[];  // kHizStages x 64 x 64 floats (+128 B)
     __shared__ __align__(8) uint64_t s_full[kHizStages];
+    __shared__ float s_l5[2][4];  // level-5 texels of the quadrants, double-buffered by tile
+    // The job in shared memory for the tail, whose fields of levels 7.. the tiles never read
+    // (read from the parameter space, each level would wait for a cold constant-cache line).
+    __shared__ __align__(16) HizJob s_J;
     // TMA writes its boxes at 128-byte aligned shared addresses.
     float* s_stage = reinterpret_cast<float*>(s_raw + ((128u - (smem_u32(s_raw) & 127u)) & 127u));
-    __shared__ float s_m3[8][9];
     const uint32_t tiles = J.tiles_x * J.tiles_y, G = gridDim.x;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int tid = threadIdx.x, lane = tid & 31, q = tid >> 5;
     auto issue = [&](uint32_t t, int s) {
         const uint32_t ty = t / J.tiles_x, tx = t - ty * J.tiles_x;
         mbar_arrive_expect_tx(&s_full[s], kHizTileBytes);
@@ -84,36 +192,56 @@ __global__ void __launch_bounds__(256, 4) hiz_build_tma_kernel(const __grid_cons
         for (int s = 0; s < kHizStages; ++s)
             if (blockIdx.x + s * G < tiles) issue(blockIdx.x + s * G, s);
     }
+    for (int i = tid; i < (int)(sizeof(HizJob) / 4); i += kHizTmaThreads)
+        reinterpret_cast<uint32_t*>(&s_J)[i] = reinterpret_cast<const uint32_t*>(&J)[i];
     __syncthreads();
-    const int tx4 = lane & 15, ty4 = warp * 2 + (lane >> 4);
-    uint32_t k = 0;
+    // The lane's 8x4 block within a staged tile.
+    const int block = (32 * (q >> 1) + 8 * (lane >> 3)) * (int)kHizTile + 32 * (q & 1) + 4 * (lane & 7);
+    uint32_t k = 0, prev = 0;
+    bool failed = false;
+    // The level-0 copy of the CTA's last tile waits until the CTA has taken its ticket, so
+    // that the ticket's release does not wait for those stores.
+    bool deferred = false;
+    uint32_t dX0 = 0, dY0 = 0;
+    float v[8][4];
     for (;; ++k) {
         const uint32_t t = blockIdx.x + k * G;
         if (t >= tiles) break;
         const int s = (int)(k % kHizStages);
         const bool landed = mbar_wait_bounded(&s_full[s], (k / kHizStages) & 1u, kHizWaitPolls);
+        const float* tile = s_stage + s * (kHizTile * kHizTile) + block;
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+            const float4 x = *reinterpret_cast<const float4*>(tile + r * kHizTile);
+            v[r][0] = x.x;
+            v[r][1] = x.y;
+            v[r][2] = x.z;
+            v[r][3] = x.w;
+        }
+        // Stage s is read by every warp (and the previous tile's level-5 texels are in s_l5).
         if (__syncthreads_or(!landed)) {
             if (tid == 0) atomicOr(error, kDevTimeout);
+            failed = true;
             break;
         }
-        float v[4][4];
-        const float* tile = s_stage + s * (kHizTile * kHizTile) + (4 * ty4) * kHizTile + 4 * tx4;
-#pragma unroll
-        for (int r = 0; r < 4; ++r) {
-            const float4 q = *reinterpret_cast<const float4*>(tile + r * kHizTile);
-            v[r][0] = q.x;
-            v[r][1] = q.y;
-            v[r][2] = q.z;
-            v[r][3] = q.w;
+        const uint32_t ty = t / J.tiles_x, tx = t - ty * J.tiles_x;
+        const uint32_t X0 = tx * kHizTile, Y0 = ty * kHizTile;
+        if (tid == 0) {
+            if (t + kHizStages * G < tiles) issue(t + kHizStages * G, s);
+            if (k > 0 && J.mip_count > 6) hiz_quad_level6(J, prev, s_l5[(k - 1) & 1]);
         }
-        __syncthreads();  // stage s is read (and warp 0 is done with the last tile's s_m3)
-        if (tid == 0 && t + kHizStages * G < tiles) issue(t + kHizStages * G, s);
-        hiz_tile_copy0(J, t, v);
-        if (J.mip_count <= 1) continue;
-        hiz_tile_levels123(J, t, v, s_m3);
-        if (J.mip_count <= 3) continue;
-        __syncthreads();
-        if (warp == 0) hiz_tile_levels456(J, t, s_m3);
+        if (J.mip_count > 1) {
+            const float m5 = hiz_quad_levels(J, X0, Y0, q, v);
+            if (lane == 0) s_l5[k & 1][q] = m5;
+        }
+        if (t + G >= tiles && J.mip_count > 7) {
+            deferred = true;
+            dX0 = X0;
+            dY0 = Y0;
+        } else {
+            hiz_quad_copy0(J, X0, Y0, q, v);
+        }
+        prev = t;
     }
     // A wait that gave up leaves later loads in flight: wait for them (bounded) before
     // the tail reuses the staging buffers or the CTA's shared memory is released.
@@ -122,23 +250,24 @@ __global__ void __launch_bounds__(256, 4) hiz_build_tma_kernel(const __grid_cons
             if (blockIdx.x + j * G < tiles)
                 mbar_wait_bounded(&s_full[j % kHizStages], (j / kHizStages) & 1u, kHizWaitPolls);
     }
-    // Levels 7..: every CTA takes one ticket after its last tile (one fence per CTA,
-    // not per tile: warp 0 wrote all of this CTA's level-6 texels); the CTA that takes
-    // the last ticket builds the tail with all 8 warps.
+    __syncthreads();  // the last tile's level-5 texels
+    if (tid == 0 && !failed && k > 0 && J.mip_count > 6) hiz_quad_level6(J, prev, s_l5[(k - 1) & 1]);
+    // Levels 7..: every CTA takes one ticket after its last tile; thread 0 wrote all of this
+    // CTA's level-6 texels, and its acquire-release add publishes them and, in the CTA with
+    // the last ticket, sees every other CTA's. That CTA builds the tail with all 4 warps.
     if (J.mip_count > 7) {
         __shared__ uint32_t s_last;
         if (tid == 0) {
-            __threadfence();
-            const uint32_t last = (atomicAdd(ticket, 1u) + 1u == G) ? 1u : 0u;
+            uint32_t old;
+            asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], 1;" : "=r"(old) : "l"(ticket) : "memory");
+            const uint32_t last = (old + 1u == G) ? 1u : 0u;
             if (last) *ticket = 0u;  // every other CTA has taken its ticket
             s_last = last;
         }
         __syncthreads();
-        if (s_last) {
-            __threadfence();
-            // Every tile has landed and been read: the staging buffers hold the tail's levels.
-            hiz_tail_in<8, 2>(J, s_stage, s_stage + kHizTailBuf);
-        }
+        if (deferred) hiz_quad_copy0(J, dX0, dY0, q, v);
+        // Every tile has landed and been read: the staging buffers hold the tail's levels.
+        if (s_last) hiz_tail_body<4, 4>(s_J, s_stage, s_stage + kHizTailBuf);
     }
 }
 
@@ -244,7 +373,7 @@ void launch_hiz_build_tma(const CUtensorMap& src, const HizJob& job, uint32_t* t
             int sms = 0, per_sm = 0;
             cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
             cudaFuncSetAttribute(hiz_build_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hiz_build_tma_kernel, 256, smem);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hiz_build_tma_kernel, kHizTmaThreads, smem);
             full = std::max(1, sms) * std::max(1, per_sm);
             if (dev >= 0 && dev < kMaxDevices) grid_of[dev] = full;
         } else {
@@ -253,7 +382,7 @@ void launch_hiz_build_tma(const CUtensorMap& src, const HizJob& job, uint32_t* t
     }
     const uint32_t grid = std::min<uint32_t>(tiles, (uint32_t)full);
     helio_launch_begin("hiz_build_tma", stream);
-    hiz_build_tma_kernel<<<grid, 256, smem, stream>>>(src, job, ticket_dev, error_dev);
+    hiz_build_tma_kernel<<<grid, kHizTmaThreads, smem, stream>>>(src, job, ticket_dev, error_dev);
     helio_launch_end(stream);
 }
 

@@ -51,7 +51,7 @@ __device__ __forceinline__ void hiz_tail_sync() {
 }
 
 template <int kWarps, int kRows>
-static __device__ __noinline__ void hiz_tail_in(const HizJob& J, float* bufA, float* bufB) {
+static __device__ __forceinline__ void hiz_tail_body(const HizJob& J, float* bufA, float* bufB) {
     const uint32_t lane = threadIdx.x & 31u, w = (threadIdx.x >> 5) % (uint32_t)kWarps;
     const uint32_t mips = J.mip_count;
     float* cur = nullptr;  // shared copy of the current source level (or null: read global)
@@ -105,6 +105,12 @@ static __device__ __noinline__ void hiz_tail_in(const HizJob& J, float* bufA, fl
             cur = nullptr;
         }
     }
+}
+
+// The same as a call of its own (callers that keep few registers live across it).
+template <int kWarps, int kRows>
+static __device__ __noinline__ void hiz_tail_in(const HizJob& J, float* bufA, float* bufB) {
+    hiz_tail_body<kWarps, kRows>(J, bufA, bufB);
 }
 
 // The tail with its two shared buffers declared here (bufA / bufB of kHizTailBuf floats).
