@@ -65,8 +65,8 @@ constexpr size_t kSmSelSpans = kSmSelLod + kSelectMaxViews * kBatchChunk;       
 constexpr size_t kSmSelMask = kSmSelSpans + 4 * kSelectMaxViews;                // u32[kSelectMaxViews][8]
 constexpr size_t kSmSelStats = kSmSelMask + 4 * 8 * kSelectMaxViews;             // u32[kSelectMaxViews][9]
 constexpr size_t kSmHizJob = kSmSelStats + 4 * 9 * kSelectMaxViews;             // HizJob
-constexpr size_t kSmHizM3 = kSmHizJob + ((sizeof(HizJob) + 15) / 16) * 16;    // float[2][8][9]
-constexpr size_t kSmMisc = kSmHizM3 + 2 * 8 * 9 * 4;                          // u32[64]
+constexpr size_t kSmHizL5 = kSmHizJob + ((sizeof(HizJob) + 15) / 16) * 16;    // float[2][4]
+constexpr size_t kSmMisc = kSmHizL5 + 2 * 4 * 4;                              // u32[64]
 constexpr size_t kSmTileBegin = kSmMisc + 64 * 4;                             // u32[kBatchMaxViews]
 constexpr size_t kSmTotal = kSmTileBegin + 4 * kBatchMaxViews;
 // An attached shadow cull's stages use the select units' LOD tile region, which no
@@ -373,7 +373,7 @@ __device__ void phase_hiz_tile(const BatchParams& P, uint32_t tile, char* sm) {
     const HizJob& J = *reinterpret_cast<const HizJob*>(sm + kSmHizJob);
     volatile uint32_t* s_job = reinterpret_cast<volatile uint32_t*>(sm + kSmMisc);
     const uint32_t* s_tb = reinterpret_cast<const uint32_t*>(sm + kSmTileBegin);
-    __syncthreads();  // the previous unit's warp 0 may still read s_m3 / J
+    __syncthreads();  // the previous unit's threads 0 and 32 may still read its level-5 texels / J
     if (threadIdx.x < 32) {
         uint32_t lo = 0, hi = P.view_count - 1;
         while (lo < hi) {
@@ -388,24 +388,29 @@ __device__ void phase_hiz_tile(const BatchParams& P, uint32_t tile, char* sm) {
         }
     }
     __syncthreads();
-    // Both tiles' loads are in flight together; warps 0 and 1 then finish one tile each.
+    // Warps 0..3 take the quadrants of the unit's first tile, warps 4..7 those of its
+    // second; each warp reduces its quadrant to level 5 alone, and one barrier brings the
+    // quadrants' level-5 texels together for level 6.
     const uint32_t lp = tile - s_tb[*s_job], t0 = 2u * lp, t1 = t0 + 1u;
     const bool has1 = t1 < J.tiles_x * J.tiles_y;  // uniform over the CTA
-    float (*m3a)[9] = reinterpret_cast<float(*)[9]>(sm + kSmHizM3);
-    float (*m3b)[9] = m3a + 8;
-    float v0[4][4], v1[4][4];
-    hiz_tile_load(J, t0, v0);
-    if (has1) hiz_tile_load(J, t1, v1);
-    hiz_tile_copy0(J, t0, v0);
-    if (has1) hiz_tile_copy0(J, t1, v1);
-    if (J.mip_count <= 1) return;
-    hiz_tile_levels123(J, t0, v0, m3a);
-    if (has1) hiz_tile_levels123(J, t1, v1, m3b);
-    if (J.mip_count <= 3) return;
+    const uint32_t warp = threadIdx.x >> 5, half = warp >> 2;
+    const int q = (int)(warp & 3u);
+    float* s_l5 = reinterpret_cast<float*>(sm + kSmHizL5);  // [2][4]
+    if (half == 0u || has1) {
+        const uint32_t t = half ? t1 : t0;
+        const uint32_t ty = t / J.tiles_x, tx = t - ty * J.tiles_x;
+        float v[8][4];
+        hiz_quad_load(J, t, q, v);
+        hiz_quad_copy0(J, tx * kHizTile, ty * kHizTile, q, v);
+        if (J.mip_count > 1) {
+            const float m5 = hiz_quad_levels(J, tx * kHizTile, ty * kHizTile, q, v);
+            if ((threadIdx.x & 31u) == 0u) s_l5[half * 4u + q] = m5;
+        }
+    }
+    if (J.mip_count <= 6) return;
     __syncthreads();
-    const uint32_t warp = threadIdx.x >> 5;
-    if (warp == 0) hiz_tile_levels456(J, t0, m3a);
-    else if (warp == 1 && has1) hiz_tile_levels456(J, t1, m3b);
+    if (threadIdx.x == 0) hiz_quad_level6(J, t0, s_l5);
+    else if (threadIdx.x == 32 && has1) hiz_quad_level6(J, t1, s_l5 + 4);
 }
 
 // ── Phase 1b: object select against a group of views (vg_cull.wgsl:282-352) ──

@@ -305,4 +305,137 @@ __device__ __forceinline__ void hiz_tile(const HizJob& J, uint32_t job, uint32_t
     hiz_ticket_tail(J, job, tickets);
 }
 
+// ── Warp per 32x32 quadrant ─────────────────────────────────────────────────
+// Warp q (0..3; q = 2 * row + column) of a tile reduces quadrant q alone: lane l holds
+// the 8-row x 4-column block at quadrant column 4 (l % 8), row 8 (l / 8); registers give
+// levels 1 and 2, shuffles levels 3..5, and the four quadrants' level-5 texels give
+// level 6 (hiz_quad_level6, one thread, after a barrier). Each 2x2 step takes its texels
+// in the order of the 4x4-per-thread form above (top-left, top-right, bottom-left,
+// bottom-right) through hiz_red4, so both forms give identical pyramids.
+
+// Level 0 of the lane's 8x4 block of quadrant q of tile `tile` from global memory;
+// outside the image the block reads 0 (those texels are never used).
+__device__ __forceinline__ void hiz_quad_load(const HizJob& J, uint32_t tile, int q, float (&v)[8][4]) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t tile_y = tile / J.tiles_x, tile_x = tile - tile_y * J.tiles_x;
+    const uint32_t bx = tile_x * kHizTile + 32u * (q & 1) + 4u * (lane & 7);
+    const uint32_t by = tile_y * kHizTile + 32u * (q >> 1) + 8u * (lane >> 3);
+    const uint32_t W = J.lw[0], H = J.lh[0];
+    const bool aligned = ((J.depth_pitch & 3u) == 0u) && ((reinterpret_cast<uintptr_t>(J.depth) & 15u) == 0u);
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+        const float* row = J.depth + (size_t)(by + r) * J.depth_pitch + bx;
+        if (aligned && bx + 4 <= W && by + r < H) {
+            const float4 x = __ldcs(reinterpret_cast<const float4*>(row));
+            v[r][0] = x.x;
+            v[r][1] = x.y;
+            v[r][2] = x.z;
+            v[r][3] = x.w;
+        } else {
+#pragma unroll
+            for (int c = 0; c < 4; ++c) v[r][c] = (bx + c < W && by + r < H) ? __ldcs(row + c) : 0.0f;
+        }
+    }
+}
+
+// Level 0 of the lane's 8x4 block of quadrant q of the tile at (X0, Y0) into the pyramid,
+// when the job does not alias it.
+__device__ __forceinline__ void hiz_quad_copy0(const HizJob& J, uint32_t X0, uint32_t Y0, int q,
+                                               const float (&v)[8][4]) {
+    if (!J.copy_mip0) return;
+    const int lane = threadIdx.x & 31;
+    const uint32_t bx = X0 + 32u * (q & 1) + 4u * (lane & 7), by = Y0 + 32u * (q >> 1) + 8u * (lane >> 3);
+    const uint32_t W = J.lw[0], H = J.lh[0], p0 = J.lpitch[0];
+    float* L0 = J.levels[0];
+    const bool al0 = ((p0 & 3u) == 0u) && ((reinterpret_cast<uintptr_t>(L0) & 15u) == 0u);
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+        if (by + r >= H) break;
+        float* row = L0 + (size_t)(by + r) * p0 + bx;
+        if (al0 && bx + 4 <= W) {
+            *reinterpret_cast<float4*>(row) = make_float4(v[r][0], v[r][1], v[r][2], v[r][3]);
+        } else {
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+                if (bx + c < W) row[c] = v[r][c];
+        }
+    }
+}
+
+// Stores texel (x, y) of level l when it lies inside the level.
+__device__ __forceinline__ void hiz_put(const HizJob& J, int l, uint32_t x, uint32_t y, float m) {
+    if (x < J.lw[l] && y < J.lh[l]) J.levels[l][(size_t)y * J.lpitch[l] + x] = m;
+}
+
+// Levels 1..5 of quadrant q of the tile at (X0, Y0) from the lane's 8x4 block v (lane =
+// 8 * block row + block column); returns the quadrant's level-5 texel in lane 0.
+__device__ __forceinline__ float hiz_quad_levels(const HizJob& J, uint32_t X0, uint32_t Y0, int q,
+                                                 const float (&v)[8][4]) {
+    const int lane = threadIdx.x & 31, lx = lane & 7, ly = lane >> 3;
+    const uint32_t qx = (uint32_t)(q & 1), qy = (uint32_t)(q >> 1);
+    // Level 1: 4 rows x 2 columns per lane.
+    float m1[4][2];
+    {
+        const bool xc = J.lw[0] == 1u, yc = J.lh[0] == 1u;
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int i = 0; i < 2; ++i)
+                m1[j][i] = hiz_red4(v[2 * j][2 * i], v[2 * j][2 * i + 1], v[2 * j + 1][2 * i],
+                                    v[2 * j + 1][2 * i + 1], xc, yc);
+        const uint32_t x1 = (X0 >> 1) + 16u * qx + 2u * lx, y1 = (Y0 >> 1) + 16u * qy + 4u * ly;
+        float* L1 = J.levels[1];
+        const uint32_t p1 = J.lpitch[1];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            if (y1 + j >= J.lh[1]) break;
+            float* row = L1 + (size_t)(y1 + j) * p1 + x1;
+            if (x1 + 2 <= J.lw[1] && ((p1 & 1u) == 0u)) {
+                *reinterpret_cast<float2*>(row) = make_float2(m1[j][0], m1[j][1]);
+            } else {
+                if (x1 < J.lw[1]) row[0] = m1[j][0];
+                if (x1 + 1 < J.lw[1]) row[1] = m1[j][1];
+            }
+        }
+    }
+    if (J.mip_count <= 2) return 0.0f;
+    // Level 2: 2 rows x 1 column per lane.
+    float m2[2];
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+        m2[j] = hiz_red4(m1[2 * j][0], m1[2 * j][1], m1[2 * j + 1][0], m1[2 * j + 1][1], J.lw[1] == 1u,
+                         J.lh[1] == 1u);
+        hiz_put(J, 2, (X0 >> 2) + 8u * qx + lx, (Y0 >> 2) + 8u * qy + 2u * ly + j, m2[j]);
+    }
+    if (J.mip_count <= 3) return 0.0f;
+    // Level 3: the right neighbour is lane + 1 (lanes with an even block column).
+    const float r0 = __shfl_xor_sync(0xffffffffu, m2[0], 1);
+    const float r1 = __shfl_xor_sync(0xffffffffu, m2[1], 1);
+    const float m3 = hiz_red4(m2[0], r0, m2[1], r1, J.lw[2] == 1u, J.lh[2] == 1u);
+    if ((lx & 1) == 0) hiz_put(J, 3, (X0 >> 3) + 4u * qx + (lx >> 1), (Y0 >> 3) + 4u * qy + ly, m3);
+    if (J.mip_count <= 4) return 0.0f;
+    // Level 4: right = lane + 2, below = lane + 8 (lanes with block column % 4 == 0 and
+    // an even block row).
+    const float b4 = __shfl_xor_sync(0xffffffffu, m3, 2);
+    const float c4 = __shfl_xor_sync(0xffffffffu, m3, 8);
+    const float d4 = __shfl_xor_sync(0xffffffffu, m3, 10);
+    const float m4 = hiz_red4(m3, b4, c4, d4, J.lw[3] == 1u, J.lh[3] == 1u);
+    if ((lx & 3) == 0 && (ly & 1) == 0)
+        hiz_put(J, 4, (X0 >> 4) + 2u * qx + (lx >> 2), (Y0 >> 4) + 2u * qy + (ly >> 1), m4);
+    if (J.mip_count <= 5) return 0.0f;
+    // Level 5: right = lane + 4, below = lane + 16 (lane 0).
+    const float b5 = __shfl_xor_sync(0xffffffffu, m4, 4);
+    const float c5 = __shfl_xor_sync(0xffffffffu, m4, 16);
+    const float d5 = __shfl_xor_sync(0xffffffffu, m4, 20);
+    const float m5 = hiz_red4(m4, b5, c5, d5, J.lw[4] == 1u, J.lh[4] == 1u);
+    if (lane == 0) hiz_put(J, 5, (X0 >> 5) + qx, (Y0 >> 5) + qy, m5);
+    return m5;
+}
+
+// Level 6 of tile t from its four quadrants' level-5 texels (one thread).
+__device__ __forceinline__ void hiz_quad_level6(const HizJob& J, uint32_t t, const float* l5) {
+    const uint32_t ty = t / J.tiles_x, tx = t - ty * J.tiles_x;
+    hiz_put(J, 6, tx, ty, hiz_red4(l5[0], l5[1], l5[2], l5[3], J.lw[5] == 1u, J.lh[5] == 1u));
+}
+
 }  // namespace helio
