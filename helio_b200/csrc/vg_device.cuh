@@ -126,6 +126,15 @@ __device__ __forceinline__ bool meshlet_hiz_visible(const CullView& C, F3 c, flo
             const float uvr = fmul(ndc_r, 0.5f);
             const float u0 = fsub(uv_x, uvr), v0 = fsub(uv_y, uvr), u1 = fadd(uv_x, uvr), v1 = fadd(uv_y, uvr);
             if (u0 >= 0.0f && v0 >= 0.0f && u1 <= 1.0f && v1 <= 1.0f) {
+                // The four texel loads first: the sphere's nearest depth below is computed
+                // while they are in flight (neither depends on the other).
+                const float half_h = fmul((float)C.screen_height, 0.5f);
+                const float dpx = fmaxf(fmul(fmul(ndc_r, half_h), 2.0f), 1.0f);
+                const uint32_t mip = min(ceil_log2_exact(dpx), C.hiz_mip_count - 1u);
+                const float h00 = hiz_sample<kCoherentHiz>(hz, u0, v0, mip);
+                const float h01 = hiz_sample<kCoherentHiz>(hz, u1, v0, mip);
+                const float h10 = hiz_sample<kCoherentHiz>(hz, u0, v1, mip);
+                const float h11 = hiz_sample<kCoherentHiz>(hz, u1, v1, mip);
                 const float dist_sq = dot3(ctc, ctc);
                 float near_z = 0.0f;
                 if (dist_sq > fmul(wr, wr)) {
@@ -134,13 +143,6 @@ __device__ __forceinline__ bool meshlet_hiz_visible(const CullView& C, F3 c, flo
                     const float4 nc = mat4_point4(C.vp, nws);
                     if (nc.w > 0.0f) near_z = clampf(fdiv(nc.z, nc.w), 0.0f, 1.0f);
                 }
-                const float half_h = fmul((float)C.screen_height, 0.5f);
-                const float dpx = fmaxf(fmul(fmul(ndc_r, half_h), 2.0f), 1.0f);
-                const uint32_t mip = min(ceil_log2_exact(dpx), C.hiz_mip_count - 1u);
-                const float h00 = hiz_sample<kCoherentHiz>(hz, u0, v0, mip);
-                const float h01 = hiz_sample<kCoherentHiz>(hz, u1, v0, mip);
-                const float h10 = hiz_sample<kCoherentHiz>(hz, u0, v1, mip);
-                const float h11 = hiz_sample<kCoherentHiz>(hz, u1, v1, mip);
                 const float hzv = fmaxf(fmaxf(h00, h01), fmaxf(h10, h11));
                 if (near_z > fadd(hzv, 1.0f / 65536.0f)) return false;
             }
