@@ -94,29 +94,44 @@ __device__ __forceinline__ uint32_t ld_cg(const uint32_t* p) { return __ldcg(p);
 // the wait gave up after P.spin_limit polls: kBatchErrTimeout is set and the caller
 // must end the CTA, since the data of the phase before the barrier may be incomplete
 // (the other CTAs then time out at their next barrier and end too).
+// GPU-scope acquire / release operations of the barrier and the setup counter.
+__device__ __forceinline__ uint32_t atom_add_acq_rel(uint32_t* p, uint32_t v) {
+    uint32_t old;
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
+__device__ __forceinline__ void red_add_release(uint32_t* p, uint32_t v) {
+    asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ uint32_t ld_acquire(const uint32_t* p) {
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Thread 0 of each CTA arrives with an acquire-release add (releasing what the CTA wrote
+// before the block barrier); the last arrival resets the count and releases the next
+// generation, which the others poll with acquire loads (spinning first, then backing off).
 __device__ bool grid_sync(const BatchParams& P) {
     __syncthreads();
     int timed_out = 0;
     if (threadIdx.x == 0) {
-        volatile uint32_t* gen = P.barrier + 1;
-        const uint32_t g = *gen;
-        __threadfence();
-        if (atomicAdd(P.barrier, 1u) == gridDim.x - 1 + P.barrier_extra) {
+        uint32_t* gen = P.barrier + 1;
+        const uint32_t g = ld_acquire(gen);
+        if (atom_add_acq_rel(P.barrier, 1u) == gridDim.x - 1 + P.barrier_extra) {
             P.barrier[0] = 0u;
-            __threadfence();
-            atomicAdd(P.barrier + 1, 1u);
+            red_add_release(gen, 1u);
         } else {
             uint32_t polls = 0;
-            while (*gen == g) {
+            while (ld_acquire(gen) == g) {
                 if (++polls > P.spin_limit) {
                     atomicOr(P.error, kBatchErrTimeout);
                     timed_out = 1;
                     break;
                 }
-                __nanosleep(polls < 256 ? 64 : 256);
+                if (polls > 64) __nanosleep(polls < 512 ? 64 : 256);
             }
         }
-        __threadfence();
     }
     return __syncthreads_or(timed_out) == 0;
 }
@@ -351,8 +366,7 @@ __device__ void phase_setup(const BatchParams& P) {
             c.hiz_mip_count = V.hiz_mip_count;
             c.pad[0] = c.pad[1] = 0u;
             P.cviews[v] = c;
-            __threadfence();
-            atomicAdd(P.setup_done, 1u);  // the select units wait for every view
+            red_add_release(P.setup_done, 1u);  // the select units wait for every view
         }
         __syncwarp();
     }
@@ -985,15 +999,14 @@ __device__ bool load_sel_views(const BatchParams& P, char* sm) {
     int timed_out = 0;
     if (threadIdx.x == 0) {
         uint32_t polls = 0;
-        while (ld_cg(P.setup_done) < P.view_count) {
+        while (ld_acquire(P.setup_done) < P.view_count) {
             if (++polls > P.spin_limit) {
                 atomicOr(P.error, kBatchErrTimeout);
                 timed_out = 1;
                 break;
             }
-            __nanosleep(polls < 256 ? 64 : 256);
+            if (polls > 64) __nanosleep(polls < 512 ? 64 : 256);
         }
-        __threadfence();
     }
     if (__syncthreads_or(timed_out)) return false;
     SelView* s_sv = reinterpret_cast<SelView*>(sm + kSmSelViews);
