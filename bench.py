@@ -1116,7 +1116,29 @@ def run_serve(args, rank, world, local_rank):
         "plain_per_request": plain, "cpu_baseline": cpu, "e2e": None, "roofline": None,
         "gpu_launches": int(launches), "clocks": clk,
         "batch_requests_mean": statistics.mean(c["batch_requests"] for c in timed),
+        "device": device_occupancy(timed),
     }
+
+
+def device_occupancy(completions) -> dict:
+    """How busy the device was over the timed requests' batches: the union of the batches'
+    device intervals (CUDA events on each slot's stream) over the span from the first
+    batch start to the last batch end, and the mean device time of a batch."""
+    spans = sorted({(c["device_start_ms"], c["device_end_ms"]) for c in completions if c["status"] == 0})
+    if not spans:
+        return None
+    busy, cur_s, cur_e = 0.0, spans[0][0], spans[0][1]
+    for s0, e0 in spans[1:]:
+        if s0 > cur_e:
+            busy += cur_e - cur_s
+            cur_s, cur_e = s0, e0
+        else:
+            cur_e = max(cur_e, e0)
+    busy += cur_e - cur_s
+    total = spans[-1][1] - spans[0][0] if len(spans) > 1 else busy
+    total = max(total, max(e for _, e in spans) - spans[0][0])
+    return {"batches": len(spans), "busy_fraction": busy / total if total > 0 else None,
+            "batch_device_ms_mean": statistics.mean(e - s for s, e in spans), "span_ms": total}
 
 
 # ── CPU baseline / reference arm (the oracle) ────────────────────────────────

@@ -441,7 +441,8 @@ int32_t helio_batch_growth_bytes(const helio_batch* b, const helio_batch_config*
     helio_batch* mb = const_cast<helio_batch*>(b);
     for (int k = 0; k < kBatchBufs; ++k) {
         const DevBuf& d = mb->buf(k);
-        if (!d.ptr || plan.need[k] > d.bytes) grow += plan.need[k] - (d.ptr ? d.bytes : 0);
+        const size_t held = d.ptr ? d.bytes : 0;
+        if (!d.ptr || plan.need[k] > d.bytes) grow += helio::grow_capacity(plan.need[k], held) - held;
     }
     *bytes = grow;
     return HELIO_OK;

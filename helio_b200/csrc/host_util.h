@@ -25,6 +25,17 @@ namespace helio {
 inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 
 // Owned device allocation with grow-only semantics.
+// Bytes to hold for `need` when `held` bytes are allocated: a buffer that must grow takes at
+// least 1.5x what it held, so that a buffer which keeps growing (a server's batches of
+// changing shapes) is reallocated a logarithmic number of times (cudaFree synchronises the
+// whole device). A first allocation takes exactly `need`.
+inline size_t grow_capacity(size_t need, size_t held) {
+    if (need <= held) return held;
+    if (held == 0) return need;
+    const size_t g = held + held / 2;
+    return need > g ? need : g;
+}
+
 struct DevBuf {
     void* ptr = nullptr;
     size_t bytes = 0;
@@ -39,10 +50,11 @@ struct DevBuf {
     }
     cudaError_t ensure(size_t need) {
         if (need <= bytes && ptr) return cudaSuccess;
-        release();
         if (need == 0) need = 16;
-        cudaError_t e = cudaMalloc(&ptr, need);
-        if (e == cudaSuccess) bytes = need;
+        const size_t cap = grow_capacity(need, ptr ? bytes : 0);
+        release();
+        cudaError_t e = cudaMalloc(&ptr, cap);
+        if (e == cudaSuccess) bytes = cap;
         return e;
     }
     template <typename T>
