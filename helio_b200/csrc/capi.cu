@@ -737,7 +737,7 @@ int32_t helio_vg_execute(helio_vg_pass* p, const HelioGpuCameraUniforms* camera_
     cp.capacity = p->max_draw_count;  // min(draw_capacity, buffer lengths), vg_cull.wgsl:248-251
     cp.num_tiles = p->num_tiles;
     cp.items_per_warp = p->items_per_warp;
-    helio::launch_vg_cull(cp, s);
+    HELIO_CK(helio::launch_vg_cull(cp, s));
     HELIO_CK(cudaGetLastError());
     return HELIO_OK;
 }

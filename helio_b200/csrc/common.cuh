@@ -213,6 +213,15 @@ __device__ __forceinline__ bool sphere_visible_vg(const Planes& pl, F3 c, float 
     return v;
 }
 
+// Programmatic dependent launch. A kernel launched with programmatic stream serialization
+// may start while the previous kernel of its stream still runs; pdl_wait returns once that
+// kernel has completed and its writes are visible (at once in a kernel launched normally), so
+// it goes before the first read of anything the previous kernel wrote. pdl_launch_dependents
+// lets the stream's next kernel, when so launched, be scheduled once every CTA of this kernel
+// has called it or ended.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 // Device error word values.
 enum : uint32_t { kDevOk = 0u, kDevTimeout = 1u };
 

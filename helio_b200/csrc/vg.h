@@ -119,6 +119,6 @@ void launch_instance_cull_data(const HelioGpuInstanceData* inst, uint32_t n, Hel
 void launch_vg_view_setup(const ViewSetupParams& p, cudaStream_t stream);
 void launch_vg_select(const VgSelectParams& p, cudaStream_t stream);
 // Test kernel then emit kernel on `stream`.
-void launch_vg_cull(const VgCullParams& p, cudaStream_t stream);
+cudaError_t launch_vg_cull(const VgCullParams& p, cudaStream_t stream);
 
 }  // namespace helio

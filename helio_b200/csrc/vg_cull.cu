@@ -120,6 +120,7 @@ __global__ void __launch_bounds__(32) vg_view_setup_kernel(ViewSetupParams P) {
 
 __global__ void __launch_bounds__(256) vg_select_kernel(VgSelectParams P) {
     __shared__ CullView s_view;
+    pdl_launch_dependents();  // the meshlet tests may be scheduled (they wait for this grid)
     if (P.compute_view) {
         // The view setup folded in: warp 0 builds the constants; block 0 publishes them.
         if (threadIdx.x < 32) view_setup_warp(P.setup, s_view);
@@ -242,7 +243,9 @@ __global__ void __launch_bounds__(kCullWarps * 32) vg_cull_test_kernel(VgCullPar
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const VgSceneDev& S = P.scene;
     const uint32_t tile = blockIdx.x;
+    pdl_launch_dependents();  // the emission may be scheduled (it waits for this grid)
     for (int k = lane; k < kBitWordsPerWarp; k += 32) s_bits[warp][k] = 0u;
+    pdl_wait();  // the select's records and view constants
     const bool mine = (uint32_t)lane < P.items_per_warp;
     const uint32_t w_idx = (tile * kCullWarps + warp) * P.items_per_warp + lane;
     const WarpItems it = load_warp_items(S, P.sel, mine ? w_idx : 0xFFFFFFFFu);
@@ -309,6 +312,7 @@ __global__ void __launch_bounds__(kCullWarps * 32) vg_cull_emit_kernel(VgCullPar
     __shared__ uint32_t s_prefix;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t tile = blockIdx.x;
+    pdl_wait();  // the meshlet tests' counts and window bits
     const uint32_t count = P.scratch.tile_counts[tile];
     if (count == 0u) return;  // uniform: the whole CTA leaves
 
@@ -403,14 +407,36 @@ void launch_vg_select(const VgSelectParams& p, cudaStream_t stream) {
     helio_launch_end(stream);
 }
 
-void launch_vg_cull(const VgCullParams& p, cudaStream_t stream) {
-    if (!p.num_tiles) return;
+namespace {
+
+// The meshlet tests and the emission are launched with programmatic stream serialization:
+// each may be scheduled while the kernel before it finishes (its CTAs wait in pdl_wait), which
+// hides a launch gap per kernel.
+cudaError_t launch_after(void (*kernel)(VgCullParams), uint32_t grid, const VgCullParams& p, cudaStream_t stream) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(kCullWarps * 32);
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, p);
+}
+
+}  // namespace
+
+cudaError_t launch_vg_cull(const VgCullParams& p, cudaStream_t stream) {
+    if (!p.num_tiles) return cudaSuccess;
     helio_launch_begin("vg_cull_test", stream);
-    vg_cull_test_kernel<<<p.num_tiles, kCullWarps * 32, 0, stream>>>(p);
+    cudaError_t e = launch_after(vg_cull_test_kernel, p.num_tiles, p, stream);
     helio_launch_end(stream);
+    if (e != cudaSuccess) return e;
     helio_launch_begin("vg_cull_emit", stream);
-    vg_cull_emit_kernel<<<p.num_tiles, kCullWarps * 32, 0, stream>>>(p);
+    e = launch_after(vg_cull_emit_kernel, p.num_tiles, p, stream);
     helio_launch_end(stream);
+    return e;
 }
 
 }  // namespace helio
