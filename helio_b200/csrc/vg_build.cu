@@ -229,7 +229,6 @@ struct BuildOut {
 __global__ void __launch_bounds__(kThreads) place_kernel(helio_vg_build_inputs in, const uint32_t* first_ref,
                                                          const uint64_t* block_base, BuildOut out) {
     __shared__ uint64_t s[kVals][kThreads / 32];
-    const uint32_t lane = threadIdx.x & 31u;
     uint64_t carry[kVals];
 #pragma unroll
     for (uint32_t k = 0; k < kVals; ++k) carry[k] = block_base[(size_t)blockIdx.x * kVals + k];
@@ -246,21 +245,6 @@ __global__ void __launch_bounds__(kThreads) place_kernel(helio_vg_build_inputs i
             at[k] = (uint32_t)(carry[k] + x[k] - v.v[k]);
             carry[k] += total[k];
         }
-        // The warp's used slots have consecutive object indices: their instances are
-        // copied by the whole warp, 16-byte words in order (coalesced reads and writes).
-        const uint32_t used_mask = __ballot_sync(0xffffffffu, v.used);
-        if (used_mask) {
-            constexpr uint32_t kW = sizeof(HelioGpuInstanceData) / 16;  // 9 words per instance
-            const uint32_t obj0 = __shfl_sync(0xffffffffu, at[0], __ffs(used_mask) - 1u);
-            const uint32_t slot0 = o - lane;
-            const uint4* src = reinterpret_cast<const uint4*>(in.slot_instances);
-            uint4* dst = reinterpret_cast<uint4*>(out.instances + obj0);
-            const uint32_t words = __popc(used_mask) * kW;
-            for (uint32_t w = lane; w < words; w += 32u) {
-                const uint32_t k = w / kW;  // k-th used lane of the warp
-                dst[w] = src[(size_t)(slot0 + nth_set_bit(used_mask, k)) * kW + (w - k * kW)];
-            }
-        }
         if (v.used) {
             out.obj_of_slot[o] = at[0];
             for (uint32_t i = 0; i < v.v[2]; ++i)
@@ -274,7 +258,8 @@ __global__ void __launch_bounds__(kThreads) place_kernel(helio_vg_build_inputs i
 }
 
 // One thread per slot. A warp's used slots have consecutive object indices, so the
-// warp writes their records as one contiguous run of 16-byte words: lane t of round r
+// warp copies their instances and writes their records as contiguous runs of 16-byte
+// words. For the records, lane t of round r
 // takes word w = t % 8 of the warp's k-th used slot (k = (32 r + t) / 8), reads that
 // word of its mesh record (four whole records per load instruction) and stores it in
 // place. The object record is the mesh record with word 0 replaced (object index,
@@ -290,6 +275,20 @@ __global__ void __launch_bounds__(kThreads) objects_kernel(helio_vg_build_inputs
     const uint32_t lead = __ffs(used_mask) - 1u;
     const uint32_t obj0 = __shfl_sync(0xffffffffu, used ? out.obj_of_slot[o] : 0u, lead);
     const uint32_t n_used = __popc(used_mask);
+    // The warp's instances, copied by the whole warp as 16-byte words in order (coalesced
+    // reads and writes); done here rather than after the placement scan, whose block
+    // barriers would hold the loads back.
+    {
+        constexpr uint32_t kW = sizeof(HelioGpuInstanceData) / 16;  // 9 words per instance
+        const uint32_t slot0 = o - lane;
+        const uint4* src = reinterpret_cast<const uint4*>(in.slot_instances);
+        uint4* idst = reinterpret_cast<uint4*>(out.instances + obj0);
+        const uint32_t words = n_used * kW;
+        for (uint32_t w = lane; w < words; w += 32u) {
+            const uint32_t k = w / kW;  // k-th used lane of the warp
+            idst[w] = src[(size_t)(slot0 + nth_set_bit(used_mask, k)) * kW + (w - k * kW)];
+        }
+    }
     uint4* dst = reinterpret_cast<uint4*>(out.objects + obj0);
     bool over = false;
     const uint32_t rounds = (n_used * 8u + 31u) / 32u;  // the same for every lane of the warp
