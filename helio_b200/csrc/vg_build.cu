@@ -221,7 +221,22 @@ struct BuildOut {
     uint32_t* obj_of_slot;  // [slot_count]: object index of a used slot
     uint32_t* mesh_base;    // [mesh_count]: first descriptor of a used mesh in the output
     uint32_t* mesh_order;   // [used meshes]: mesh of each first reference, in slot order
+    const uint64_t* totals;  // the scan's kVals totals, then the error word
+    uint64_t cap_objects, cap_meshlets, cap_items;  // records the output buffers hold
 };
+
+// The output passes are launched before the host has read the scan's totals, with the
+// buffers the builder holds. They write only when the totals fit those buffers and the
+// reference would not have stopped (a used mesh's descriptors leave the pool, or a count
+// exceeds u32); otherwise every thread leaves at once and the host, after reading the
+// totals, grows the buffers and runs the passes again (or reports the error).
+__device__ __forceinline__ bool outputs_fit(const BuildOut& o) {
+    const uint64_t objects = __ldcg(o.totals + 0), descs = __ldcg(o.totals + 1), items = __ldcg(o.totals + 2);
+    const uint64_t draws = __ldcg(o.totals + 4);
+    const uint32_t err = __ldcg(reinterpret_cast<const uint32_t*>(o.totals + kVals));
+    return (err & kErrPool) == 0u && descs <= 0xFFFFFFFFull && items <= 0xFFFFFFFFull && draws <= 0xFFFFFFFFull &&
+           objects <= o.cap_objects && descs <= o.cap_meshlets && items <= o.cap_items;
+}
 
 // A block of kScanBlock slots, as kSub sub-blocks of 256 in slot order: each sub-block's
 // scan plus the block's base and the earlier sub-blocks' sums gives every slot its
@@ -229,6 +244,7 @@ struct BuildOut {
 __global__ void __launch_bounds__(kThreads) place_kernel(helio_vg_build_inputs in, const uint32_t* first_ref,
                                                          const uint64_t* block_base, BuildOut out) {
     __shared__ uint64_t s[kVals][kThreads / 32];
+    if (!outputs_fit(out)) return;  // uniform over the grid
     uint64_t carry[kVals];
 #pragma unroll
     for (uint32_t k = 0; k < kVals; ++k) carry[k] = block_base[(size_t)blockIdx.x * kVals + k];
@@ -241,7 +257,7 @@ __global__ void __launch_bounds__(kThreads) place_kernel(helio_vg_build_inputs i
         block_scan5<kThreads>(x, s, total);  // uniform over the block: every thread takes part
         uint32_t at[kVals];
 #pragma unroll
-        for (uint32_t k = 0; k < kVals; ++k) {  // the totals fit in u32 (checked on the host before this launch)
+        for (uint32_t k = 0; k < kVals; ++k) {  // the totals fit in u32 (outputs_fit)
             at[k] = (uint32_t)(carry[k] + x[k] - v.v[k]);
             carry[k] += total[k];
         }
@@ -267,6 +283,7 @@ __global__ void __launch_bounds__(kThreads) place_kernel(helio_vg_build_inputs i
 // mesh's base.
 __global__ void __launch_bounds__(kThreads) objects_kernel(helio_vg_build_inputs in, BuildOut out, uint32_t* error) {
     static_assert(sizeof(HelioGpuVgObject) == 128 && sizeof(HelioVgMeshRecord) == 128, "record layouts");
+    if (!outputs_fit(out)) return;  // uniform over the grid
     const uint32_t o = blockIdx.x * kThreads + threadIdx.x, lane = threadIdx.x & 31u;
     const uint32_t m = o < in.slot_count ? in.slot_mesh[o] : HELIO_VG_NO_MESH;
     const bool used = o < in.slot_count && mesh_used(in.meshes, in.mesh_count, m);
@@ -311,7 +328,10 @@ __global__ void __launch_bounds__(kThreads) objects_kernel(helio_vg_build_inputs
 }
 
 // One warp per used mesh, in first-reference order: its descriptors, 4 x 16 bytes each.
-__global__ void copy_descriptors_kernel(helio_vg_build_inputs in, BuildOut out, uint32_t used_meshes) {
+// The grid is sized for every mesh of the library; the used ones are counted by the scan.
+__global__ void copy_descriptors_kernel(helio_vg_build_inputs in, BuildOut out) {
+    if (!outputs_fit(out)) return;  // uniform over the grid
+    const uint32_t used_meshes = (uint32_t)__ldcg(out.totals + 3);
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t w0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, W = (gridDim.x * blockDim.x) >> 5;
     for (uint32_t r = w0; r < used_meshes; r += W) {
@@ -392,6 +412,35 @@ int32_t helio_vg_builder_run(helio_vg_builder* b, const helio_vg_build_inputs* i
                                                   b->totals.as<uint64_t>());
         helio_launch_note();
     }
+    // The output passes with the buffers held now (a first run, or a larger library, finds
+    // them too small: the passes then leave at once and run again below, once sized).
+    auto outputs = [&]() {
+        BuildOut o{b->meshlets.as<HelioGpuMeshletEntry>(), b->objects.as<HelioGpuVgObject>(),
+                   b->instances.as<HelioGpuInstanceData>(), b->items.as<HelioGpuVgWorkItem>(),
+                   b->obj_of_slot.as<uint32_t>(), b->mesh_base.as<uint32_t>(), b->mesh_order.as<uint32_t>(),
+                   b->totals.as<uint64_t>(), 0, 0, 0};
+        o.cap_objects = std::min(b->objects.bytes / sizeof(HelioGpuVgObject),
+                                 b->instances.bytes / sizeof(HelioGpuInstanceData));
+        o.cap_meshlets = b->meshlets.bytes / sizeof(HelioGpuMeshletEntry);
+        o.cap_items = b->items.bytes / sizeof(HelioGpuVgWorkItem);
+        return o;
+    };
+    auto launch_outputs = [&](const BuildOut& o) {
+        if (!S) return;
+        place_kernel<<<blocks, kThreads, 0, s>>>(*in, b->first_ref.as<uint32_t>(), b->block_base.as<uint64_t>(), o);
+        helio_launch_note();
+        objects_kernel<<<(uint32_t)(((uint64_t)S + kThreads - 1) / kThreads), kThreads, 0, s>>>(*in, o, error);
+        helio_launch_note();
+        if (M) {
+            copy_descriptors_kernel<<<grid_for((uint64_t)M * 32u, kThreads), kThreads, 0, s>>>(*in, o);
+            helio_launch_note();
+        }
+    };
+    const BuildOut held = outputs();
+    launch_outputs(held);
+    // The bracket ends with the last launch, before the read-back (later launches of a run
+    // that had to grow its outputs are counted, not timed).
+    if (any) helio_launch_end(s);
     cudaError_t e = cudaGetLastError();
     uint64_t tot[kVals + 1] = {0};
     if (e == cudaSuccess) e = cudaMemcpyAsync(tot, b->totals.ptr, sizeof(tot), cudaMemcpyDeviceToHost, s);
@@ -404,37 +453,19 @@ int32_t helio_vg_builder_run(helio_vg_builder* b, const helio_vg_build_inputs* i
                       : tot[2] > 0xFFFFFFFFull ? "virtual geometry exceeds the u32 work-item address space"
                       : tot[4] > 0xFFFFFFFFull ? "virtual geometry indirect draw capacity exceeds u32"
                                                : nullptr;
-    if (why) {
-        if (any) helio_launch_end(s);
-        return helio_fail(e != cudaSuccess ? HELIO_ERR_CUDA : HELIO_ERR_INVALID_ARG, "%s", why);
+    if (why) return helio_fail(e != cudaSuccess ? HELIO_ERR_CUDA : HELIO_ERR_INVALID_ARG, "%s", why);
+    const uint64_t objects = tot[0], descriptors = tot[1], items = tot[2];
+    if (objects > held.cap_objects || descriptors > held.cap_meshlets || items > held.cap_items) {
+        if ((e = b->meshlets.ensure(descriptors * sizeof(HelioGpuMeshletEntry))) == cudaSuccess &&
+            (e = b->objects.ensure(objects * sizeof(HelioGpuVgObject))) == cudaSuccess &&
+            (e = b->instances.ensure(objects * sizeof(HelioGpuInstanceData))) == cudaSuccess)
+            e = b->items.ensure(items * sizeof(HelioGpuVgWorkItem));
+        if (e != cudaSuccess) return helio_fail(HELIO_ERR_CUDA, "vg_build outputs: %s", cudaGetErrorString(e));
+        launch_outputs(outputs());
+        HELIO_CK(cudaGetLastError());
+        HELIO_CK(cudaMemcpyAsync(&err, error, 4, cudaMemcpyDeviceToHost, s));
+        HELIO_CK(cudaStreamSynchronize(s));
     }
-    const uint64_t objects = tot[0], descriptors = tot[1], items = tot[2], used_meshes = tot[3];
-    if ((e = b->meshlets.ensure(descriptors * sizeof(HelioGpuMeshletEntry))) == cudaSuccess &&
-        (e = b->objects.ensure(objects * sizeof(HelioGpuVgObject))) == cudaSuccess &&
-        (e = b->instances.ensure(objects * sizeof(HelioGpuInstanceData))) == cudaSuccess)
-        e = b->items.ensure(items * sizeof(HelioGpuVgWorkItem));
-    if (e != cudaSuccess) {
-        if (any) helio_launch_end(s);
-        return helio_fail(HELIO_ERR_CUDA, "vg_build outputs: %s", cudaGetErrorString(e));
-    }
-    BuildOut o{b->meshlets.as<HelioGpuMeshletEntry>(), b->objects.as<HelioGpuVgObject>(),
-               b->instances.as<HelioGpuInstanceData>(), b->items.as<HelioGpuVgWorkItem>(),
-               b->obj_of_slot.as<uint32_t>(), b->mesh_base.as<uint32_t>(), b->mesh_order.as<uint32_t>()};
-    if (S) {
-        place_kernel<<<blocks, kThreads, 0, s>>>(*in, b->first_ref.as<uint32_t>(), b->block_base.as<uint64_t>(), o);
-        helio_launch_note();
-        objects_kernel<<<(uint32_t)(((uint64_t)S + kThreads - 1) / kThreads), kThreads, 0, s>>>(*in, o, error);
-        helio_launch_note();
-    }
-    if (used_meshes) {
-        copy_descriptors_kernel<<<grid_for(used_meshes * 32u, kThreads), kThreads, 0, s>>>(*in, o,
-                                                                                          (uint32_t)used_meshes);
-        helio_launch_note();
-    }
-    if (any) helio_launch_end(s);
-    HELIO_CK(cudaGetLastError());
-    HELIO_CK(cudaMemcpyAsync(&err, error, 4, cudaMemcpyDeviceToHost, s));
-    HELIO_CK(cudaStreamSynchronize(s));
     HELIO_ARG(!(err & kErrOffset), "virtual geometry descriptor offset overflow");
     b->object_count = (uint32_t)objects;
     b->meshlet_count = (uint32_t)descriptors;

@@ -84,6 +84,33 @@ def test_reference_rebuild_tests(cuda):
     assert [[ids[i["object_index"]], int(i["local_meshlet_base"])] for i in items] == k["expected"]
 
 
+def test_reused_builder_grows_and_shrinks(cuda):
+    """One builder over libraries of changing size: the output passes run before the host
+    has read the totals, with the buffers the builder holds; when those are too small they
+    leave and run again once sized. Every run matches the oracle byte for byte, and the
+    error of a bad library leaves the builder usable."""
+    libs = [random_library(21, slots=300), random_library(22, slots=5000), random_library(23, slots=300),
+            random_library(24, slots=5000)]
+    b = None
+    for i, lib in enumerate(libs * 2):
+        ref = O.vg_rebuild(lib.pool, lib.meshes, lib.slot_mesh, lib.slot_instances)
+        b, host, _ = gpu_build(lib, b)
+        assert_same(host, ref)
+        assert b.frame_data().object_count == len(ref["objects"]), f"run {i}"
+    bad = random_library(25, slots=5000)
+    used = int(bad.slot_mesh[bad.slot_mesh < len(bad.meshes)][0])
+    bad.meshes[used]["meshlet_count"] = max(int(bad.meshes[used]["meshlet_count"]), 1)
+    bad.meshes[used]["lod_count"] = max(int(bad.meshes[used]["lod_count"]), 1)
+    bad.meshes[used]["first_meshlet"] = len(bad.pool)
+    from helio_b200 import native as N
+
+    with pytest.raises(N.HelioError):
+        gpu_build(bad, b)
+    ref = O.vg_rebuild(libs[1].pool, libs[1].meshes, libs[1].slot_mesh, libs[1].slot_instances)
+    _, host, _ = gpu_build(libs[1], b)
+    assert_same(host, ref)
+
+
 def test_empty_and_all_free(cuda):
     from helio_b200 import native as N
 
