@@ -815,7 +815,7 @@ __device__ void phase_test(const BatchParams& P, uint32_t groups, char* sm) {
                     const HelioGpuInstanceData* in = S.instances + j_inst;
                     const HelioInstanceCullData cd = load_cull(S.cull + j_inst);
                     const Mat4 model = ldg_mat4(in->model);
-                    cand = meshlet_frustum_cone(cv, load_meshlet(S, mi, in), model, cd, c, wr);
+                    cand = meshlet_frustum_cone_lazy(cv, S, mi, in, model, cd, c, wr);
                 }
             }
             const uint32_t b = __ballot_sync(0xffffffffu, cand);
@@ -1138,7 +1138,7 @@ __global__ void __launch_bounds__(kBatchThreads, 3) batch_kernel(const __grid_co
 // Phases 4..6 as a second cooperative launch: the meshlet tests need fewer registers
 // than the select, so this kernel runs more warps per SM. The kernel boundary is the
 // barrier after the expansion.
-__global__ void __launch_bounds__(kBatchThreads, 4) batch_cull_kernel(BatchParams P) {
+__global__ void __launch_bounds__(kBatchThreads, 5) batch_cull_kernel(BatchParams P) {
     extern __shared__ __align__(16) char sm[];
     uint32_t* s_tmp = reinterpret_cast<uint32_t*>(sm + kSm2Misc);
     // A barrier of the first launch gave up: its span list may be incomplete.

@@ -109,6 +109,36 @@ __device__ __forceinline__ bool meshlet_frustum_cone(const CullView& C, const Me
     return true;
 }
 
+// The same tests with the cone inputs (apex, axis, the instance's normal matrix) loaded
+// only for meshlets whose sphere passes the frustum: fewer registers live at a time, for
+// kernels that run more warps per SM instead of more loads per warp.
+__device__ __forceinline__ bool meshlet_frustum_cone_lazy(const CullView& C, const VgSceneDev& S, uint32_t mi,
+                                                          const HelioGpuInstanceData* inst, const Mat4& model,
+                                                          const HelioInstanceCullData& cd, F3& c, float& wr) {
+    if (cd.valid_transform == 0u) return false;
+    const float4 b = __ldg(S.m_bounds + mi);
+    c = mat4_point3(model, f3(b.x, b.y, b.z));
+    wr = fmaxf(fmul(b.w, cd.max_scale), 0.0f);
+    if (!sphere_visible_vg(C.planes, c, wr)) return false;
+    if (cd.cone_cull_enabled != 0u) {
+        const F3 cam = f3(C.pos_near.x, C.pos_near.y, C.pos_near.z);
+        const F3 ctc = sub3(c, cam);
+        const float cam_dist_sq = dot3(ctc, ctc);
+        const float guard = fmul(wr, 1.5f);
+        const float4 cone = __ldg(S.m_cone + mi);
+        if (cam_dist_sq > fmul(guard, guard) && cone.w <= 1.0f) {
+            const float4 axis = __ldg(S.m_axis + mi);
+            const float4* nm = reinterpret_cast<const float4*>(inst->normal_mat);
+            const F3 a = mat3_vec(__ldg(nm), __ldg(nm + 1), __ldg(nm + 2), f3(axis.x, axis.y, axis.z));
+            const F3 apex = mat4_point3(model, f3(cone.x, cone.y, cone.z));
+            const F3 cta = sub3(apex, cam);
+            const float ads = dot3(cta, cta);
+            if (ads > 1.0e-12f && cone_rejects(a, cta, ads, cone.w)) return false;
+        }
+    }
+    return true;
+}
+
 // cull_meshlet, second part (vg_cull.wgsl:184-240): the conservative Hi-Z test of
 // the sphere (c, wr). True = visible. kCoherentHiz: the pyramid was written
 // earlier in the same launch.
