@@ -20,6 +20,8 @@
 //     The reference appends with atomicAdd (vg_cull.wgsl:247), so its order is
 //     unspecified; this order is reproducible and first_instance = slot.
 
+#include <algorithm>
+
 #include "common.cuh"
 #include "kernels.h"
 #include "vg.h"
@@ -236,7 +238,13 @@ __device__ __forceinline__ WarpItems load_warp_items(const VgSceneDev& S, const 
 
 constexpr int kBitWordsPerWarp = kWindowsPerWarp + 2;  // +2 so bit-field reads stay in bounds
 
-__global__ void __launch_bounds__(kCullWarps * 32) vg_cull_test_kernel(VgCullParams P) {
+// kWide: the form for large scenes, whose warps each walk many windows (32 work items per
+// warp) and whose launch has more tiles than fit at four CTAs per SM: they gain more from a
+// fifth resident CTA than they lose to loading the cone inputs after the frustum test (10M
+// meshlets at 3840x2160: 27.3 -> 25.0 us). With fewer items per warp each warp's latency
+// dominates, and the loads stay together (1M meshlets: 43.6 against 45.5 us per step).
+template <bool kWide>
+__global__ void __launch_bounds__(kCullWarps * 32, kWide ? 5 : 4) vg_cull_test_kernel(VgCullParams P) {
     __shared__ CullView s_view;
     __shared__ uint32_t s_bits[kCullWarps][kBitWordsPerWarp];
 
@@ -271,7 +279,7 @@ __global__ void __launch_bounds__(kCullWarps * 32) vg_cull_test_kernel(VgCullPar
                 const HelioGpuInstanceData* in = S.instances + j_inst;
                 const HelioInstanceCullData cd = load_cull(S.cull + j_inst);
                 const Mat4 model = ldg_mat4(in->model);
-                vis = meshlet_visible(S, s_view, mi, model, cd, in);
+                vis = meshlet_visible<false, kWide>(S, s_view, mi, model, cd, in);
             }
         }
         const uint32_t bits = __ballot_sync(0xffffffffu, vis);
@@ -429,8 +437,12 @@ cudaError_t launch_after(void (*kernel)(VgCullParams), uint32_t grid, const VgCu
 
 cudaError_t launch_vg_cull(const VgCullParams& p, cudaStream_t stream) {
     if (!p.num_tiles) return cudaSuccess;
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const bool wide = p.items_per_warp >= 32u && p.num_tiles > 4u * (uint32_t)std::max(sms, 1);
     helio_launch_begin("vg_cull_test", stream);
-    cudaError_t e = launch_after(vg_cull_test_kernel, p.num_tiles, p, stream);
+    cudaError_t e = launch_after(wide ? vg_cull_test_kernel<true> : vg_cull_test_kernel<false>, p.num_tiles, p, stream);
     helio_launch_end(stream);
     if (e != cudaSuccess) return e;
     helio_launch_begin("vg_cull_emit", stream);

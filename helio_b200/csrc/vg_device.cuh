@@ -181,14 +181,17 @@ __device__ __forceinline__ bool meshlet_hiz_visible(const CullView& C, F3 c, flo
     return true;
 }
 
-// cull_meshlet decision part (vg_cull.wgsl:143-240): true = emit a draw.
-template <bool kCoherentHiz = false>
+// cull_meshlet decision part (vg_cull.wgsl:143-240): true = emit a draw. kLazyCone: the
+// cone inputs are loaded after the frustum test (fewer live registers), else with the sphere.
+template <bool kCoherentHiz = false, bool kLazyCone = false>
 __device__ __forceinline__ bool meshlet_visible(const VgSceneDev& S, const CullView& C, uint32_t mi,
                                                 const Mat4& model, const HelioInstanceCullData& cd,
                                                 const HelioGpuInstanceData* inst) {
     F3 c;
     float wr;
-    if (!meshlet_frustum_cone(C, load_meshlet(S, mi, inst), model, cd, c, wr)) return false;
+    const bool cand = kLazyCone ? meshlet_frustum_cone_lazy(C, S, mi, inst, model, cd, c, wr)
+                                : meshlet_frustum_cone(C, load_meshlet(S, mi, inst), model, cd, c, wr);
+    if (!cand) return false;
     return meshlet_hiz_visible<kCoherentHiz>(C, c, wr);
 }
 
