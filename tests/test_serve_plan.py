@@ -35,3 +35,25 @@ def test_empty_queue_and_invalid_head(native_built):
         plan_batch([(0, 129)], 128)
     with pytest.raises(N.HelioError):
         plan_batch([(0, 0)], 128)
+
+
+def test_device_occupancy_is_the_union_of_batch_intervals():
+    """The serving bench line's `device` figures: overlapping batches (two slots) count once,
+    gaps count as idle, and requests of one batch (same interval) count once."""
+    import sys
+    from pathlib import Path
+
+    sys.path.insert(0, str(Path(__file__).resolve().parents[1]))
+    from bench import device_occupancy
+
+    comps = [{"status": 0, "device_start_ms": 0.0, "device_end_ms": 2.0},
+             {"status": 0, "device_start_ms": 1.0, "device_end_ms": 3.0},  # overlaps the first
+             {"status": 0, "device_start_ms": 5.0, "device_end_ms": 6.0},
+             {"status": 0, "device_start_ms": 5.0, "device_end_ms": 6.0},  # same batch
+             {"status": 7, "device_start_ms": 6.0, "device_end_ms": 9.0}]  # failed: not counted
+    d = device_occupancy(comps)
+    assert d["batches"] == 3
+    assert d["span_ms"] == 6.0
+    assert abs(d["busy_fraction"] - 4.0 / 6.0) < 1e-12
+    assert abs(d["batch_device_ms_mean"] - 5.0 / 3.0) < 1e-12
+    assert device_occupancy([{"status": 7, "device_start_ms": 0.0, "device_end_ms": 1.0}]) is None
